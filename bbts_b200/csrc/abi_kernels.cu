@@ -1,0 +1,596 @@
+// C-ABI entry points for the block kernels (declared in include/bbts_b200.h).
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#include "bbts_b200.h"
+#include "common.h"
+#include "gemm_f32.cuh"
+#include "gemm_tc.cuh"
+#include "stream_ops.cuh"
+
+namespace bbx {
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string t_last_error;
+
+int set_error(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  t_last_error = buf;
+  return code;
+}
+
+const std::string& last_error() { return t_last_error; }
+
+#define BBX_CUDA(call)                                                                  \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return set_error(BBX_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                       __FILE__, __LINE__);                                             \
+  } while (0)
+
+#define BBX_CHECK_LAUNCH(name)                                                          \
+  do {                                                                                  \
+    cudaError_t e_ = cudaGetLastError();                                                \
+    if (e_ != cudaSuccess)                                                              \
+      return set_error(BBX_ERR_CUDA, "launch of %s failed: %s", name, cudaGetErrorString(e_)); \
+  } while (0)
+
+// ------------------------------------------------------------------ per-device state
+struct DeviceState {
+  bool ready = false;
+  int sms = 148;
+  uint32_t* status = nullptr;       // kernel status word
+  unsigned int* scratch = nullptr;  // absmax word for FP8 quantisation
+  uint32_t attr_done = 0;           // bitmask of tcgen05 kernels with smem attribute set
+};
+static std::mutex g_dev_mu;
+static DeviceState g_dev[64];
+
+int device_state(DeviceState** out) {
+  int dev = 0;
+  BBX_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return set_error(BBX_ERR_INVALID, "device index %d out of range", dev);
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  DeviceState& d = g_dev[dev];
+  if (!d.ready) {
+    BBX_CUDA(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
+    BBX_CUDA(cudaMalloc(&d.status, 256));
+    BBX_CUDA(cudaMemset(d.status, 0, 256));
+    d.scratch = (unsigned int*)(d.status + 16);
+    d.ready = true;
+  }
+  *out = &d;
+  return BBX_OK;
+}
+
+static inline int grid_for(long long work_items, int threads, int sms) {
+  long long blocks = (work_items + threads - 1) / threads;
+  long long cap = (long long)sms * 8;  // 8 resident blocks of 256 threads per SM
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  return (int)blocks;
+}
+
+// ------------------------------------------------------------------ tensor maps
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static int get_encode_fn(EncodeTiledFn* fn) {
+  static EncodeTiledFn cached = nullptr;
+  static std::once_flag once;
+  static cudaError_t err = cudaSuccess;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    err = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
+    if (err == cudaSuccess && q == cudaDriverEntryPointSuccess) cached = (EncodeTiledFn)p;
+  });
+  if (!cached)
+    return set_error(BBX_ERR_CUDA, "cuTensorMapEncodeTiled unavailable (%s)", cudaGetErrorString(err));
+  *fn = cached;
+  return BBX_OK;
+}
+
+// 2-D map over a row-major matrix with `rows` rows of `cols` elements and pitch
+// `ld` elements; box = box_cols x box_rows, 128-byte swizzle, zero OOB fill.
+static int make_map(CUtensorMap* map, const void* base, int dtype, long long rows, long long cols,
+                    long long ld, int box_cols, int box_rows) {
+  EncodeTiledFn enc;
+  int rc = get_encode_fn(&enc);
+  if (rc) return rc;
+  const int esz = dtype == BBX_E4M3 ? 1 : 2;
+  CUtensorMapDataType dt =
+      dtype == BBX_E4M3 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)(ld * esz)};
+  cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    return set_error(BBX_ERR_INVALID,
+                     "cuTensorMapEncodeTiled failed (%d): rows=%lld cols=%lld ld=%lld box=%dx%d",
+                     (int)r, rows, cols, ld, box_cols, box_rows);
+  return BBX_OK;
+}
+
+// ------------------------------------------------------------------ tcgen05 dispatch
+template <int BN, bool AMN, bool BMN, bool FP8>
+static int launch_tc_variant(const TcArgs& args, int grid, cudaStream_t st, DeviceState* d,
+                             int bit) {
+  using C = TcCfg<BN, AMN, BMN, FP8>;
+  auto kern = tc_gemm_kernel<BN, AMN, BMN, FP8>;
+  if (!(d->attr_done & (1u << bit))) {
+    BBX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM_BYTES));
+    d->attr_done |= (1u << bit);
+  }
+  kern<<<grid, C::THREADS, C::SMEM_BYTES, st>>>(args);
+  BBX_CHECK_LAUNCH("tc_gemm_kernel");
+  return BBX_OK;
+}
+
+static int launch_tc(int bn, bool amn, bool bmn, bool fp8, const TcArgs& args, int grid,
+                     cudaStream_t st, DeviceState* d) {
+  const int bit = (bn == 256 ? 8 : 0) | (amn ? 4 : 0) | (bmn ? 2 : 0) | (fp8 ? 1 : 0);
+#define TC_CASE(BN_, A_, B_, F_)                                                         \
+  if (bn == BN_ && amn == A_ && bmn == B_ && fp8 == F_)                                  \
+    return launch_tc_variant<BN_, A_, B_, F_>(args, grid, st, d, bit);
+  TC_CASE(256, false, false, false) TC_CASE(256, false, true, false)
+  TC_CASE(256, true, false, false) TC_CASE(256, true, true, false)
+  TC_CASE(128, false, false, false) TC_CASE(128, false, true, false)
+  TC_CASE(128, true, false, false) TC_CASE(128, true, true, false)
+  TC_CASE(256, false, false, true) TC_CASE(256, false, true, true)
+  TC_CASE(256, true, false, true) TC_CASE(256, true, true, true)
+  TC_CASE(128, false, false, true) TC_CASE(128, false, true, true)
+  TC_CASE(128, true, false, true) TC_CASE(128, true, true, true)
+#undef TC_CASE
+  return set_error(BBX_ERR_UNSUPPORTED, "no tcgen05 variant for tile_n=%d", bn);
+}
+
+// Validates one public problem and fills the device record (minus tile_start).
+static int build_problem(int in_dtype, const bbx_tc_problem_t& q, int bn, TcProblem* out) {
+  if (!q.a || !q.b || !q.c) return set_error(BBX_ERR_INVALID, "null operand pointer");
+  if (q.m <= 0 || q.n <= 0 || q.k <= 0)
+    return set_error(BBX_ERR_INVALID, "bad shape m=%d n=%d k=%d", q.m, q.n, q.k);
+  const int esz = in_dtype == BBX_E4M3 ? 1 : 2;
+  if ((((uintptr_t)q.a) | ((uintptr_t)q.b)) & 15)
+    return set_error(BBX_ERR_INVALID, "tensor-core operands must be 16-byte aligned");
+  if (((q.lda * esz) & 15) || ((q.ldb * esz) & 15))
+    return set_error(BBX_ERR_INVALID, "operand pitches must be multiples of 16 bytes (lda=%lld ldb=%lld)",
+                     q.lda, q.ldb);
+  const bool amn = q.trans_a != 0, bmn = q.trans_b == 0;
+  const int bk = 128 / esz, mnbox = 128 / esz;
+  std::memset(out, 0, sizeof(TcProblem));
+  int rc;
+  // A: op(A) is m x k. Not transposed -> stored m x k (K-major); transposed -> k x m (MN-major).
+  if (!amn) {
+    if (q.lda < q.k) return set_error(BBX_ERR_INVALID, "lda < k");
+    rc = make_map(&out->tmap_a, q.a, in_dtype, q.m, q.k, q.lda, bk, 128);
+  } else {
+    if (q.lda < q.m) return set_error(BBX_ERR_INVALID, "lda < m");
+    rc = make_map(&out->tmap_a, q.a, in_dtype, q.k, q.m, q.lda, mnbox, bk);
+  }
+  if (rc) return rc;
+  // B: op(B) is k x n. Not transposed -> stored k x n (MN-major); transposed -> n x k (K-major).
+  if (!bmn) {
+    if (q.ldb < q.k) return set_error(BBX_ERR_INVALID, "ldb < k");
+    rc = make_map(&out->tmap_b, q.b, in_dtype, q.n, q.k, q.ldb, bk, bn);
+  } else {
+    if (q.ldb < q.n) return set_error(BBX_ERR_INVALID, "ldb < n");
+    rc = make_map(&out->tmap_b, q.b, in_dtype, q.k, q.n, q.ldb, mnbox, bk);
+  }
+  if (rc) return rc;
+  if (q.ldc < q.n) return set_error(BBX_ERR_INVALID, "ldc < n");
+  if ((q.flags & BBX_EPI_BIAS) && !q.bias) return set_error(BBX_ERR_INVALID, "bias flag without bias");
+  out->c = q.c;
+  out->bias = q.bias;
+  out->ldc = q.ldc;
+  out->m = q.m;
+  out->n = q.n;
+  out->k = q.k;
+  out->tiles_m = (q.m + 127) / 128;
+  out->tiles_n = (q.n + bn - 1) / bn;
+  out->alpha = q.alpha;
+  out->beta = q.beta;
+  out->flags = q.flags & (EPI_RELU | EPI_OUT_BF16 | EPI_BIAS | EPI_BETA);
+  return BBX_OK;
+}
+
+int pick_tile_n(const bbx_tc_problem_t* probs, int count) {
+  int maxn = 0;
+  for (int i = 0; i < count; ++i) maxn = std::max(maxn, probs[i].n);
+  return maxn > 128 ? 256 : 128;
+}
+
+// Layout class shared by every problem of a group (one kernel variant per launch).
+static int group_layout(const bbx_tc_problem_t* probs, int count, bool* amn, bool* bmn) {
+  *amn = probs[0].trans_a != 0;
+  *bmn = probs[0].trans_b == 0;
+  for (int i = 1; i < count; ++i)
+    if ((probs[i].trans_a != 0) != *amn || (probs[i].trans_b == 0) != *bmn)
+      return set_error(BBX_ERR_INVALID, "all problems of a group must share transpose flags");
+  return BBX_OK;
+}
+
+}  // namespace bbx
+
+using namespace bbx;
+
+struct bbx_tc_plan {
+  int dtype = BBX_BF16;
+  int bn = 256;
+  bool amn = false, bmn = true;
+  int count = 0;
+  int total_tiles = 0;
+  int device = 0;
+  TcProblem* d_table = nullptr;
+  std::vector<TcProblem> host;  // kept for inline launches (count <= kTcMaxInline)
+};
+
+extern "C" {
+
+const char* bbx_version(void) { return "bbts_b200 0.1 (sm_100a)"; }
+
+int bbx_last_error(char* buf, size_t len) {
+  const std::string& e = last_error();
+  if (buf && len) {
+    size_t n = std::min(len - 1, e.size());
+    memcpy(buf, e.data(), n);
+    buf[n] = 0;
+  }
+  return (int)e.size();
+}
+
+int bbx_num_sms(void) {
+  DeviceState* d;
+  if (device_state(&d)) return -1;
+  return d->sms;
+}
+
+int bbx_check_device_status(void* stream, uint32_t* code_out) {
+  DeviceState* d;
+  int rc = device_state(&d);
+  if (rc) return rc;
+  BBX_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+  uint32_t code = 0;
+  BBX_CUDA(cudaMemcpy(&code, d->status, 4, cudaMemcpyDeviceToHost));
+  if (code_out) *code_out = code;
+  if (code) {
+    BBX_CUDA(cudaMemset(d->status, 0, 4));
+    return set_error(BBX_ERR_DEVICE, "a kernel reported device status %u (bounded wait expired)", code);
+  }
+  return BBX_OK;
+}
+
+int bbx_matmul_f32(const float* a, const float* b, float* c, int m, int n, int k, long long lda,
+                   long long ldb, long long ldc, int trans_a, int trans_b, float alpha, float beta,
+                   const float* bias, int relu, int batch, long long stride_a, long long stride_b,
+                   long long stride_c, void* stream) {
+  if (!a || !b || !c) return set_error(BBX_ERR_INVALID, "null pointer");
+  if (m <= 0 || n <= 0 || k < 0 || batch <= 0 || batch > 65535)
+    return set_error(BBX_ERR_INVALID, "bad shape m=%d n=%d k=%d batch=%d", m, n, k, batch);
+  F32GemmArgs g;
+  g.a = a; g.b = b; g.c = c; g.bias = bias;
+  g.m = m; g.n = n; g.k = k;
+  g.lda = lda; g.ldb = ldb; g.ldc = ldc;
+  g.stride_a = stride_a; g.stride_b = stride_b; g.stride_c = stride_c;
+  g.trans_a = trans_a; g.trans_b = trans_b;
+  g.alpha = alpha; g.beta = beta; g.relu = relu;
+  dim3 grid((n + F32_BN - 1) / F32_BN, (m + F32_BM - 1) / F32_BM, batch);
+  if (grid.y > 65535) return set_error(BBX_ERR_INVALID, "m too large");
+  k_gemm_f32<<<grid, 256, 0, (cudaStream_t)stream>>>(g);
+  BBX_CHECK_LAUNCH("k_gemm_f32");
+  return BBX_OK;
+}
+
+int bbx_tc_plan_create(int in_dtype, const bbx_tc_problem_t* problems, int count, int tile_n,
+                       bbx_tc_plan_t** out) {
+  if (!out || !problems || count <= 0) return set_error(BBX_ERR_INVALID, "bad plan arguments");
+  if (in_dtype != BBX_BF16 && in_dtype != BBX_E4M3)
+    return set_error(BBX_ERR_UNSUPPORTED, "tensor-core input dtype must be bf16 or e4m3");
+  if (tile_n == 0) tile_n = pick_tile_n(problems, count);
+  if (tile_n != 128 && tile_n != 256) return set_error(BBX_ERR_INVALID, "tile_n must be 128 or 256");
+  DeviceState* d;
+  int rc = device_state(&d);
+  if (rc) return rc;
+  auto* p = new bbx_tc_plan();
+  p->dtype = in_dtype;
+  p->bn = tile_n;
+  p->count = count;
+  cudaGetDevice(&p->device);
+  rc = group_layout(problems, count, &p->amn, &p->bmn);
+  if (rc) { delete p; return rc; }
+  p->host.resize(count);
+  int tiles = 0;
+  for (int i = 0; i < count; ++i) {
+    rc = build_problem(in_dtype, problems[i], tile_n, &p->host[i]);
+    if (rc) { delete p; return rc; }
+    p->host[i].tile_start = tiles;
+    tiles += p->host[i].tiles_m * p->host[i].tiles_n;
+  }
+  p->total_tiles = tiles;
+  if (count > kTcMaxInline) {
+    cudaError_t e = cudaMalloc(&p->d_table, sizeof(TcProblem) * count);
+    if (e != cudaSuccess) { delete p; return set_error(BBX_ERR_CUDA, "cudaMalloc(plan table): %s", cudaGetErrorString(e)); }
+    e = cudaMemcpy(p->d_table, p->host.data(), sizeof(TcProblem) * count, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { cudaFree(p->d_table); delete p; return set_error(BBX_ERR_CUDA, "plan upload: %s", cudaGetErrorString(e)); }
+  }
+  *out = p;
+  return BBX_OK;
+}
+
+int bbx_tc_plan_launch(bbx_tc_plan_t* p, void* stream) {
+  if (!p) return set_error(BBX_ERR_INVALID, "null plan");
+  DeviceState* d;
+  int rc = device_state(&d);
+  if (rc) return rc;
+  TcArgs args;
+  memset(&args, 0, sizeof(args));
+  args.table = p->d_table;
+  args.num_problems = p->count;
+  args.total_tiles = p->total_tiles;
+  args.status = d->status;
+  if (!p->d_table)
+    for (int i = 0; i < p->count; ++i) args.inline_probs[i] = p->host[i];
+  const int grid = std::min(p->total_tiles, d->sms);
+  return launch_tc(p->bn, p->amn, p->bmn, p->dtype == BBX_E4M3, args, grid,
+                   (cudaStream_t)stream, d);
+}
+
+int bbx_tc_plan_destroy(bbx_tc_plan_t* p) {
+  if (!p) return BBX_OK;
+  if (p->d_table) cudaFree(p->d_table);
+  delete p;
+  return BBX_OK;
+}
+
+int bbx_matmul_tc(int in_dtype, const bbx_tc_problem_t* problems, int count, int tile_n,
+                  void* stream) {
+  if (count <= 0 || !problems) return set_error(BBX_ERR_INVALID, "no problems");
+  if (count <= kTcMaxInline) {
+    bbx_tc_plan_t* p = nullptr;
+    int rc = bbx_tc_plan_create(in_dtype, problems, count, tile_n, &p);
+    if (rc) return rc;
+    rc = bbx_tc_plan_launch(p, stream);
+    bbx_tc_plan_destroy(p);  // inline plans own no device memory
+    return rc;
+  }
+  // Larger groups: stream-ordered table upload, freed after the launch in stream order.
+  if (in_dtype != BBX_BF16 && in_dtype != BBX_E4M3)
+    return set_error(BBX_ERR_UNSUPPORTED, "tensor-core input dtype must be bf16 or e4m3");
+  if (tile_n == 0) tile_n = pick_tile_n(problems, count);
+  DeviceState* d;
+  int rc = device_state(&d);
+  if (rc) return rc;
+  bool amn, bmn;
+  rc = group_layout(problems, count, &amn, &bmn);
+  if (rc) return rc;
+  std::vector<TcProblem> host(count);
+  int tiles = 0;
+  for (int i = 0; i < count; ++i) {
+    rc = build_problem(in_dtype, problems[i], tile_n, &host[i]);
+    if (rc) return rc;
+    host[i].tile_start = tiles;
+    tiles += host[i].tiles_m * host[i].tiles_n;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  TcProblem* table = nullptr;
+  BBX_CUDA(cudaMallocAsync(&table, sizeof(TcProblem) * count, st));
+  BBX_CUDA(cudaMemcpyAsync(table, host.data(), sizeof(TcProblem) * count, cudaMemcpyHostToDevice, st));
+  // The pageable source above is staged by the driver before cudaMemcpyAsync returns.
+  TcArgs args;
+  memset(&args, 0, sizeof(args));
+  args.table = table;
+  args.num_problems = count;
+  args.total_tiles = tiles;
+  args.status = d->status;
+  rc = launch_tc(tile_n, amn, bmn, in_dtype == BBX_E4M3, args, std::min(tiles, d->sms), st, d);
+  cudaFreeAsync(table, st);
+  return rc;
+}
+
+int bbx_add_f32(const float* a, const float* b, float* c, long long n, void* stream) {
+  return bbx_binary_f32(BBX_B_ADD, a, b, c, n, 1.f, 1.f, stream);
+}
+
+int bbx_binary_f32(int op, const float* a, const float* b, float* c, long long n, float ca,
+                   float cb, void* stream) {
+  if (op < 0 || op > B_DIV) return set_error(BBX_ERR_INVALID, "unknown binary op %d", op);
+  if (n == 0) return BBX_OK;
+  if (!a || !b || !c || n < 0) return set_error(BBX_ERR_INVALID, "bad binary arguments");
+  DeviceState* d;
+  int rc = device_state(&d);
+  if (rc) return rc;
+  k_binary<<<grid_for((n + 3) / 4, 256, d->sms), 256, 0, (cudaStream_t)stream>>>(op, a, b, c, n, ca, cb);
+  BBX_CHECK_LAUNCH("k_binary");
+  return BBX_OK;
+}
+
+int bbx_unary_f32(int op, const float* in, float* out, long long n, float param, void* stream) {
+  if (op < 0 || op > U_SCALE) return set_error(BBX_ERR_INVALID, "unknown unary op %d", op);
+  if (n == 0) return BBX_OK;
+  if (!in || !out || n < 0) return set_error(BBX_ERR_INVALID, "bad unary arguments");
+  DeviceState* d;
+  int rc = device_state(&d);
+  if (rc) return rc;
+  k_unary<<<grid_for((n + 3) / 4, 256, d->sms), 256, 0, (cudaStream_t)stream>>>(op, in, out, n, param);
+  BBX_CHECK_LAUNCH("k_unary");
+  return BBX_OK;
+}
+
+int bbx_reduce_f32(const float* const* inputs, int n_in, float* out, long long n, int kahan,
+                   void* stream) {
+  if (!inputs || !out || n_in < 1 || n < 0) return set_error(BBX_ERR_INVALID, "bad reduce arguments");
+  for (int i = 0; i < n_in; ++i)
+    if (!inputs[i]) return set_error(BBX_ERR_INVALID, "null reduce input %d", i);
+  if (n == 0) return BBX_OK;
+  DeviceState* d;
+  int rc = device_state(&d);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  // Chunks of up to 32 inputs; later chunks fold into `out` first, which keeps
+  // the left-to-right order (out = ((in0+...+in31) + in32) + ...). With Kahan
+  // the compensation restarts at chunk boundaries.
+  int done = 0;
+  while (done < n_in) {
+    ReduceArgs ra;
+    int cnt = 0;
+    if (done > 0) ra.in[cnt++] = out;
+    while (cnt < kMaxReduceInputs && done < n_in) ra.in[cnt++] = inputs[done++];
+    if (cnt == 1) {
+      if (ra.in[0] != out) BBX_CUDA(cudaMemcpyAsync(out, ra.in[0], n * 4, cudaMemcpyDeviceToDevice, st));
+      continue;
+    }
+    const int grid = grid_for((n + 3) / 4, 256, d->sms);
+    if (kahan) k_reduce<true><<<grid, 256, 0, st>>>(ra, cnt, out, n);
+    else k_reduce<false><<<grid, 256, 0, st>>>(ra, cnt, out, n);
+    BBX_CHECK_LAUNCH("k_reduce");
+  }
+  return BBX_OK;
+}
+
+int bbx_bias_add_f32(const float* in, const float* bias, float* out, int rows, int cols, int relu,
+                     void* stream) {
+  if (!in || !bias || !out || rows < 0 || cols <= 0) return set_error(BBX_ERR_INVALID, "bad bias_add arguments");
+  if (rows == 0) return BBX_OK;
+  DeviceState* d;
+  int rc = device_state(&d);
+  if (rc) return rc;
+  k_bias_add<<<grid_for((long long)rows * cols, 256, d->sms), 256, 0, (cudaStream_t)stream>>>(in, bias, out, rows, cols, relu);
+  BBX_CHECK_LAUNCH("k_bias_add");
+  return BBX_OK;
+}
+
+int bbx_colsum_f32(const float* in, float* out, int rows, int cols, long long ld, int accumulate,
+                   void* stream) {
+  if (!in || !out || rows < 0 || cols <= 0 || ld < cols) return set_error(BBX_ERR_INVALID, "bad colsum arguments");
+  k_colsum<<<(cols + 127) / 128, 128, 0, (cudaStream_t)stream>>>(in, out, rows, cols, ld, accumulate);
+  BBX_CHECK_LAUNCH("k_colsum");
+  return BBX_OK;
+}
+
+int bbx_cast(int src_dtype, const void* in, int dst_dtype, void* out, long long n, void* stream) {
+  if (!in || !out || n < 0) return set_error(BBX_ERR_INVALID, "bad cast arguments");
+  if (n == 0) return BBX_OK;
+  DeviceState* d;
+  int rc = device_state(&d);
+  if (rc) return rc;
+  const int grid = grid_for(n, 256, d->sms);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (src_dtype == BBX_F32 && dst_dtype == BBX_BF16) {
+    k_f32_to_bf16<<<grid, 256, 0, st>>>((const float*)in, (__nv_bfloat16*)out, n);
+  } else if (src_dtype == BBX_BF16 && dst_dtype == BBX_F32) {
+    k_bf16_to_f32<<<grid, 256, 0, st>>>((const __nv_bfloat16*)in, (float*)out, n);
+  } else if (src_dtype == dst_dtype) {
+    BBX_CUDA(cudaMemcpyAsync(out, in, n * (src_dtype == BBX_F32 ? 4 : src_dtype == BBX_BF16 ? 2 : 1),
+                             cudaMemcpyDeviceToDevice, st));
+    return BBX_OK;
+  } else {
+    return set_error(BBX_ERR_UNSUPPORTED, "cast %d -> %d", src_dtype, dst_dtype);
+  }
+  BBX_CHECK_LAUNCH("cast");
+  return BBX_OK;
+}
+
+int bbx_quantize_e4m3(int src_dtype, const void* in, void* out, int rows, int cols, int transpose,
+                      float* scale_out, void* stream) {
+  if (!in || !out || !scale_out || rows <= 0 || cols <= 0) return set_error(BBX_ERR_INVALID, "bad quantize arguments");
+  if (src_dtype != BBX_F32 && src_dtype != BBX_BF16) return set_error(BBX_ERR_UNSUPPORTED, "quantize source dtype");
+  DeviceState* d;
+  int rc = device_state(&d);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long n = (long long)rows * cols;
+  const int grid = grid_for(n, 256, d->sms);
+  BBX_CUDA(cudaMemsetAsync(d->scratch, 0, 4, st));
+  if (src_dtype == BBX_F32) {
+    k_absmax<float><<<grid, 256, 0, st>>>((const float*)in, n, d->scratch);
+    k_quant_e4m3<float><<<grid, 256, 0, st>>>((const float*)in, (__nv_fp8_e4m3*)out, rows, cols, d->scratch, scale_out, transpose);
+  } else {
+    k_absmax<__nv_bfloat16><<<grid, 256, 0, st>>>((const __nv_bfloat16*)in, n, d->scratch);
+    k_quant_e4m3<__nv_bfloat16><<<grid, 256, 0, st>>>((const __nv_bfloat16*)in, (__nv_fp8_e4m3*)out, rows, cols, d->scratch, scale_out, transpose);
+  }
+  BBX_CHECK_LAUNCH("quantize_e4m3");
+  return BBX_OK;
+}
+
+int bbx_fill_philox(int dtype, void* out, long long n, unsigned long long seed, int dist, float a,
+                    float b, void* stream) {
+  if (!out || n < 0 || (dist != 0 && dist != 1)) return set_error(BBX_ERR_INVALID, "bad fill arguments");
+  if (n == 0) return BBX_OK;
+  DeviceState* d;
+  int rc = device_state(&d);
+  if (rc) return rc;
+  const int grid = grid_for((n + 3) / 4, 256, d->sms);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == BBX_F32) k_fill_philox<float><<<grid, 256, 0, st>>>((float*)out, n, seed, dist, a, b);
+  else if (dtype == BBX_BF16) k_fill_philox<__nv_bfloat16><<<grid, 256, 0, st>>>((__nv_bfloat16*)out, n, seed, dist, a, b);
+  else return set_error(BBX_ERR_UNSUPPORTED, "fill dtype %d", dtype);
+  BBX_CHECK_LAUNCH("k_fill_philox");
+  return BBX_OK;
+}
+
+int bbx_softmax_ce_f32(const float* logits, const int* labels, float* loss, float* grad, int rows,
+                       int cols, long long ld, float grad_scale, void* stream) {
+  if (!logits || !labels || !loss || rows < 0 || cols <= 0 || ld < cols)
+    return set_error(BBX_ERR_INVALID, "bad softmax_ce arguments");
+  if (rows == 0) return BBX_OK;
+  DeviceState* d;
+  int rc = device_state(&d);
+  if (rc) return rc;
+  const int warps = 8;
+  int grid = std::min((rows + warps - 1) / warps, d->sms * 8);
+  k_softmax_ce<<<grid, warps * 32, 0, (cudaStream_t)stream>>>(logits, labels, loss, grad, rows, cols, ld, grad_scale);
+  BBX_CHECK_LAUNCH("k_softmax_ce");
+  return BBX_OK;
+}
+
+int bbx_permute(const float* in, int rank, const long long* in_dims, const int* perm, int dst_dtype,
+                void* out, void* stream) {
+  if (!in || !out || !in_dims || !perm || rank < 1 || rank > 4)
+    return set_error(BBX_ERR_INVALID, "bad permute arguments");
+  if (dst_dtype != BBX_F32 && dst_dtype != BBX_BF16) return set_error(BBX_ERR_UNSUPPORTED, "permute dtype");
+  PermArgs pa;
+  memset(&pa, 0, sizeof(pa));
+  pa.rank = rank;
+  long long istr[4];
+  long long s = 1;
+  for (int d = rank - 1; d >= 0; --d) { istr[d] = s; s *= in_dims[d]; }
+  const long long n = s;
+  unsigned seen = 0;
+  for (int d = 0; d < rank; ++d) {
+    if (perm[d] < 0 || perm[d] >= rank || (seen & (1u << perm[d])))
+      return set_error(BBX_ERR_INVALID, "perm is not a permutation");
+    seen |= 1u << perm[d];
+    pa.odims[d] = in_dims[perm[d]];
+    pa.istride[d] = istr[perm[d]];
+  }
+  s = 1;
+  for (int d = rank - 1; d >= 0; --d) { pa.ostride[d] = s; s *= pa.odims[d]; }
+  if (n == 0) return BBX_OK;
+  DeviceState* dv;
+  int rc = device_state(&dv);
+  if (rc) return rc;
+  const int grid = grid_for(n, 256, dv->sms);
+  if (dst_dtype == BBX_F32) k_permute<float><<<grid, 256, 0, (cudaStream_t)stream>>>(in, (float*)out, pa, n);
+  else k_permute<__nv_bfloat16><<<grid, 256, 0, (cudaStream_t)stream>>>(in, (__nv_bfloat16*)out, pa, n);
+  BBX_CHECK_LAUNCH("k_permute");
+  return BBX_OK;
+}
+
+}  // extern "C"

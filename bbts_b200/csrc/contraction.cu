@@ -1,0 +1,261 @@
+// einsum contraction of the reference's "cutensor" block library
+// (libraries/cutensor/contraction.h): out = alpha * sum(lhs * rhs) over the
+// modes absent from the output, on column-major rank<=4 FP32 tensors.
+//
+// Lowering (one stream, stream-ordered temporaries):
+//   1. classify every mode as I (lhs+out), N (rhs+out), K (lhs+rhs, summed),
+//      B (all three, batch), L (lhs only, summed) or R (rhs only, summed) --
+//      the same classes the reference's cpu_op plan uses (contraction.h:229-253);
+//   2. gather lhs into Lc[b][m][k] and rhs into Rc[b][n][k] (k contiguous,
+//      pitch padded to 16 bytes for the tensor-core path, L/R modes summed in
+//      the gather);
+//   3. batched matmul Ct[b][n][m] = alpha * Rc[b] * Lc[b]^T: SIMT FP32 or
+//      tcgen05 BF16 with f32 accumulation;
+//   4. if the output's mode order is (I..., N..., B...), Ct already is the
+//      column-major output and step 3 wrote it in place; otherwise gather Ct
+//      into the output order.
+// Inside every group, modes are flattened column-major (first mode fastest),
+// I/N/B in output order and K in lhs order.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <cstring>
+#include <vector>
+#include "bbts_b200.h"
+#include "common.h"
+
+namespace bbx {
+
+struct GatherArgs {
+  int rank_o;               // output modes, outermost first
+  long long odims[4], istride[4], ostride[4];
+  int rank_s;               // summed modes
+  long long sdims[4], sstride[4];
+};
+
+template <typename TO>
+__global__ void k_gather_sum(const float* __restrict__ in, TO* out, const __grid_constant__ GatherArgs a,
+                             long long n) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    long long rem = e, src = 0, dst = 0;
+    for (int d = a.rank_o - 1; d >= 0; --d) {
+      long long idx = rem % a.odims[d];
+      rem /= a.odims[d];
+      src += idx * a.istride[d];
+      dst += idx * a.ostride[d];
+    }
+    float v;
+    if (a.rank_s == 0) {
+      v = in[src];
+    } else {
+      long long ns = 1;
+      for (int d = 0; d < a.rank_s; ++d) ns *= a.sdims[d];
+      v = 0.f;
+      for (long long s = 0; s < ns; ++s) {
+        long long r = s, off = 0;
+        for (int d = 0; d < a.rank_s; ++d) {
+          off += (r % a.sdims[d]) * a.sstride[d];
+          r /= a.sdims[d];
+        }
+        v += in[src + off];
+      }
+    }
+    if constexpr (sizeof(TO) == 4) out[dst] = v;
+    else out[dst] = __float2bfloat16_rn(v);
+  }
+}
+
+template <typename TO>
+static int launch_gather(const float* in, TO* out, const GatherArgs& a, long long n, cudaStream_t st) {
+  if (n == 0) return BBX_OK;
+  long long blocks = (n + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_gather_sum<TO><<<(int)blocks, 256, 0, st>>>(in, out, a, n);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(BBX_ERR_CUDA, "k_gather_sum: %s", cudaGetErrorString(e));
+  return BBX_OK;
+}
+
+enum { CI = 0, CN = 1, CB = 2, CK = 3, CL = 4, CR = 5 };
+
+}  // namespace bbx
+
+using namespace bbx;
+
+extern "C" int bbx_contraction(const float* lhs, int rank_l, const long long* dims_l,
+                               const int* modes_l, const float* rhs, int rank_r,
+                               const long long* dims_r, const int* modes_r, float* out, int rank_o,
+                               const int* modes_o, float alpha, int precision, void* stream) {
+  if (!lhs || !rhs || !out) return set_error(BBX_ERR_INVALID, "null tensor");
+  if (rank_l < 0 || rank_l > 4 || rank_r < 0 || rank_r > 4 || rank_o < 0 || rank_o > 4)
+    return set_error(BBX_ERR_INVALID, "ranks must be in [0,4] (MAXRANK of the cutensor format)");
+  if (precision != BBX_F32 && precision != BBX_BF16)
+    return set_error(BBX_ERR_UNSUPPORTED, "contraction precision %d", precision);
+  constexpr int MAXM = 16;
+  long long ext[MAXM];
+  bool inl[MAXM] = {}, inr[MAXM] = {}, ino[MAXM] = {};
+  for (int i = 0; i < MAXM; ++i) ext[i] = -1;
+  long long strl[MAXM] = {}, strr[MAXM] = {};
+  long long s = 1;
+  for (int d = 0; d < rank_l; ++d) {
+    int m = modes_l[d];
+    if (m < 0 || m >= MAXM || inl[m]) return set_error(BBX_ERR_INVALID, "bad lhs mode %d", m);
+    inl[m] = true; ext[m] = dims_l[d]; strl[m] = s; s *= dims_l[d];
+  }
+  s = 1;
+  for (int d = 0; d < rank_r; ++d) {
+    int m = modes_r[d];
+    if (m < 0 || m >= MAXM || inr[m]) return set_error(BBX_ERR_INVALID, "bad rhs mode %d", m);
+    if (ext[m] >= 0 && ext[m] != dims_r[d])
+      return set_error(BBX_ERR_INVALID, "mode %d has extent %lld in lhs and %lld in rhs", m, ext[m], dims_r[d]);
+    inr[m] = true; ext[m] = dims_r[d]; strr[m] = s; s *= dims_r[d];
+  }
+  for (int d = 0; d < rank_o; ++d) {
+    int m = modes_o[d];
+    if (m < 0 || m >= MAXM || ino[m]) return set_error(BBX_ERR_INVALID, "bad out mode %d", m);
+    if (!inl[m] && !inr[m]) return set_error(BBX_ERR_INVALID, "output mode %d is not an input mode", m);
+    ino[m] = true;
+  }
+  auto cls = [&](int m) {
+    if (inl[m] && inr[m]) return ino[m] ? (int)CB : (int)CK;
+    if (inl[m]) return ino[m] ? (int)CI : (int)CL;
+    return ino[m] ? (int)CN : (int)CR;
+  };
+  std::vector<int> gI, gN, gB, gK, gL, gR;
+  for (int d = 0; d < rank_o; ++d) {
+    int c = cls(modes_o[d]);
+    (c == CI ? gI : c == CN ? gN : gB).push_back(modes_o[d]);
+  }
+  for (int d = 0; d < rank_l; ++d) {
+    int c = cls(modes_l[d]);
+    if (c == CK) gK.push_back(modes_l[d]);
+    if (c == CL) gL.push_back(modes_l[d]);
+  }
+  for (int d = 0; d < rank_r; ++d)
+    if (cls(modes_r[d]) == CR) gR.push_back(modes_r[d]);
+  auto prod = [&](const std::vector<int>& g) { long long p = 1; for (int m : g) p *= ext[m]; return p; };
+  const long long nb = prod(gB), nm = prod(gI), nn = prod(gN), nk = prod(gK);
+  if (nb == 0 || nm == 0 || nn == 0) return BBX_OK;  // empty output
+  if (nm > (1ll << 31) - 1 || nn > (1ll << 31) - 1 || nk > (1ll << 31) - 1)
+    return set_error(BBX_ERR_INVALID, "contraction group too large");
+
+  cudaStream_t st = (cudaStream_t)stream;
+  const bool bf16 = precision == BBX_BF16;
+  const long long kdim = nk > 0 ? nk : 1;  // no contracted mode: an outer product, k = 1
+  const long long pk = bf16 ? ((kdim + 7) / 8) * 8 : kdim;
+  const int esz = bf16 ? 2 : 4;
+
+  // Column-major group flattening: stride of each mode inside its group.
+  auto group_strides = [&](const std::vector<int>& g, long long base, long long* st_of) {
+    long long p = base;
+    for (int m : g) { st_of[m] = p; p *= ext[m]; }
+  };
+  // Gather arguments: output modes listed outermost first (B, then M or N, then K).
+  auto make_gather = [&](const std::vector<int>& outer, const std::vector<int>& mid,
+                         const std::vector<int>& inner, const std::vector<int>& summed,
+                         const long long* src_stride, long long mid_n, long long pitch, GatherArgs* a) {
+    long long dst_of[MAXM] = {};
+    group_strides(inner, 1, dst_of);
+    group_strides(mid, pitch, dst_of);
+    group_strides(outer, pitch * mid_n, dst_of);
+    std::vector<int> order;  // outermost first; inside a group the last mode is outermost
+    for (int i = (int)outer.size() - 1; i >= 0; --i) order.push_back(outer[i]);
+    for (int i = (int)mid.size() - 1; i >= 0; --i) order.push_back(mid[i]);
+    for (int i = (int)inner.size() - 1; i >= 0; --i) order.push_back(inner[i]);
+    memset(a, 0, sizeof(*a));
+    a->rank_o = (int)order.size();
+    for (int d = 0; d < a->rank_o; ++d) {
+      a->odims[d] = ext[order[d]];
+      a->istride[d] = src_stride[order[d]];
+      a->ostride[d] = dst_of[order[d]];
+    }
+    a->rank_s = (int)summed.size();
+    for (int d = 0; d < a->rank_s; ++d) {
+      a->sdims[d] = ext[summed[d]];
+      a->sstride[d] = src_stride[summed[d]];
+    }
+  };
+  // Empty groups behave as extent 1 (prod() of nothing), so rank-0 pieces work.
+  GatherArgs ga, gb;
+  make_gather(gB, gI, gK, gL, strl, nm, pk, &ga);
+  make_gather(gB, gN, gK, gR, strr, nn, pk, &gb);
+  if (ga.rank_o == 0) { ga.rank_o = 1; ga.odims[0] = 1; }
+  if (gb.rank_o == 0) { gb.rank_o = 1; gb.odims[0] = 1; }
+
+  // Direct write when the output order is I..., N..., B...
+  bool direct = true;
+  int last = -1;
+  for (int d = 0; d < rank_o; ++d) {
+    int c = cls(modes_o[d]);
+    int rank_c = c == CI ? 0 : c == CN ? 1 : 2;
+    if (rank_c < last) direct = false;
+    last = rank_c;
+  }
+
+  void *Lc = nullptr, *Rc = nullptr;
+  float* Ct = nullptr;
+  cudaError_t e;
+  e = cudaMallocAsync(&Lc, (size_t)(nb * nm * pk * esz + 16), st);
+  if (e != cudaSuccess) return set_error(BBX_ERR_CUDA, "cudaMallocAsync: %s", cudaGetErrorString(e));
+  e = cudaMallocAsync(&Rc, (size_t)(nb * nn * pk * esz + 16), st);
+  if (e != cudaSuccess) { cudaFreeAsync(Lc, st); return set_error(BBX_ERR_CUDA, "cudaMallocAsync: %s", cudaGetErrorString(e)); }
+  if (!direct) {
+    e = cudaMallocAsync((void**)&Ct, (size_t)(nb * nn * nm * 4), st);
+    if (e != cudaSuccess) { cudaFreeAsync(Lc, st); cudaFreeAsync(Rc, st); return set_error(BBX_ERR_CUDA, "cudaMallocAsync: %s", cudaGetErrorString(e)); }
+  }
+  float* C = direct ? out : Ct;
+  int rc = BBX_OK;
+  const long long nl = nb * nm * kdim, nr = nb * nn * kdim;
+  if (bf16) {
+    rc = launch_gather<__nv_bfloat16>(lhs, (__nv_bfloat16*)Lc, ga, nl, st);
+    if (!rc) rc = launch_gather<__nv_bfloat16>(rhs, (__nv_bfloat16*)Rc, gb, nr, st);
+  } else {
+    rc = launch_gather<float>(lhs, (float*)Lc, ga, nl, st);
+    if (!rc) rc = launch_gather<float>(rhs, (float*)Rc, gb, nr, st);
+  }
+  if (!rc) {
+    const long long pitch = pk;
+    if (!bf16) {
+      rc = bbx_matmul_f32((const float*)Rc, (const float*)Lc, C, (int)nn, (int)nm, (int)kdim, pitch,
+                          pitch, nm, 0, 1, alpha, 0.f, nullptr, 0, (int)nb, nn * pitch, nm * pitch,
+                          nn * nm, stream);
+    } else {
+      std::vector<bbx_tc_problem_t> probs((size_t)nb);
+      for (long long b = 0; b < nb; ++b) {
+        bbx_tc_problem_t& q = probs[(size_t)b];
+        memset(&q, 0, sizeof(q));
+        q.a = (const __nv_bfloat16*)Rc + b * nn * pitch;
+        q.b = (const __nv_bfloat16*)Lc + b * nm * pitch;
+        q.c = C + b * nn * nm;
+        q.m = (int)nn; q.n = (int)nm; q.k = (int)kdim;
+        q.trans_a = 0; q.trans_b = 1;
+        q.lda = pitch; q.ldb = pitch; q.ldc = nm;
+        q.alpha = alpha; q.beta = 0.f;
+      }
+      rc = bbx_matmul_tc(BBX_BF16, probs.data(), (int)nb, 0, stream);
+    }
+  }
+  if (!rc && !direct) {
+    // Ct[b][n][m] -> column-major output in modes_o order.
+    long long src_of[MAXM] = {};
+    group_strides(gI, 1, src_of);
+    group_strides(gN, nm, src_of);
+    group_strides(gB, nm * nn, src_of);
+    GatherArgs go;
+    memset(&go, 0, sizeof(go));
+    long long p = 1, ostr[MAXM] = {};
+    for (int d = 0; d < rank_o; ++d) { ostr[modes_o[d]] = p; p *= ext[modes_o[d]]; }
+    go.rank_o = rank_o;
+    for (int d = 0; d < rank_o; ++d) {
+      int m = modes_o[rank_o - 1 - d];
+      go.odims[d] = ext[m];
+      go.istride[d] = src_of[m];
+      go.ostride[d] = ostr[m];
+    }
+    rc = launch_gather<float>(Ct, out, go, p, st);
+  }
+  cudaFreeAsync(Lc, st);
+  cudaFreeAsync(Rc, st);
+  if (Ct) cudaFreeAsync(Ct, st);
+  return rc;
+}

@@ -1,0 +1,331 @@
+// Block matmul on the 5th-generation tensor cores (tcgen05) for sm_100a.
+//
+// One persistent kernel computes a *group* of independent block products
+//     C_p = alpha_p * op(A_p) * op(B_p) (+ beta_p * C_p) (+ bias_p) (relu)
+// for p = 0..P-1. This is the device side of the reference's block matmul ud
+// (src/ud_functions/impls/dense_matrix_mult.cc:50-86: row-major C = op(A)op(B)
+// with the transpose flags taken from params b0/b1) and of the FNN matmuls
+// (applications/fnn/ffnn_activation_mult.cc:56-96 adds a column bias;
+// ffnn_back_mult.cc:52-91 is the trans_a case).
+//
+// Layout: A_p is M x K (or K x M when trans_a), B_p is K x N (or N x K when
+// trans_b), all row-major with arbitrary pitches that are multiples of 16 bytes.
+// Operands whose K dimension is contiguous ("K-major") and operands whose M/N
+// dimension is contiguous ("MN-major") are both read directly by TMA with the
+// 128-byte swizzle; no transpose pass is needed.
+//
+// Roles inside a 192-thread CTA:
+//   warp 0      TMA producer (one elected lane) feeding a STAGES-deep smem ring
+//   warp 1      TMEM allocator + MMA issuer (one elected lane)
+//   warps 2..5  epilogue: tcgen05.ld from TMEM -> registers -> global
+// The accumulator is double buffered in TMEM (2 x BN f32 columns), so the
+// epilogue of tile t overlaps the main loop of tile t+1.
+#pragma once
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+#include "ptx.cuh"
+
+namespace bbx {
+
+enum : int {
+  EPI_RELU = 1,      // max(x, 0) after bias
+  EPI_OUT_BF16 = 2,  // store bf16 instead of f32
+  EPI_BIAS = 4,      // add bias[col]
+  EPI_BETA = 8,      // read C and add beta * C
+};
+
+// One block product. 64-byte alignment is required by the tensor maps.
+struct alignas(64) TcProblem {
+  CUtensorMap tmap_a;  // 128 B
+  CUtensorMap tmap_b;  // 128 B
+  void* c;
+  const float* bias;
+  long long ldc;       // elements
+  int m, n, k;
+  int tile_start;      // first global tile index of this problem
+  int tiles_m, tiles_n;
+  float alpha, beta;
+  int flags;
+  int pad_;
+};
+
+constexpr int kTcMaxInline = 4;
+
+struct TcArgs {
+  const TcProblem* table;  // device table, or nullptr to use `inline_probs`
+  int num_problems;
+  int total_tiles;
+  uint32_t* status;        // device status word (0 = ok)
+  TcProblem inline_probs[kTcMaxInline];
+};
+
+template <int BN, bool A_MN, bool B_MN, bool FP8>
+struct TcCfg {
+  static constexpr int BM = 128;
+  static constexpr int BK_BYTES = 128;                // one 128-byte swizzle row of K
+  static constexpr int ELEM = FP8 ? 1 : 2;
+  static constexpr int BK = BK_BYTES / ELEM;          // 64 bf16 or 128 e4m3
+  static constexpr int UMMA_K = FP8 ? 32 : 16;
+  static constexpr int A_BYTES = BM * BK_BYTES;       // 16 KiB
+  static constexpr int B_BYTES = BN * BK_BYTES;       // 32 or 16 KiB
+  static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+  static constexpr int STAGES = (BN == 256) ? 4 : 6;
+  static constexpr int TMEM_COLS = 2 * BN;            // double-buffered accumulator
+  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align slack*/ + 256 /*bars*/;
+  static constexpr int THREADS = 192;
+  static constexpr int MN_BOX = 128 / ELEM;           // MN-major TMA box width (elements)
+};
+
+__device__ __forceinline__ const TcProblem* tc_problem(const TcArgs& args, int p) {
+  return args.table ? (args.table + p) : (args.inline_probs + p);
+}
+
+// Map a global tile index to (problem, tile_m, tile_n). Tiles inside a problem
+// are visited in groups of 8 tile-rows so concurrently running CTAs share
+// operand tiles in L2.
+__device__ __forceinline__ void tc_locate(const TcArgs& args, int t, int& p, int& tm, int& tn) {
+  int lo = 0, hi = args.num_problems - 1;
+  while (lo < hi) {  // last problem with tile_start <= t
+    int mid = (lo + hi + 1) >> 1;
+    if (tc_problem(args, mid)->tile_start <= t) lo = mid; else hi = mid - 1;
+  }
+  p = lo;
+  const TcProblem* pr = tc_problem(args, p);
+  int lt = t - pr->tile_start;
+  constexpr int G = 8;
+  int per_group = G * pr->tiles_n;
+  int group = lt / per_group;
+  int first_m = group * G;
+  int gsize = min(pr->tiles_m - first_m, G);
+  int r = lt - group * per_group;
+  tm = first_m + r % gsize;
+  tn = r / gsize;
+}
+
+template <int BN, bool A_MN, bool B_MN, bool FP8>
+__global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__ TcArgs args) {
+  using C = TcCfg<BN, A_MN, B_MN, FP8>;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  // 1024-byte alignment for the 128B-swizzle atoms.
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t* stage_base = smem;
+  uint64_t* bars = (uint64_t*)(smem + C::STAGES * C::STAGE_BYTES);
+  uint64_t* full_bar = bars;                       // [STAGES]
+  uint64_t* empty_bar = bars + C::STAGES;          // [STAGES]
+  uint64_t* tfull_bar = bars + 2 * C::STAGES;      // [2]
+  uint64_t* tempty_bar = bars + 2 * C::STAGES + 2; // [2]
+  uint32_t* tmem_slot = (uint32_t*)(bars + 2 * C::STAGES + 4);
+  volatile uint32_t* status = args.status;
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < C::STAGES; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull_bar[b], 1);
+      mbar_init(&tempty_bar[b], 128);
+    }
+    fence_mbar_init();
+  }
+  if (warp == 1) tmem_alloc(tmem_slot, C::TMEM_COLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < args.total_tiles && ok; t += gridDim.x) {
+        int p, tm, tn;
+        tc_locate(args, t, p, tm, tn);
+        const TcProblem* pr = tc_problem(args, p);
+        const int kb_n = (pr->k + C::BK - 1) / C::BK;
+        for (int kb = 0; kb < kb_n; ++kb) {
+          if (!mbar_wait(&empty_bar[s], ph ^ 1, status, DEV_TIMEOUT_EMPTY)) { ok = false; break; }
+          uint8_t* sa = stage_base + s * C::STAGE_BYTES;
+          uint8_t* sb = sa + C::A_BYTES;
+          mbar_arrive_expect_tx(&full_bar[s], C::STAGE_BYTES);
+          const int k0 = kb * C::BK;
+          if constexpr (!A_MN) {
+            tma_load_2d(sa, &pr->tmap_a, &full_bar[s], k0, tm * C::BM);
+          } else {
+#pragma unroll
+            for (int j = 0; j < C::BM / C::MN_BOX; ++j)
+              tma_load_2d(sa + j * (C::BK * 128), &pr->tmap_a, &full_bar[s],
+                          tm * C::BM + j * C::MN_BOX, k0);
+          }
+          if constexpr (!B_MN) {
+            tma_load_2d(sb, &pr->tmap_b, &full_bar[s], k0, tn * BN);
+          } else {
+#pragma unroll
+            for (int j = 0; j < BN / C::MN_BOX; ++j)
+              tma_load_2d(sb + j * (C::BK * 128), &pr->tmap_b, &full_bar[s],
+                          tn * BN + j * C::MN_BOX, k0);
+          }
+          if (++s == C::STAGES) { s = 0; ph ^= 1; }
+        }
+      }
+      // Drain: make sure every issued TMA has landed before the CTA may exit.
+      for (int i = 0; i < C::STAGES; ++i) {
+        if (!mbar_wait(&empty_bar[s], ph ^ 1, status, DEV_TIMEOUT_EMPTY)) break;
+        if (++s == C::STAGES) { s = 0; ph ^= 1; }
+      }
+      if (*status != DEV_OK) {
+        // Error path: the consumer stopped early, so give copies still in
+        // flight a bounded grace period (~100 us) before the CTA exits.
+        const long long t0 = clock64();
+        while (clock64() - t0 < 200000) {}
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      constexpr uint32_t kFmt = FP8 ? 0u : 1u;  // e4m3 / bf16
+      constexpr uint32_t idesc = make_idesc(C::BM, BN, kFmt, A_MN, B_MN);
+      int s = 0;
+      uint32_t ph = 0;
+      int acc = 0;
+      uint32_t acc_ph = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < args.total_tiles && ok; t += gridDim.x) {
+        int p, tm, tn;
+        tc_locate(args, t, p, tm, tn);
+        const TcProblem* pr = tc_problem(args, p);
+        const int kb_n = (pr->k + C::BK - 1) / C::BK;
+        if (!mbar_wait(&tempty_bar[acc], acc_ph ^ 1, status, DEV_TIMEOUT_TMEM_EMPTY)) break;
+        tc_fence_after();
+        const uint32_t d_tmem = tmem_base + acc * BN;
+        for (int kb = 0; kb < kb_n; ++kb) {
+          if (!mbar_wait(&full_bar[s], ph, status, DEV_TIMEOUT_FULL)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t sa = smem_u32(stage_base + s * C::STAGE_BYTES);
+          const uint32_t sb = sa + C::A_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < C::BK / C::UMMA_K; ++kk) {
+            uint64_t da, db;
+            if constexpr (!A_MN) da = smem_desc_sw128(sa + kk * 32, 16, 1024);
+            else da = smem_desc_sw128(sa + kk * (C::UMMA_K * 128), C::BK * 128, 1024);
+            if constexpr (!B_MN) db = smem_desc_sw128(sb + kk * 32, 16, 1024);
+            else db = smem_desc_sw128(sb + kk * (C::UMMA_K * 128), C::BK * 128, 1024);
+            const uint32_t accum = (kb > 0 || kk > 0) ? 1u : 0u;
+            if constexpr (FP8) umma_f8(d_tmem, da, db, idesc, accum);
+            else umma_f16(d_tmem, da, db, idesc, accum);
+          }
+          umma_commit(&empty_bar[s]);  // frees the stage once these MMAs retire
+          if (++s == C::STAGES) { s = 0; ph ^= 1; }
+        }
+        if (!ok) break;
+        umma_commit(&tfull_bar[acc]);  // accumulator ready for the epilogue
+        if (++acc == 2) { acc = 0; acc_ph ^= 1; }
+      }
+    }
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int lane_base = 32 * (warp & 3);
+    int acc = 0;
+    uint32_t acc_ph = 0;
+    for (int t = blockIdx.x; t < args.total_tiles; t += gridDim.x) {
+      int p, tm, tn;
+      tc_locate(args, t, p, tm, tn);
+      const TcProblem* pr = tc_problem(args, p);
+      // Warp-uniform outcome: tcgen05.ld below is warp-collective.
+      const bool got = mbar_wait(&tfull_bar[acc], acc_ph, status, DEV_TIMEOUT_TMEM_FULL);
+      if (!__all_sync(0xffffffffu, got)) break;
+      tc_fence_after();
+      const int row = tm * C::BM + lane_base + lane;
+      const bool row_ok = row < pr->m;
+      const int flags = pr->flags;
+      const float alpha = pr->alpha, beta = pr->beta;
+      const long long ldc = pr->ldc;
+      const int n = pr->n;
+      const uint32_t t_row = tmem_base + acc * BN + ((uint32_t)lane_base << 16);
+      for (int c = 0; c < BN / 16; ++c) {
+        const int col0 = tn * BN + c * 16;
+        if (col0 >= n) break;  // warp-uniform
+        float v[16];
+        tmem_ld16(t_row + c * 16, v);
+        if (!row_ok) continue;
+        const bool full = (col0 + 16 <= n);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          float x = v[i] * alpha;
+          if ((flags & EPI_BIAS) && (full || col0 + i < n)) x += pr->bias[col0 + i];
+          v[i] = x;
+        }
+        if (flags & EPI_OUT_BF16) {
+          __nv_bfloat16* cp = (__nv_bfloat16*)pr->c + (long long)row * ldc + col0;
+          if (flags & EPI_BETA) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+              if (full || col0 + i < n) v[i] += beta * __bfloat162float(cp[i]);
+          }
+          if (flags & EPI_RELU) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i], 0.f);
+          }
+          if (full && ((((uintptr_t)cp) & 15) == 0)) {
+            uint4 pk[2];
+            __nv_bfloat162* h = (__nv_bfloat162*)pk;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) h[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+            ((uint4*)cp)[0] = pk[0];
+            ((uint4*)cp)[1] = pk[1];
+          } else {
+            for (int i = 0; i < 16; ++i)
+              if (col0 + i < n) cp[i] = __float2bfloat16_rn(v[i]);
+          }
+        } else {
+          float* cp = (float*)pr->c + (long long)row * ldc + col0;
+          const bool vec = full && ((((uintptr_t)cp) & 15) == 0);
+          if (flags & EPI_BETA) {
+            if (vec) {
+#pragma unroll
+              for (int q = 0; q < 4; ++q) {
+                float4 o = ((const float4*)cp)[q];
+                v[4 * q + 0] += beta * o.x; v[4 * q + 1] += beta * o.y;
+                v[4 * q + 2] += beta * o.z; v[4 * q + 3] += beta * o.w;
+              }
+            } else {
+              for (int i = 0; i < 16; ++i)
+                if (col0 + i < n) v[i] += beta * cp[i];
+            }
+          }
+          if (flags & EPI_RELU) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i], 0.f);
+          }
+          if (vec) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              ((float4*)cp)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+          } else {
+            for (int i = 0; i < 16; ++i)
+              if (col0 + i < n) cp[i] = v[i];
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&tempty_bar[acc]);
+      if (++acc == 2) { acc = 0; acc_ph ^= 1; }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem_base, C::TMEM_COLS);
+  }
+}
+
+}  // namespace bbx

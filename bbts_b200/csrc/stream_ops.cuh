@@ -1,0 +1,357 @@
+// HBM-streaming block kernels: add, n-ary reduce, elementwise, bias and
+// column sums, casts / FP8 quantisation, softmax cross-entropy, Philox fill,
+// and the rank<=4 permutation used by the contraction.
+//
+// All of them are grid-stride loops sized to a multiple of the SM count, use
+// 128-bit loads/stores when the pointers allow it, and are bit-exact against
+// the reference's CPU loops where the reference fixes the order of operations
+// (add, left-fold reduce, relu, relu', hadamard, weighted sum, column sum).
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+#include <cstdint>
+
+namespace bbx {
+
+enum UnaryOp : int {
+  U_RELU = 0,        // dense_matrix_relu.cc:63-69
+  U_RELU_DIF = 1,    // dense_matrix_relu_dif.cc:63-69 (1 if > 0 else 0)
+  U_SIGMOID_REF = 2, // dense_matrix_sigmoid.cc:64-70: 1/(1+exp(v)) as the reference computes it
+  U_SIGMOID = 3,     // 1/(1+exp(-v)), cutensor ew uop 0 (libraries/cutensor/ew.h:158-161)
+  U_EXP = 4,
+  U_SQUARE = 5,
+  U_SQRT = 6,
+  U_ADD_SCALAR = 7,  // v + param
+  U_SCALE = 8,       // v * param
+};
+
+enum BinaryOp : int {
+  B_ADD = 0,          // dense_matrix_add.cc:67-73
+  B_WEIGHTED = 1,     // dense_matrix_weighted_sum.cc:70-76: ca*a + cb*b
+  B_HADAMARD = 2,     // dense_matrix_hadamard.cc:67-73
+  B_MAX = 3,
+  B_MIN = 4,
+  B_SUB = 5,
+  B_DIV = 6,
+};
+
+constexpr int kMaxReduceInputs = 32;
+
+struct ReduceArgs {
+  const float* in[kMaxReduceInputs];
+};
+
+// ------------------------------------------------------------------ helpers
+__device__ __forceinline__ float apply_unary(int op, float v, float p) {
+  switch (op) {
+    case U_RELU: return v > 0.f ? v : 0.f;
+    case U_RELU_DIF: return v > 0.f ? 1.f : 0.f;
+    case U_SIGMOID_REF: return __fdiv_rn(1.f, __fadd_rn(1.f, expf(v)));
+    case U_SIGMOID: return __fdiv_rn(1.f, __fadd_rn(1.f, expf(-v)));
+    case U_EXP: return expf(v);
+    case U_SQUARE: return __fmul_rn(v, v);
+    case U_SQRT: return sqrtf(v);
+    case U_ADD_SCALAR: return __fadd_rn(v, p);
+    case U_SCALE: return __fmul_rn(v, p);
+  }
+  return v;
+}
+
+__device__ __forceinline__ float apply_binary(int op, float a, float b, float ca, float cb) {
+  switch (op) {
+    case B_ADD: return __fadd_rn(a, b);
+    case B_WEIGHTED: return __fadd_rn(__fmul_rn(ca, a), __fmul_rn(cb, b));
+    case B_HADAMARD: return __fmul_rn(a, b);
+    case B_MAX: return a > b ? a : b;
+    case B_MIN: return a < b ? a : b;
+    case B_SUB: return __fsub_rn(a, b);
+    case B_DIV: return __fdiv_rn(a, b);
+  }
+  return a;
+}
+
+// ------------------------------------------------------------------ kernels
+__global__ void k_unary(int op, const float* __restrict__ in, float* out, long long n, float p) {
+  long long i4 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const bool vec = ((((uintptr_t)in) | ((uintptr_t)out)) & 15) == 0;
+  if (vec) {
+    const long long n4 = n >> 2;
+    for (long long i = i4; i < n4; i += stride) {
+      float4 v = ((const float4*)in)[i];
+      v.x = apply_unary(op, v.x, p); v.y = apply_unary(op, v.y, p);
+      v.z = apply_unary(op, v.z, p); v.w = apply_unary(op, v.w, p);
+      ((float4*)out)[i] = v;
+    }
+    for (long long i = (n4 << 2) + i4; i < n; i += stride) out[i] = apply_unary(op, in[i], p);
+  } else {
+    for (long long i = i4; i < n; i += stride) out[i] = apply_unary(op, in[i], p);
+  }
+}
+
+__global__ void k_binary(int op, const float* a, const float* b, float* c, long long n, float ca,
+                         float cb) {
+  long long i4 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const bool vec = ((((uintptr_t)a) | ((uintptr_t)b) | ((uintptr_t)c)) & 15) == 0;
+  if (vec) {
+    const long long n4 = n >> 2;
+    for (long long i = i4; i < n4; i += stride) {
+      float4 x = ((const float4*)a)[i];
+      float4 y = ((const float4*)b)[i];
+      float4 z;
+      z.x = apply_binary(op, x.x, y.x, ca, cb); z.y = apply_binary(op, x.y, y.y, ca, cb);
+      z.z = apply_binary(op, x.z, y.z, ca, cb); z.w = apply_binary(op, x.w, y.w, ca, cb);
+      ((float4*)c)[i] = z;
+    }
+    for (long long i = (n4 << 2) + i4; i < n; i += stride) c[i] = apply_binary(op, a[i], b[i], ca, cb);
+  } else {
+    for (long long i = i4; i < n; i += stride) c[i] = apply_binary(op, a[i], b[i], ca, cb);
+  }
+}
+
+// out = in[0] + in[1] + ... + in[n_in-1], left to right (the order of the
+// reference's local reduce, src/operations/local_reduce_op.cc:23-91). With
+// kahan != 0 the running sum carries a Kahan compensation term; with kahan == 0
+// the result is bit-identical to the reference's pairwise left fold.
+// `out` may alias in[0] (the reference marks matrix_add inputs in-place, {0,1}).
+template <bool KAHAN>
+__global__ void k_reduce(const __grid_constant__ ReduceArgs args, int n_in, float* out,
+                         long long n) {
+  long long i4 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  bool vec = (((uintptr_t)out) & 15) == 0;
+  for (int j = 0; j < n_in; ++j) vec = vec && ((((uintptr_t)args.in[j]) & 15) == 0);
+  const long long n4 = vec ? (n >> 2) : 0;
+  for (long long i = i4; i < n4; i += stride) {
+    float4 s = ((const float4*)args.in[0])[i];
+    float4 comp = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int j = 1; j < n_in; ++j) {
+      float4 x = ((const float4*)args.in[j])[i];
+      if (KAHAN) {
+        float y, t;
+        y = __fsub_rn(x.x, comp.x); t = __fadd_rn(s.x, y); comp.x = __fsub_rn(__fsub_rn(t, s.x), y); s.x = t;
+        y = __fsub_rn(x.y, comp.y); t = __fadd_rn(s.y, y); comp.y = __fsub_rn(__fsub_rn(t, s.y), y); s.y = t;
+        y = __fsub_rn(x.z, comp.z); t = __fadd_rn(s.z, y); comp.z = __fsub_rn(__fsub_rn(t, s.z), y); s.z = t;
+        y = __fsub_rn(x.w, comp.w); t = __fadd_rn(s.w, y); comp.w = __fsub_rn(__fsub_rn(t, s.w), y); s.w = t;
+      } else {
+        s.x = __fadd_rn(s.x, x.x); s.y = __fadd_rn(s.y, x.y);
+        s.z = __fadd_rn(s.z, x.z); s.w = __fadd_rn(s.w, x.w);
+      }
+    }
+    ((float4*)out)[i] = s;
+  }
+  for (long long i = (n4 << 2) + i4; i < n; i += stride) {
+    float s = args.in[0][i], comp = 0.f;
+    for (int j = 1; j < n_in; ++j) {
+      float x = args.in[j][i];
+      if (KAHAN) {
+        float y = __fsub_rn(x, comp);
+        float t = __fadd_rn(s, y);
+        comp = __fsub_rn(__fsub_rn(t, s), y);
+        s = t;
+      } else {
+        s = __fadd_rn(s, x);
+      }
+    }
+    out[i] = s;
+  }
+}
+
+// out[r][c] = in[r][c] + bias[c]   (ffnn_activation_mult.cc:88-94)
+__global__ void k_bias_add(const float* in, const float* __restrict__ bias, float* out, int rows,
+                           int cols, int relu) {
+  const long long n = (long long)rows * cols;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    float v = __fadd_rn(in[i], bias[i % cols]);
+    out[i] = (relu && v < 0.f) ? 0.f : v;
+  }
+}
+
+// out[c] = (accumulate ? out[c] : 0) + sum_r in[r][c], rows summed in order
+// (ffnn_back_mult.cc:86-90 sums rows 0..R-1 into the bias). One thread per
+// column; consecutive threads read consecutive columns so each row read is
+// coalesced; the row loop is unrolled to keep many loads in flight.
+__global__ void k_colsum(const float* __restrict__ in, float* out, int rows, int cols, long long ld,
+                         int accumulate) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cols) return;
+  float s = accumulate ? out[c] : 0.f;
+  int r = 0;
+  for (; r + 8 <= rows; r += 8) {
+    float v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = in[(long long)(r + u) * ld + c];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) s = __fadd_rn(s, v[u]);
+  }
+  for (; r < rows; ++r) s = __fadd_rn(s, in[(long long)r * ld + c]);
+  out[c] = s;
+}
+
+__global__ void k_f32_to_bf16(const float* __restrict__ in, __nv_bfloat16* out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = __float2bfloat16_rn(in[i]);
+}
+
+__global__ void k_bf16_to_f32(const __nv_bfloat16* __restrict__ in, float* out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = __bfloat162float(in[i]);
+}
+
+// Block absmax into *amax (float bits compared as integers; values are >= 0).
+template <typename T>
+__global__ void k_absmax(const T* __restrict__ in, long long n, unsigned int* amax) {
+  float m = 0.f;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    float v;
+    if constexpr (sizeof(T) == 4) v = in[i]; else v = __bfloat162float(in[i]);
+    m = fmaxf(m, fabsf(v));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(amax, __float_as_uint(m));
+}
+
+// q = e4m3(x * 448 / amax); *scale_out = amax / 448 (the dequantisation factor).
+// With transpose != 0 the rows x cols input is written as cols x rows, which
+// turns an MN-major operand into the K-major layout the FP8 MMA reads.
+template <typename T>
+__global__ void k_quant_e4m3(const T* __restrict__ in, __nv_fp8_e4m3* out, int rows, int cols,
+                             const unsigned int* amax, float* scale_out, int transpose) {
+  const float a = __uint_as_float(*amax);
+  const float s = a > 0.f ? 448.f / a : 1.f;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *scale_out = a > 0.f ? a / 448.f : 1.f;
+  const long long n = (long long)rows * cols;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    float v;
+    if constexpr (sizeof(T) == 4) v = in[i]; else v = __bfloat162float(in[i]);
+    long long o = i;
+    if (transpose) {
+      long long r = i / cols, c = i % cols;
+      o = c * rows + r;
+    }
+    out[o] = __nv_fp8_e4m3(v * s);
+  }
+}
+
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy
+// as 1, 2, 3", SC 2011). Counter = (i, 0, 0, 0) for output word group i,
+// key = (seed_lo, seed_hi).
+__host__ __device__ inline void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+  for (int r = 0; r < 10; ++r) {
+    uint64_t p0 = (uint64_t)M0 * c[0];
+    uint64_t p1 = (uint64_t)M1 * c[2];
+    uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+    uint32_t n0 = hi1 ^ c[1] ^ k0, n1 = lo1, n2 = hi0 ^ c[3] ^ k1, n3 = lo0;
+    c[0] = n0; c[1] = n1; c[2] = n2; c[3] = n3;
+    k0 += W0; k1 += W1;
+  }
+}
+
+// Uniform in [lo, hi) from the top 24 bits of each Philox word; normal via
+// Box-Muller on word pairs. dist: 0 uniform, 1 normal(mean=lo, std=hi).
+template <typename T>
+__global__ void k_fill_philox(T* out, long long n, unsigned long long seed, int dist, float lo,
+                              float hi) {
+  const long long groups = (n + 3) / 4;
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < groups;
+       g += (long long)gridDim.x * blockDim.x) {
+    uint32_t c[4] = {(uint32_t)g, (uint32_t)(g >> 32), 0u, 0u};
+    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    float v[4];
+    if (dist == 0) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) v[j] = __fmaf_rn(hi - lo, (float)(c[j] >> 8) * (1.0f / 16777216.0f), lo);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; j += 2) {
+        float u1 = ((c[j] >> 8) + 1) * (1.0f / 16777217.0f);
+        float u2 = (c[j + 1] >> 8) * (1.0f / 16777216.0f);
+        float r = sqrtf(-2.f * logf(u1));
+        float sn, cs;
+        sincospif(2.f * u2, &sn, &cs);
+        v[j] = lo + hi * r * cs;
+        v[j + 1] = lo + hi * r * sn;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      long long i = g * 4 + j;
+      if (i < n) {
+        if constexpr (sizeof(T) == 4) out[i] = v[j];
+        else out[i] = __float2bfloat16_rn(v[j]);
+      }
+    }
+  }
+}
+
+// Softmax cross-entropy over rows of `logits` (rows x cols, pitch ld) against
+// integer labels. Writes the per-row loss and, if grad != nullptr, the
+// gradient (softmax - onehot) * grad_scale in the same layout. One warp per row.
+__global__ void k_softmax_ce(const float* __restrict__ logits, const int* __restrict__ labels,
+                             float* loss, float* grad, int rows, int cols, long long ld,
+                             float grad_scale) {
+  const int warps_per_block = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31;
+  for (int r = blockIdx.x * warps_per_block + (threadIdx.x >> 5); r < rows;
+       r += gridDim.x * warps_per_block) {
+    const float* z = logits + (long long)r * ld;
+    float mx = -INFINITY;
+    for (int c = lane; c < cols; c += 32) mx = fmaxf(mx, z[c]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    float se = 0.f;
+    for (int c = lane; c < cols; c += 32) se += expf(z[c] - mx);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) se += __shfl_xor_sync(0xffffffffu, se, o);
+    const int y = labels[r];
+    const float lse = mx + logf(se);
+    if (lane == 0) loss[r] = lse - z[y];
+    if (grad) {
+      float* g = grad + (long long)r * ld;
+      const float inv = 1.f / se;
+      for (int c = lane; c < cols; c += 32) {
+        float p = expf(z[c] - mx) * inv;
+        g[c] = (p - (c == y ? 1.f : 0.f)) * grad_scale;
+      }
+    }
+  }
+}
+
+// out[e] for e over the output dims: general rank<=4 gather with optional
+// f32 -> bf16 cast. `ostride[d]` is the output stride of output dim d and
+// `istride[d]` the input stride of the input dim that feeds output dim d;
+// `odims` are the output extents (row-major flattening of the output index).
+struct PermArgs {
+  int rank;
+  long long odims[4];
+  long long ostride[4];
+  long long istride[4];
+};
+
+template <typename TO>
+__global__ void k_permute(const float* __restrict__ in, TO* out, const __grid_constant__ PermArgs a,
+                          long long n) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    long long rem = e, src = 0, dst = 0;
+    for (int d = a.rank - 1; d >= 0; --d) {
+      long long idx = rem % a.odims[d];
+      rem /= a.odims[d];
+      src += idx * a.istride[d];
+      dst += idx * a.ostride[d];
+    }
+    if constexpr (sizeof(TO) == 4) out[dst] = in[src];
+    else out[dst] = __float2bfloat16_rn(in[src]);
+  }
+}
+
+}  // namespace bbx

@@ -1,0 +1,302 @@
+"""Block-op DAG throughput on one B200 (or N independent replicas).
+
+Workload (cross-product blocked matmul): C = A.B with A 32768x4096 and B
+4096x32768 split into 4096x4096 blocks (8x1 and 1x8 grids), entries U(-1,1),
+BF16 inputs, FP32 accumulation and FP32 output: 64 independent matrix_mult
+block ops, 2*32768^2*4096 = 8.796 TFLOP per step. A step runs the whole DAG
+(all 64 block products) as ONE grouped persistent tcgen05 launch.
+
+Reported (one JSON line on rank 0):
+  value       TFLOP/s of the grouped tensor-core path, inputs resident in HBM
+  e2e         the same through the C ABI with pinned HOST blocks: H2D of the
+              16 input blocks + the launch + D2H of the 64 output blocks
+  plain_fp32  the plain FP32 per-op path (one SIMT launch per block op)
+  roofline    dominant kernel vs the measured bf16 tensor peak
+  cpu_baseline  the CPU restatement of the reference's SGEMM on host cores
+`--impl reference` times the reference's CPU block matmul (the oracle port) instead.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+GRID = 8            # 8 row blocks of A, 8 column blocks of B
+BS = 4096           # block edge
+FLOP_PER_STEP = 2.0 * (GRID * BS) ** 2 * BS
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--tile-n", type=int, default=0)
+    p.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparator leg")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    return p.parse_args()
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return d["hbm_gbs"], d["bf16_tflops"], d.get("bf16_tflops_sustained"), "measured"
+    return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit())
+        mx = max(float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = [n for i, n in enumerate(names) if any(s[3 + i] == "Active" for s in self.samples)]
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def cpu_sample_tflops(threads):
+    """One 4096x4096 output block with K=4096 (137 GFLOP) through the oracle's
+    blocked FP32 SGEMM, the CPU restatement of dense_matrix_mult (one block op)."""
+    import numpy as np
+    import oracle
+    rng = np.random.default_rng(0)
+    a = rng.uniform(-1, 1, (BS, BS)).astype(np.float32)
+    b = rng.uniform(-1, 1, (BS, BS)).astype(np.float32)
+    t0 = time.perf_counter()
+    oracle.sgemm(a, b, threads=threads)
+    dt = time.perf_counter() - t0
+    return 2.0 * BS ** 3 / dt / 1e12, dt
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        pass  # the CPU path has no warm-up state beyond the first call
+    vals, ts = [], []
+    for _ in range(args.steps):
+        v, dt = cpu_sample_tflops(threads)
+        vals.append(v)
+        ts.append(dt)
+    v = sum(vals) / len(vals)
+    line = {"impl": "reference", "metric": "block-op DAG TFLOP/s (cross-product blocked matmul)",
+            "value": round(v, 5), "unit": "TFLOP/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1000 * FLOP_PER_STEP / (v * 1e12), 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic U(-1,1), seeded",
+            "config": {"workload": "cpmm 32768x4096 . 4096x32768 in 4096^2 blocks (64 matrix_mult ops)",
+                       "sample": "1 of 64 block products per step (4096^3), extrapolated per step"},
+            "cpu_baseline": {"value": round(v, 5), "unit": "TFLOP/s", "cores": threads, "kind": "port",
+                             "sample": "one 4096^3 FP32 block matmul per step (oracle blocked SGEMM)"},
+            "e2e": {"value": round(v, 5), "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+    import bbts_b200
+    from bbts_b200 import ops
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+
+    # ---------------- inputs: 8 A blocks + 8 B blocks (BF16), 64 C blocks (FP32)
+    A = [torch.empty(BS, BS, dtype=torch.bfloat16, device=dev) for _ in range(GRID)]
+    B = [torch.empty(BS, BS, dtype=torch.bfloat16, device=dev) for _ in range(GRID)]
+    for i in range(GRID):
+        ops.fill_philox(A[i], seed=1000 + i + 100 * rank, dist=0, a=-1.0, b=1.0)
+        ops.fill_philox(B[i], seed=2000 + i + 100 * rank, dist=0, a=-1.0, b=1.0)
+    Cblk = [torch.empty(BS, BS, dtype=torch.float32, device=dev) for _ in range(GRID * GRID)]
+    probs = [ops.tc_problem(A[i], B[j], Cblk[i * GRID + j]) for i in range(GRID) for j in range(GRID)]
+    plan = ops.TcPlan(probs, tile_n=args.tile_n)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---------------- device-resident timing of the grouped tensor-core path
+    for _ in range(args.warmup):
+        plan.launch()
+    barrier()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    with ClockSampler(local) as clk:
+        ev[0].record(stream)
+        for s in range(args.steps):
+            plan.launch()
+            ev[s + 1].record(stream)
+        barrier()
+    step_ms = [ev[s].elapsed_time(ev[s + 1]) for s in range(args.steps)]
+    total_ms = ev[0].elapsed_time(ev[-1])
+    rc = bbts_b200.lib.bbx_check_device_status(None, None)
+    if rc != 0:
+        raise RuntimeError(bbts_b200.last_error())
+    t = torch.tensor([total_ms], device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    ms = total_ms / args.steps
+    value = world * FLOP_PER_STEP / (ms * 1e-3) / 1e12
+
+    # ---------------- roofline of the dominant kernel (the grouped tcgen05 launch)
+    hbm, bf16_peak, bf16_sust, src = load_peaks()
+    kern_ms = sum(step_ms) / len(step_ms)
+    achieved = FLOP_PER_STEP / (kern_ms * 1e-3) / 1e12
+    roofline = {"bound": "tensor", "achieved": round(achieved, 1), "peak": bf16_peak,
+                "unit": "TFLOP/s", "frac": round(achieved / bf16_peak, 4), "traffic": None,
+                "peak_source": src + " bf16 (burst)"}
+    prof = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(prof):
+        try:
+            roofline["traffic"] = json.load(open(prof)).get("tc_gemm_cpmm_bytes_per_launch")
+        except Exception:
+            pass
+
+    # ---------------- e2e through the C ABI with pinned host blocks
+    hA = [torch.empty(BS, BS, dtype=torch.bfloat16, pin_memory=True) for _ in range(GRID)]
+    hB = [torch.empty(BS, BS, dtype=torch.bfloat16, pin_memory=True) for _ in range(GRID)]
+    for i in range(GRID):
+        hA[i].copy_(A[i])
+        hB[i].copy_(B[i])
+    hC = [torch.empty(BS, BS, dtype=torch.float32, pin_memory=True) for _ in range(GRID * GRID)]
+    h2d = sum(x.numel() * x.element_size() for x in hA + hB)
+    d2h = sum(x.numel() * x.element_size() for x in hC)
+
+    def e2e_step():
+        for i in range(GRID):
+            A[i].copy_(hA[i], non_blocking=True)
+            B[i].copy_(hB[i], non_blocking=True)
+        plan.launch()
+        for i in range(GRID * GRID):
+            hC[i].copy_(Cblk[i], non_blocking=True)
+
+    e2e_steps = max(1, min(args.steps, 3))
+    e2e_step()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    barrier()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    t = torch.tensor([e2e_ms], device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t.item())
+    e2e_val = world * FLOP_PER_STEP / (e2e_ms * 1e-3) / 1e12
+
+    # ---------------- plain FP32 per-op path (the comparator): one SIMT launch per block op
+    plain = None
+    if not args.no_plain:
+        Af = [torch.empty(BS, BS, dtype=torch.float32, device=dev) for _ in range(GRID)]
+        Bf = [torch.empty(BS, BS, dtype=torch.float32, device=dev) for _ in range(GRID)]
+        for i in range(GRID):
+            ops.cast(A[i], Af[i])
+            ops.cast(B[i], Bf[i])
+
+        def plain_step():
+            for i in range(GRID):
+                for j in range(GRID):
+                    ops.matmul_f32(Af[i], Bf[j], Cblk[i * GRID + j])
+
+        plain_step()
+        barrier()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        plain_step()
+        p1.record(stream)
+        barrier()
+        pms = p0.elapsed_time(p1)
+        plain = {"value": round(world * FLOP_PER_STEP / (pms * 1e-3) / 1e12, 3), "unit": "TFLOP/s",
+                 "ms_per_step": round(pms, 2), "launches_per_step": GRID * GRID,
+                 "dtype": "f32", "speedup_of_value": round(value / (world * FLOP_PER_STEP / (pms * 1e-3) / 1e12), 2)}
+        del Af, Bf
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        v, dt = cpu_sample_tflops(threads)
+        cpu = {"value": round(v, 5), "unit": "TFLOP/s", "cores": threads, "kind": "port",
+               "sample": "one 4096^3 FP32 block matmul (1/64 of a step), oracle blocked SGEMM, %.1f s" % dt}
+
+    plan.close()
+    if rank == 0:
+        line = {"metric": "block-op DAG TFLOP/s (cross-product blocked matmul)", "value": round(value, 2),
+                "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "bf16",
+                "data": "synthetic U(-1,1) from a seeded Philox generator",
+                "config": {"workload": "cpmm 32768x4096 . 4096x32768 in 4096^2 blocks (64 matrix_mult ops), "
+                                       "bf16 in, f32 accumulate/out, one grouped launch per step",
+                           "parallelism": "replicas" if world > 1 else "single-gpu",
+                           "l2": "inputs+outputs (4.5 GiB) larger than L2"},
+                "e2e": {"value": round(e2e_val, 2), "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_ms, 2)},
+                "roofline": roofline, "plain_fp32": plain, "cpu_baseline": cpu,
+                "gpu_launches": args.steps, "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

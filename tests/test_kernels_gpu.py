@@ -1,0 +1,381 @@
+"""Parity of the CUDA block kernels (through the C ABI) against the CPU oracle."""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import golden, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def T(cuda):
+    import torch
+    from bbts_b200 import ops
+    return torch, ops
+
+
+def dev(torch, x, dtype=None):
+    t = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    return t.to(dtype) if dtype is not None else t
+
+
+def host(t):
+    import torch
+    torch.cuda.synchronize()
+    return t.float().cpu().numpy() if t.dtype != torch.float32 else t.cpu().numpy()
+
+
+def bf16_round(x):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(x, np.float32)).to(torch.bfloat16).float().numpy()
+
+
+# ----------------------------------------------------------------- add / reduce
+def test_add_known_answer(T):
+    torch, ops = T
+    g = golden("add_kat.npz")
+    a, b = dev(torch, g["a"]), dev(torch, g["b"])
+    ops.add(a, b, a)  # in place into input 0, as the reference test does
+    out = host(a)
+    assert np.max(np.abs(out - g["expect"])) <= 1e-4
+    assert np.array_equal(out, g["expect"])
+
+
+@pytest.mark.parametrize("n", [0, 1, 3, 1000, 1024 * 1024 + 5])
+def test_add_bit_exact(T, n):
+    torch, ops = T
+    rng = np.random.default_rng(n)
+    a = rng.standard_normal(n).astype(np.float32)
+    b = rng.standard_normal(n).astype(np.float32)
+    c = torch.empty(n, device="cuda")
+    ops.add(dev(torch, a), dev(torch, b), c)
+    assert np.array_equal(host(c), oracle.add(a, b))
+
+
+@pytest.mark.parametrize("n_in", [1, 2, 4, 16, 33, 70])
+def test_reduce_fold_bit_exact(T, n_in):
+    torch, ops = T
+    rng = np.random.default_rng(n_in)
+    ins = [rng.standard_normal(4099).astype(np.float32) for _ in range(n_in)]
+    out = torch.empty(4099, device="cuda")
+    ops.reduce([dev(torch, x) for x in ins], out, kahan=False)
+    assert np.array_equal(host(out), oracle.reduce_fold(ins))
+
+
+@pytest.mark.parametrize("n_in", [2, 4, 16])
+def test_reduce_kahan_vs_f64(T, n_in):
+    torch, ops = T
+    rng = np.random.default_rng(100 + n_in)
+    shape = (1024, 1024)
+    ins = [(rng.standard_normal(shape) * 10 ** rng.uniform(-3, 3)).astype(np.float32) for _ in range(n_in)]
+    out = torch.empty(shape, device="cuda")
+    ops.reduce([dev(torch, x) for x in ins], out, kahan=True)
+    ref = oracle.reduce_f64(ins)
+    assert rel_err(host(out), ref) <= 1e-6
+
+
+def test_reduce_cancellation_exact(T):
+    torch, ops = T
+    g = golden("reduce_cancel.npz")
+    out = torch.empty(g["expect"].shape, device="cuda")
+    ops.reduce([dev(torch, x) for x in g["inputs"]], out, kahan=True)
+    assert np.array_equal(host(out), g["expect"])
+
+
+def test_reduce_in_place_alias(T):
+    torch, ops = T
+    rng = np.random.default_rng(9)
+    ins = [rng.standard_normal(10000).astype(np.float32) for _ in range(4)]
+    d = [dev(torch, x) for x in ins]
+    ops.reduce(d, d[0], kahan=False)
+    assert np.array_equal(host(d[0]), oracle.reduce_fold(ins))
+
+
+# ----------------------------------------------------------------- elementwise
+@pytest.mark.parametrize("op", [0, 1, 5, 7, 8])
+def test_unary_bit_exact(T, op):
+    torch, ops = T
+    x = np.random.default_rng(op).standard_normal(50001).astype(np.float32)
+    out = torch.empty_like(dev(torch, x))
+    ops.unary(op, dev(torch, x), out, 0.75)
+    assert np.array_equal(host(out), oracle.unary(op, x, 0.75))
+
+
+@pytest.mark.parametrize("op", [2, 3, 4, 6])
+def test_unary_transcendental(T, op):
+    torch, ops = T
+    x = np.random.default_rng(op).standard_normal(50001).astype(np.float32)
+    if op == 6:
+        x = np.abs(x)
+    out = torch.empty_like(dev(torch, x))
+    ops.unary(op, dev(torch, x), out)
+    got, ref = host(out), oracle.unary(op, x)
+    # expf differs between libm and CUDA by at most a couple of ulp
+    assert np.max(np.abs(got - ref) / np.maximum(np.abs(ref), 1e-30)) < 4e-7
+
+
+@pytest.mark.parametrize("op", [0, 1, 2, 3, 4, 5, 6])
+def test_binary_bit_exact(T, op):
+    torch, ops = T
+    rng = np.random.default_rng(op)
+    a = rng.standard_normal(30003).astype(np.float32)
+    b = rng.standard_normal(30003).astype(np.float32)
+    out = torch.empty(30003, device="cuda")
+    ops.binary(op, dev(torch, a), dev(torch, b), out, 0.3, -1.7)
+    assert np.array_equal(host(out), oracle.binary(op, a, b, 0.3, -1.7))
+
+
+def test_elementwise_golden(T):
+    torch, ops = T
+    g = golden("elementwise.npz")
+    a, b = dev(torch, g["a"]), dev(torch, g["b"])
+    out = torch.empty_like(a)
+    assert np.array_equal(host(ops.unary(0, a, out)), g["relu"])
+    assert np.array_equal(host(ops.unary(1, a, out)), g["relu_dif"])
+    assert np.array_equal(host(ops.binary(2, a, b, out)), g["hadamard"])
+    assert np.array_equal(host(ops.binary(1, a, b, out, 2.0, -3.0)), g["wsum"])
+    cs = torch.empty(a.shape[1], device="cuda")
+    assert np.array_equal(host(ops.colsum(a, cs)), g["colsum_a"])
+
+
+def test_bias_add_and_colsum(T):
+    torch, ops = T
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal((333, 257)).astype(np.float32)
+    bias = rng.standard_normal(257).astype(np.float32)
+    out = torch.empty(333, 257, device="cuda")
+    ops.bias_add(dev(torch, x), dev(torch, bias), out, relu=True)
+    assert np.array_equal(host(out), oracle.bias_add(x, bias, relu=True))
+    cs = dev(torch, bias.copy())
+    ops.colsum(dev(torch, x), cs, accumulate=True)
+    assert np.array_equal(host(cs), oracle.colsum(x, init=bias))
+
+
+def test_softmax_ce(T):
+    torch, ops = T
+    rng = np.random.default_rng(2)
+    z = (rng.standard_normal((300, 1024)) * 3).astype(np.float32)
+    y = rng.integers(0, 1024, 300).astype(np.int32)
+    loss = torch.empty(300, device="cuda")
+    grad = torch.empty(300, 1024, device="cuda")
+    ops.softmax_ce(dev(torch, z), dev(torch, y), loss, grad, grad_scale=1.0 / 300)
+    l64, g64 = oracle.softmax_ce_f64(z, y, grad_scale=1.0 / 300)
+    assert rel_err(host(loss), l64) < 1e-5
+    assert rel_err(host(grad), g64) < 1e-5
+
+
+def test_philox_fill_matches_oracle(T):
+    torch, ops = T
+    out = torch.empty(100003, device="cuda")
+    ops.fill_philox(out, seed=0x1234_5678_9abc, dist=0, a=-1.0, b=1.0)
+    assert np.array_equal(host(out), oracle.uniform(0x1234_5678_9abc, 100003, -1.0, 1.0))
+    nrm = torch.empty(1 << 20, device="cuda")
+    ops.fill_philox(nrm, seed=7, dist=1, a=0.0, b=1.0)
+    v = host(nrm)
+    assert abs(v.mean()) < 0.01 and abs(v.std() - 1.0) < 0.01
+
+
+def test_cast_and_permute(T):
+    torch, ops = T
+    x = np.random.default_rng(4).standard_normal((7, 9, 11, 5)).astype(np.float32)
+    out = torch.empty((11, 7, 5, 9), device="cuda")
+    ops.permute(dev(torch, x), [2, 0, 3, 1], out)
+    assert np.array_equal(host(out), np.transpose(x, (2, 0, 3, 1)))
+    bf = torch.empty(x.size, dtype=torch.bfloat16, device="cuda")
+    ops.cast(dev(torch, x.ravel()), bf)
+    assert np.array_equal(host(bf), bf16_round(x.ravel()))
+
+
+# ----------------------------------------------------------------- matmul FP32
+@pytest.mark.parametrize("m,n,k", [(1024, 1024, 1024), (130, 70, 40), (1, 1, 1), (257, 129, 300)])
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+def test_matmul_f32_vs_f64(T, m, n, k, ta, tb):
+    torch, ops = T
+    rng = np.random.default_rng(m + n + k)
+    a = rng.standard_normal((k, m) if ta else (m, k)).astype(np.float32)
+    b = rng.standard_normal((n, k) if tb else (k, n)).astype(np.float32)
+    c = torch.empty(m, n, device="cuda")
+    ops.matmul_f32(dev(torch, a), dev(torch, b), c, bool(ta), bool(tb))
+    ref = oracle.matmul_f64(a, b, bool(ta), bool(tb))
+    assert rel_err(host(c), ref) <= 1e-5
+
+
+def test_matmul_f32_integer_exact(T):
+    torch, ops = T
+    g = golden("matmul_int.npz")
+    for key in ["128x256x64", "200x136x96", "256x512x256", "130x70x40"]:
+        a, b, cref = g[key + "_a"], g[key + "_b"], g[key + "_c"]
+        c = torch.empty(cref.shape, device="cuda")
+        ops.matmul_f32(dev(torch, a), dev(torch, b), c)
+        assert np.array_equal(host(c), cref)
+
+
+def test_matmul_f32_epilogue_and_batch(T):
+    torch, ops = T
+    rng = np.random.default_rng(8)
+    a = rng.standard_normal((3, 100, 64)).astype(np.float32)
+    b = rng.standard_normal((3, 64, 90)).astype(np.float32)
+    c0 = rng.standard_normal((3, 100, 90)).astype(np.float32)
+    bias = rng.standard_normal(90).astype(np.float32)
+    c = dev(torch, c0)
+    ops.matmul_f32(dev(torch, a), dev(torch, b), c, alpha=0.5, beta=2.0, bias=dev(torch, bias), relu=True)
+    ref = np.stack([oracle.matmul_f64(a[i], b[i]) for i in range(3)]) * 0.5 + 2.0 * c0 + bias
+    ref = np.maximum(ref, 0)
+    assert rel_err(host(c), ref) <= 1e-5
+
+
+# ----------------------------------------------------------------- matmul tensor cores
+@pytest.mark.parametrize("key", ["128x256x64", "200x136x96", "256x512x256", "130x70x40"])
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("tile_n", [128, 256])
+def test_matmul_tc_bf16_integer_exact(T, key, ta, tb, tile_n):
+    torch, ops = T
+    g = golden("matmul_int.npz")
+    a, b, cref = g[key + "_a"], g[key + "_b"], g[key + "_c"]
+    A = np.ascontiguousarray(a.T) if ta else a
+    B = np.ascontiguousarray(b.T) if tb else b
+    # pad pitches to 16 bytes
+    def padded(x):
+        rows, cols = x.shape
+        p = (cols + 7) // 8 * 8
+        buf = torch.zeros(rows, p, dtype=torch.bfloat16, device="cuda")
+        buf[:, :cols] = dev(torch, x, torch.bfloat16)
+        return buf[:, :cols]
+    Ad, Bd = padded(A), padded(B)
+    c = torch.full(cref.shape, -7.0, device="cuda")
+    ops.matmul_tc([ops.tc_problem(Ad, Bd, c, bool(ta), bool(tb))], tile_n=tile_n)
+    assert np.array_equal(host(c), cref)
+
+
+@pytest.mark.parametrize("m,n,k", [(1024, 1024, 1024), (384, 640, 4096), (192, 320, 136)])
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+def test_matmul_tc_bf16_random_vs_f64(T, m, n, k, ta, tb):
+    torch, ops = T
+    rng = np.random.default_rng(m * 7 + n + k)
+    a = rng.standard_normal((k, m) if ta else (m, k)).astype(np.float32)
+    b = rng.standard_normal((n, k) if tb else (k, n)).astype(np.float32)
+    ab, bb = bf16_round(a), bf16_round(b)
+    c = torch.empty(m, n, device="cuda")
+    ops.matmul_tc([ops.tc_problem(dev(torch, a, torch.bfloat16), dev(torch, b, torch.bfloat16), c,
+                                  bool(ta), bool(tb))])
+    # vs FP64 on the bf16-rounded inputs: only accumulation-order error remains
+    assert rel_err(host(c), oracle.matmul_f64(ab, bb, bool(ta), bool(tb))) <= 1e-5
+    # vs FP64 on the original FP32 inputs: the bf16 input rounding, within the 1e-2 budget
+    assert rel_err(host(c), oracle.matmul_f64(a, b, bool(ta), bool(tb))) <= 1e-2
+
+
+def test_matmul_tc_grouped_epilogues(T):
+    torch, ops = T
+    rng = np.random.default_rng(77)
+    probs, refs, outs, keep = [], [], [], []
+    shapes = [(256, 256, 128), (128, 384, 64), (300, 200, 72), (512, 128, 256), (64, 64, 64), (200, 520, 320)]
+    for i, (m, n, k) in enumerate(shapes):
+        a = bf16_round(rng.standard_normal((m, k)))
+        b = bf16_round(rng.standard_normal((k, n)))
+        c0 = rng.standard_normal((m, n)).astype(np.float32)
+        bias = rng.standard_normal(n).astype(np.float32)
+        A, B, Cd, Bi = dev(torch, a, torch.bfloat16), dev(torch, b, torch.bfloat16), dev(torch, c0), dev(torch, bias)
+        keep += [A, B, Bi]
+        relu = i % 2 == 0
+        probs.append(ops.tc_problem(A, B, Cd, alpha=0.5, beta=1.5, bias=Bi, relu=relu))
+        ref = 0.5 * oracle.matmul_f64(a, b) + 1.5 * c0 + bias
+        refs.append(np.maximum(ref, 0) if relu else ref)
+        outs.append(Cd)
+    ops.matmul_tc(probs)  # 6 problems -> device problem table path
+    for o, r in zip(outs, refs):
+        assert rel_err(host(o), r) <= 1e-5
+
+
+def test_matmul_tc_bf16_output(T):
+    torch, ops = T
+    rng = np.random.default_rng(5)
+    a = bf16_round(rng.standard_normal((256, 512)))
+    b = bf16_round(rng.standard_normal((512, 384)))
+    c = torch.empty(256, 384, dtype=torch.bfloat16, device="cuda")
+    ops.matmul_tc([ops.tc_problem(dev(torch, a, torch.bfloat16), dev(torch, b, torch.bfloat16), c)])
+    assert rel_err(host(c), oracle.matmul_f64(a, b)) <= 1e-2
+
+
+def test_matmul_tc_plan_replay(T):
+    torch, ops = T
+    rng = np.random.default_rng(6)
+    a = bf16_round(rng.standard_normal((512, 256)))
+    b = bf16_round(rng.standard_normal((256, 512)))
+    A, B = dev(torch, a, torch.bfloat16), dev(torch, b, torch.bfloat16)
+    cs = [torch.empty(512, 512, device="cuda") for _ in range(5)]
+    plan = ops.TcPlan([ops.tc_problem(A, B, c) for c in cs])
+    ref = oracle.matmul_f64(a, b)
+    for _ in range(3):
+        for c in cs:
+            c.zero_()
+        plan.launch()
+        for c in cs:
+            assert rel_err(host(c), ref) <= 1e-5
+    plan.close()
+
+
+def test_matmul_fp8_per_block_scale(T):
+    torch, ops = T
+    rng = np.random.default_rng(12)
+    m, n, k = 512, 512, 1024
+    a = rng.uniform(-1, 1, (m, k)).astype(np.float32)
+    b = rng.uniform(-1, 1, (k, n)).astype(np.float32)
+    qa = torch.empty(m, k, dtype=torch.float8_e4m3fn, device="cuda")
+    qb = torch.empty(n, k, dtype=torch.float8_e4m3fn, device="cuda")  # K-major via transpose
+    sa = torch.empty(1, device="cuda")
+    sb = torch.empty(1, device="cuda")
+    ops.quantize_e4m3(dev(torch, a), qa, sa)
+    ops.quantize_e4m3(dev(torch, b), qb, sb, transpose=True)
+    c = torch.empty(m, n, device="cuda")
+    scale = float(host(sa)[0] * host(sb)[0])
+    ops.matmul_tc([ops.tc_problem(qa, qb, c, trans_b=True, alpha=scale)], in_dtype=ops.E4M3)
+    # e4m3 keeps 3 mantissa bits (relative rounding error up to 2^-4 per input), so
+    # the normwise error of a K=1024 dot product sits at a few percent: FP8 is
+    # outside the 1e-2 budget, and the error is reported per block instead.
+    assert rel_err(host(c), oracle.matmul_f64(a, b)) <= 6e-2
+    # the same inputs dequantised exactly on the host give the kernel's own arithmetic
+    deq_a = qa.float().cpu().numpy() * host(sa)[0]
+    deq_b = qb.float().cpu().numpy().T * host(sb)[0]
+    assert rel_err(host(c), oracle.matmul_f64(np.ascontiguousarray(deq_a), np.ascontiguousarray(deq_b))) <= 1e-5
+
+
+# ----------------------------------------------------------------- contraction
+@pytest.mark.parametrize("precision", [0, 1])
+def test_contraction_golden(T, precision):
+    torch, ops = T
+    g = golden("contraction_int.npz")
+    I, J, K, L = [int(v) for v in g["c1_dims"]]
+    out = torch.empty(I * J * L, device="cuda")
+    ops.contraction(dev(torch, g["c1_lhs"]), [I, J, K], [0, 1, 2], dev(torch, g["c1_rhs"]), [K, L], [2, 3],
+                    out, [0, 1, 3], 1.0, precision)
+    assert np.array_equal(host(out), g["c1_out"])
+    B, I2, K2, J2 = [int(v) for v in g["c2_dims"]]
+    out2 = torch.empty(B * I2 * J2, device="cuda")
+    ops.contraction(dev(torch, g["c2_lhs"]), [B, I2, K2], [0, 1, 2], dev(torch, g["c2_rhs"]), [K2, J2, B], [2, 3, 0],
+                    out2, [3, 1, 0], 1.0, precision)
+    assert np.array_equal(host(out2), g["c2_out"])
+
+
+@pytest.mark.parametrize("spec", [
+    ([37, 45, 64], [0, 1, 2], [64, 129], [2, 3], [0, 1, 3]),      # ijk,kl->ijl
+    ([50, 40], [0, 1], [40, 30], [1, 2], [2, 0]),                 # transposed output
+    ([20, 30, 6], [0, 1, 2], [30, 25], [1, 3], [3, 0]),           # lhs-only mode summed
+    ([8, 9], [0, 1], [10, 11], [2, 3], [0, 2, 1, 3]),             # outer product
+])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_contraction_random_vs_f64(T, spec, precision):
+    torch, ops = T
+    dl, ml, dr, mr, mo = spec
+    rng = np.random.default_rng(len(dl) * 10 + len(mo))
+    lhs = rng.standard_normal(int(np.prod(dl))).astype(np.float32)
+    rhs = rng.standard_normal(int(np.prod(dr))).astype(np.float32)
+    ext = dict(zip(ml, dl)); ext.update(zip(mr, dr))
+    out = torch.empty(int(np.prod([ext[m] for m in mo])), device="cuda")
+    ops.contraction(dev(torch, lhs), dl, ml, dev(torch, rhs), dr, mr, out, mo, 0.5, precision)
+    if precision == 0:
+        ref = oracle.contraction_f64(lhs, dl, ml, rhs, dr, mr, mo, 0.5)
+        assert rel_err(host(out), ref) <= 1e-5
+    else:
+        ref = oracle.contraction_f64(lhs, dl, ml, rhs, dr, mr, mo, 0.5)
+        assert rel_err(host(out), ref) <= 1e-2
