@@ -594,3 +594,110 @@ int bbx_permute(const float* in, int rank, const long long* in_dims, const int* 
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ grouped streaming ops
+struct bbx_stream_plan {
+  StreamOp* d_table = nullptr;
+  int count = 0;
+  long long total_chunks = 0;
+};
+
+namespace bbx {
+static int build_stream_table(const bbx_stream_op_t* ops, int count, std::vector<StreamOp>* out,
+                              long long* total) {
+  static_assert(kStreamMaxIn == BBX_STREAM_MAX_IN, "stream op fan-in mismatch");
+  out->resize(count);
+  long long chunks = 0;
+  for (int i = 0; i < count; ++i) {
+    const bbx_stream_op_t& q = ops[i];
+    StreamOp& o = (*out)[i];
+    memset(&o, 0, sizeof(o));
+    if (q.kind < S_SUM || q.kind > S_CAST) return set_error(BBX_ERR_INVALID, "stream op %d: kind %d", i, q.kind);
+    const int need = q.kind == S_SUM ? q.n_in : (q.kind == S_BINARY ? 2 : 1);
+    if (need < 1 || need > kStreamMaxIn) return set_error(BBX_ERR_INVALID, "stream op %d: %d inputs", i, need);
+    if ((q.in_dtype != BBX_F32 && q.in_dtype != BBX_BF16) || (q.out_dtype != BBX_F32 && q.out_dtype != BBX_BF16))
+      return set_error(BBX_ERR_UNSUPPORTED, "stream op %d: dtype", i);
+    if (q.n < 0) return set_error(BBX_ERR_INVALID, "stream op %d: n < 0", i);
+    if (q.n > 0 && !q.out) return set_error(BBX_ERR_INVALID, "stream op %d: null output", i);
+    uintptr_t align = (uintptr_t)q.out;
+    for (int j = 0; j < need; ++j) {
+      if (q.n > 0 && !q.in[j]) return set_error(BBX_ERR_INVALID, "stream op %d: null input %d", i, j);
+      o.in[j] = q.in[j];
+      align |= (uintptr_t)q.in[j];
+    }
+    o.kind = q.kind; o.op = q.op; o.in_dtype = q.in_dtype; o.out_dtype = q.out_dtype;
+    o.n_in = need; o.kahan = q.kahan; o.n = q.n; o.out = q.out; o.p0 = q.p0; o.p1 = q.p1;
+    const uintptr_t need_align = (q.in_dtype == BBX_F32 || q.out_dtype == BBX_F32) ? 15 : 7;
+    o.vec = (align & need_align) == 0;
+    o.chunk_start = chunks;
+    chunks += (q.n + kStreamChunk - 1) / kStreamChunk;
+  }
+  *total = chunks;
+  return BBX_OK;
+}
+}  // namespace bbx
+
+extern "C" {
+
+int bbx_stream_plan_create(const bbx_stream_op_t* ops, int count, bbx_stream_plan_t** out) {
+  if (!ops || count <= 0 || !out) return set_error(BBX_ERR_INVALID, "bad stream plan arguments");
+  std::vector<StreamOp> table;
+  long long total = 0;
+  int rc = build_stream_table(ops, count, &table, &total);
+  if (rc) return rc;
+  auto* p = new bbx_stream_plan();
+  p->count = count;
+  p->total_chunks = total;
+  cudaError_t e = cudaMalloc(&p->d_table, sizeof(StreamOp) * count);
+  if (e == cudaSuccess) e = cudaMemcpy(p->d_table, table.data(), sizeof(StreamOp) * count, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    if (p->d_table) cudaFree(p->d_table);
+    delete p;
+    return set_error(BBX_ERR_CUDA, "stream plan upload: %s", cudaGetErrorString(e));
+  }
+  *out = p;
+  return BBX_OK;
+}
+
+int bbx_stream_plan_launch(bbx_stream_plan_t* p, void* stream) {
+  if (!p) return set_error(BBX_ERR_INVALID, "null stream plan");
+  if (p->total_chunks == 0) return BBX_OK;
+  DeviceState* d;
+  int rc = device_state(&d);
+  if (rc) return rc;
+  long long grid = std::min<long long>(p->total_chunks, (long long)d->sms * 8);
+  k_stream_group<<<(int)grid, 256, 0, (cudaStream_t)stream>>>(p->d_table, p->count, p->total_chunks);
+  BBX_CHECK_LAUNCH("k_stream_group");
+  return BBX_OK;
+}
+
+int bbx_stream_plan_destroy(bbx_stream_plan_t* p) {
+  if (!p) return BBX_OK;
+  if (p->d_table) cudaFree(p->d_table);
+  delete p;
+  return BBX_OK;
+}
+
+int bbx_stream_group(const bbx_stream_op_t* ops, int count, void* stream) {
+  if (!ops || count <= 0) return set_error(BBX_ERR_INVALID, "bad stream group arguments");
+  std::vector<StreamOp> table;
+  long long total = 0;
+  int rc = build_stream_table(ops, count, &table, &total);
+  if (rc) return rc;
+  if (total == 0) return BBX_OK;
+  DeviceState* d;
+  rc = device_state(&d);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  StreamOp* dt = nullptr;
+  BBX_CUDA(cudaMallocAsync(&dt, sizeof(StreamOp) * count, st));
+  BBX_CUDA(cudaMemcpyAsync(dt, table.data(), sizeof(StreamOp) * count, cudaMemcpyHostToDevice, st));
+  long long grid = std::min<long long>(total, (long long)d->sms * 8);
+  k_stream_group<<<(int)grid, 256, 0, st>>>(dt, count, total);
+  cudaError_t le = cudaGetLastError();
+  cudaFreeAsync(dt, st);
+  if (le != cudaSuccess) return set_error(BBX_ERR_CUDA, "k_stream_group: %s", cudaGetErrorString(le));
+  return BBX_OK;
+}
+
+}  // extern "C"

@@ -355,3 +355,161 @@ __global__ void k_permute(const float* __restrict__ in, TO* out, const __grid_co
 }
 
 }  // namespace bbx
+
+namespace bbx {
+
+// ------------------------------------------------------------------ grouped streaming ops
+// One launch processes a table of independent streaming block ops (the add /
+// reduce / elementwise / cast commands of one DAG level). Work is split into
+// chunks of kStreamChunk elements; chunk c belongs to the op whose
+// [chunk_start, chunk_start + chunks) range contains it.
+enum StreamKind : int { S_SUM = 0, S_UNARY = 1, S_BINARY = 2, S_CAST = 3 };
+constexpr int kStreamMaxIn = 16;
+constexpr long long kStreamChunk = 8192;
+
+struct StreamOp {
+  int kind, op, in_dtype, out_dtype, n_in, kahan;
+  long long n;
+  const void* in[kStreamMaxIn];
+  void* out;
+  float p0, p1;
+  long long chunk_start;
+  int vec;  // all pointers 16-byte aligned (f32) / 8-byte aligned (bf16)
+  int pad_;
+};
+
+__device__ __forceinline__ void ld4(const void* p, int dt, long long i, float (&v)[4]) {
+  if (dt == 0) {
+    float4 x = *(const float4*)((const float*)p + i);
+    v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+  } else {
+    uint2 x = *(const uint2*)((const __nv_bfloat16*)p + i);
+    __nv_bfloat162 a = *(__nv_bfloat162*)&x.x, b = *(__nv_bfloat162*)&x.y;
+    float2 fa = __bfloat1622float2(a), fb = __bfloat1622float2(b);
+    v[0] = fa.x; v[1] = fa.y; v[2] = fb.x; v[3] = fb.y;
+  }
+}
+__device__ __forceinline__ float ld1(const void* p, int dt, long long i) {
+  return dt == 0 ? ((const float*)p)[i] : __bfloat162float(((const __nv_bfloat16*)p)[i]);
+}
+__device__ __forceinline__ void st4(void* p, int dt, long long i, const float (&v)[4]) {
+  if (dt == 0) {
+    *(float4*)((float*)p + i) = make_float4(v[0], v[1], v[2], v[3]);
+  } else {
+    __nv_bfloat162 a = __floats2bfloat162_rn(v[0], v[1]), b = __floats2bfloat162_rn(v[2], v[3]);
+    uint2 x;
+    x.x = *(uint32_t*)&a;
+    x.y = *(uint32_t*)&b;
+    *(uint2*)((__nv_bfloat16*)p + i) = x;
+  }
+}
+__device__ __forceinline__ void st1(void* p, int dt, long long i, float v) {
+  if (dt == 0) ((float*)p)[i] = v;
+  else ((__nv_bfloat16*)p)[i] = __float2bfloat16_rn(v);
+}
+
+// Unary / binary / cast element (sums are evaluated inline by the caller).
+__device__ __forceinline__ float stream_eval(const StreamOp& o, const float* x) {
+  switch (o.kind) {
+    case S_UNARY: return apply_unary(o.op, x[0], o.p0);
+    case S_BINARY: return apply_binary(o.op, x[0], x[1], o.p0, o.p1);
+    default: return x[0];
+  }
+}
+
+__global__ void __launch_bounds__(256) k_stream_group(const StreamOp* __restrict__ table, int count,
+                                                      long long total_chunks) {
+  for (long long c = blockIdx.x; c < total_chunks; c += gridDim.x) {
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (table[mid].chunk_start <= c) lo = mid; else hi = mid - 1;
+    }
+    const StreamOp& o = table[lo];
+    const long long e0 = (c - o.chunk_start) * kStreamChunk;
+    const long long e1 = min(e0 + kStreamChunk, o.n);
+    const int kind = o.kind, idt = o.in_dtype, odt = o.out_dtype, nin = o.n_in;
+    if (o.vec) {
+      for (long long i = e0 + 4 * threadIdx.x; i < e1; i += 4 * blockDim.x) {
+        if (i + 4 <= e1) {
+          float a[4], b[4], r[4];
+          ld4(o.in[0], idt, i, a);
+          if (kind == S_SUM) {
+            float comp[4] = {0.f, 0.f, 0.f, 0.f};
+            for (int j = 1; j < nin; ++j) {
+              ld4(o.in[j], idt, i, b);
+#pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                if (o.kahan) {
+                  float y = __fsub_rn(b[u], comp[u]);
+                  float t = __fadd_rn(a[u], y);
+                  comp[u] = __fsub_rn(__fsub_rn(t, a[u]), y);
+                  a[u] = t;
+                } else {
+                  a[u] = __fadd_rn(a[u], b[u]);
+                }
+              }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) r[u] = a[u];
+          } else if (kind == S_BINARY) {
+            ld4(o.in[1], idt, i, b);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) r[u] = apply_binary(o.op, a[u], b[u], o.p0, o.p1);
+          } else if (kind == S_UNARY) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) r[u] = apply_unary(o.op, a[u], o.p0);
+          } else {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) r[u] = a[u];
+          }
+          st4(o.out, odt, i, r);
+        } else {
+          for (long long q = i; q < e1; ++q) {
+            float x[2] = {ld1(o.in[0], idt, q), 0.f};
+            if (kind == S_SUM) {
+              float comp = 0.f;
+              for (int j = 1; j < nin; ++j) {
+                float v = ld1(o.in[j], idt, q);
+                if (o.kahan) {
+                  float y = __fsub_rn(v, comp), t = __fadd_rn(x[0], y);
+                  comp = __fsub_rn(__fsub_rn(t, x[0]), y);
+                  x[0] = t;
+                } else {
+                  x[0] = __fadd_rn(x[0], v);
+                }
+              }
+              st1(o.out, odt, q, x[0]);
+            } else {
+              if (kind == S_BINARY) x[1] = ld1(o.in[1], idt, q);
+              st1(o.out, odt, q, stream_eval(o, x));
+            }
+          }
+        }
+      }
+    } else {
+      for (long long q = e0 + threadIdx.x; q < e1; q += blockDim.x) {
+        float x[2] = {ld1(o.in[0], idt, q), 0.f};
+        if (kind == S_SUM) {
+          float comp = 0.f;
+          for (int j = 1; j < nin; ++j) {
+            float v = ld1(o.in[j], idt, q);
+            if (o.kahan) {
+              float y = __fsub_rn(v, comp), t = __fadd_rn(x[0], y);
+              comp = __fsub_rn(__fsub_rn(t, x[0]), y);
+              x[0] = t;
+            } else {
+              x[0] = __fadd_rn(x[0], v);
+            }
+          }
+          st1(o.out, odt, q, x[0]);
+        } else {
+          if (kind == S_BINARY) x[1] = ld1(o.in[1], idt, q);
+          st1(o.out, odt, q, stream_eval(o, x));
+        }
+      }
+    }
+  }
+}
+
+}  // namespace bbx

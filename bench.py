@@ -40,6 +40,8 @@ def parse():
     p.add_argument("--tile-n", type=int, default=0)
     p.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparator leg")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--grid", type=int, default=8,
+                   help="blocks per side of A/B (8 = the full workload; smaller only for profiling captures)")
     return p.parse_args()
 
 
@@ -143,7 +145,10 @@ def run_reference(args):
 
 
 def main():
+    global GRID, FLOP_PER_STEP
     args = parse()
+    GRID = args.grid
+    FLOP_PER_STEP = 2.0 * (GRID * BS) ** 2 * BS
     if args.impl == "reference":
         return run_reference(args)
     import torch

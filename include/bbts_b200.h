@@ -169,6 +169,28 @@ int bbx_softmax_ce_f32(const float* logits, const int* labels, float* loss, floa
 int bbx_permute(const float* in, int rank, const long long* in_dims, const int* perm,
                 int dst_dtype, void* out, void* stream);
 
+/* Grouped streaming ops: ONE launch runs a whole batch of independent
+ * add / n-ary reduce / elementwise / cast block ops over f32 or bf16 payloads
+ * (inputs read once, math in f32). Used per DAG level by the executor, in
+ * place of one dense_add_kernel launch per op (dense_matrix_gpu_add.cu:74-81). */
+#define BBX_S_SUM 0    /* out = in[0] + ... + in[n_in-1], left to right (kahan optional) */
+#define BBX_S_UNARY 1  /* out = unary(op, in[0], p0) */
+#define BBX_S_BINARY 2 /* out = binary(op, in[0], in[1], p0, p1) */
+#define BBX_S_CAST 3   /* out = in[0] converted */
+#define BBX_STREAM_MAX_IN 16
+typedef struct bbx_stream_op {
+  int kind, op, in_dtype, out_dtype, n_in, kahan;
+  long long n;
+  const void* in[BBX_STREAM_MAX_IN];
+  void* out;
+  float p0, p1;
+} bbx_stream_op_t;
+int bbx_stream_group(const bbx_stream_op_t* ops, int count, void* stream);
+typedef struct bbx_stream_plan bbx_stream_plan_t;
+int bbx_stream_plan_create(const bbx_stream_op_t* ops, int count, bbx_stream_plan_t** out);
+int bbx_stream_plan_launch(bbx_stream_plan_t* plan, void* stream);
+int bbx_stream_plan_destroy(bbx_stream_plan_t* plan);
+
 /* einsum contraction of the reference's "cutensor" plugin
  * (libraries/cutensor/contraction.h:25-63 params, :131-202 semantics):
  * out = alpha * sum lhs * rhs over modes absent from the output. Tensors are
