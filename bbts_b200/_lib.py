@@ -53,6 +53,49 @@ SIGNATURES = {
     "bbx_permute": (i32, [pf, i32, C.POINTER(i64), C.POINTER(i32), i32, pf, vp]),
     "bbx_contraction": (i32, [pf, i32, C.POINTER(i64), C.POINTER(i32), pf, i32, C.POINTER(i64),
                               C.POINTER(i32), pf, i32, C.POINTER(i32), f32, i32, vp]),
+    "bbx_stream_group": (i32, [vp, i32, vp]),
+    "bbx_stream_plan_create": (i32, [vp, i32, C.POINTER(vp)]),
+    "bbx_stream_plan_launch": (i32, [vp, vp]),
+    "bbx_stream_plan_destroy": (i32, [vp]),
+    # runtime
+    "bbx_rt_create": (i32, [C.POINTER(vp)]),
+    "bbx_rt_destroy": (i32, [vp]),
+    "bbx_rt_stream": (i32, [vp, C.POINTER(vp)]),
+    "bbx_rt_fmt_id": (i32, [vp, C.c_char_p]),
+    "bbx_rt_find_impl": (i32, [vp, C.c_char_p, C.c_char_p, C.c_char_p, i32, C.POINTER(i32), C.POINTER(i32)]),
+    "bbx_rt_impl_name": (i32, [vp, i32, i32, C.c_char_p, sz]),
+    "bbx_rt_complexity": (i32, [vp, i32, i32, C.POINTER(C.c_uint32), i32, vp, i32, C.POINTER(u64)]),
+    "bbx_rt_tensor_put": (i32, [vp, i32, vp, vp, sz, i32]),
+    "bbx_rt_tensor_get": (i32, [vp, i32, vp, vp, sz, i32]),
+    "bbx_rt_tensor_payload": (i32, [vp, i32, C.POINTER(vp), C.POINTER(sz)]),
+    "bbx_rt_tensor_count": (i32, [vp]),
+    "bbx_rt_tensor_remove": (i32, [vp, i32]),
+    "bbx_rt_queue_apply": (i32, [vp, i32, i32, i32, C.POINTER(C.c_uint32), i32, C.POINTER(i32), i32,
+                                 C.POINTER(i32), i32]),
+    "bbx_rt_queue_reduce": (i32, [vp, i32, i32, i32, C.POINTER(C.c_uint32), i32, C.POINTER(i32), i32, i32]),
+    "bbx_rt_queue_delete": (i32, [vp, i32, C.POINTER(i32), i32]),
+    "bbx_rt_clear_commands": (i32, [vp]),
+    "bbx_rt_num_commands": (i32, [vp]),
+    "bbx_rt_run": (i32, [vp, i32]),
+    "bbx_rt_record": (i32, [vp, i32, vp, vp, i32, C.POINTER(i32)]),
+    "bbx_dag_build": (i32, [vp, i32, i32, C.POINTER(vp)]),
+    "bbx_dag_launch": (i32, [vp, vp]),
+    "bbx_dag_destroy": (i32, [vp]),
+    "bbx_dag_stats": (i32, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(i32), C.POINTER(i32),
+                            C.POINTER(i32), C.POINTER(i32), C.POINTER(sz)]),
+    "bbx_dag_tensor": (i32, [vp, i32, C.POINTER(vp), vp]),
+    "bbx_dag_read": (i32, [vp, i32, vp, sz]),
+    # learned cost model
+    "bbx_mlp_create": (i32, [u64, C.POINTER(vp)]),
+    "bbx_mlp_destroy": (i32, [vp]),
+    "bbx_mlp_set_norm": (i32, [vp, vp, vp]),
+    "bbx_mlp_train": (i32, [vp, vp, vp, i32, i32, i32, f32, C.POINTER(f32)]),
+    "bbx_mlp_predict": (i32, [vp, vp, i32, vp]),
+    "bbx_mlp_loss_grad": (i32, [vp, vp, vp, i32, C.POINTER(f32), vp]),
+    "bbx_mlp_num_params": (i32, []),
+    "bbx_mlp_get_params": (i32, [vp, vp]),
+    "bbx_mlp_set_params": (i32, [vp, vp]),
+    "bbx_rt_set_predictor": (i32, [vp, vp]),
 }
 
 for _name, (_res, _args) in SIGNATURES.items():

@@ -58,6 +58,26 @@ struct DeviceState {
 static std::mutex g_dev_mu;
 static DeviceState g_dev[64];
 
+template <int BN, bool AMN, bool BMN, bool FP8>
+static int set_tc_attr() {
+  BBX_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<BN, AMN, BMN, FP8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                TcCfg<BN, AMN, BMN, FP8>::SMEM_BYTES));
+  return BBX_OK;
+}
+
+static int init_tc_attributes() {
+  int rc = 0;
+  rc |= set_tc_attr<256, false, false, false>(); rc |= set_tc_attr<256, false, true, false>();
+  rc |= set_tc_attr<256, true, false, false>();  rc |= set_tc_attr<256, true, true, false>();
+  rc |= set_tc_attr<128, false, false, false>(); rc |= set_tc_attr<128, false, true, false>();
+  rc |= set_tc_attr<128, true, false, false>();  rc |= set_tc_attr<128, true, true, false>();
+  rc |= set_tc_attr<256, false, false, true>();  rc |= set_tc_attr<256, false, true, true>();
+  rc |= set_tc_attr<256, true, false, true>();   rc |= set_tc_attr<256, true, true, true>();
+  rc |= set_tc_attr<128, false, false, true>();  rc |= set_tc_attr<128, false, true, true>();
+  rc |= set_tc_attr<128, true, false, true>();   rc |= set_tc_attr<128, true, true, true>();
+  return rc ? BBX_ERR_CUDA : BBX_OK;
+}
+
 int device_state(DeviceState** out) {
   int dev = 0;
   BBX_CUDA(cudaGetDevice(&dev));
@@ -69,6 +89,11 @@ int device_state(DeviceState** out) {
     BBX_CUDA(cudaMalloc(&d.status, 256));
     BBX_CUDA(cudaMemset(d.status, 0, 256));
     d.scratch = (unsigned int*)(d.status + 16);
+    // Dynamic shared-memory opt-in for every tcgen05 variant, once, here: never
+    // inside a stream capture.
+    int rc = init_tc_attributes();
+    if (rc) return rc;
+    d.attr_done = 0xFFFFu;
     d.ready = true;
   }
   *out = &d;
@@ -362,46 +387,20 @@ int bbx_tc_plan_destroy(bbx_tc_plan_t* p) {
 int bbx_matmul_tc(int in_dtype, const bbx_tc_problem_t* problems, int count, int tile_n,
                   void* stream) {
   if (count <= 0 || !problems) return set_error(BBX_ERR_INVALID, "no problems");
-  if (count <= kTcMaxInline) {
+  if (tile_n == 0) tile_n = pick_tile_n(problems, count);
+  // Problems travel in the kernel parameters, kTcMaxInline per launch: no
+  // device table, no host-to-device copy, so the call is safe to capture in a
+  // CUDA graph. Large groups that are launched repeatedly should use a plan.
+  for (int i = 0; i < count; i += kTcMaxInline) {
+    const int c = std::min(kTcMaxInline, count - i);
     bbx_tc_plan_t* p = nullptr;
-    int rc = bbx_tc_plan_create(in_dtype, problems, count, tile_n, &p);
+    int rc = bbx_tc_plan_create(in_dtype, problems + i, c, tile_n, &p);
     if (rc) return rc;
     rc = bbx_tc_plan_launch(p, stream);
     bbx_tc_plan_destroy(p);  // inline plans own no device memory
-    return rc;
-  }
-  // Larger groups: stream-ordered table upload, freed after the launch in stream order.
-  if (in_dtype != BBX_BF16 && in_dtype != BBX_E4M3)
-    return set_error(BBX_ERR_UNSUPPORTED, "tensor-core input dtype must be bf16 or e4m3");
-  if (tile_n == 0) tile_n = pick_tile_n(problems, count);
-  DeviceState* d;
-  int rc = device_state(&d);
-  if (rc) return rc;
-  bool amn, bmn;
-  rc = group_layout(problems, count, &amn, &bmn);
-  if (rc) return rc;
-  std::vector<TcProblem> host(count);
-  int tiles = 0;
-  for (int i = 0; i < count; ++i) {
-    rc = build_problem(in_dtype, problems[i], tile_n, &host[i]);
     if (rc) return rc;
-    host[i].tile_start = tiles;
-    tiles += host[i].tiles_m * host[i].tiles_n;
   }
-  cudaStream_t st = (cudaStream_t)stream;
-  TcProblem* table = nullptr;
-  BBX_CUDA(cudaMallocAsync(&table, sizeof(TcProblem) * count, st));
-  BBX_CUDA(cudaMemcpyAsync(table, host.data(), sizeof(TcProblem) * count, cudaMemcpyHostToDevice, st));
-  // The pageable source above is staged by the driver before cudaMemcpyAsync returns.
-  TcArgs args;
-  memset(&args, 0, sizeof(args));
-  args.table = table;
-  args.num_problems = count;
-  args.total_tiles = tiles;
-  args.status = d->status;
-  rc = launch_tc(tile_n, amn, bmn, in_dtype == BBX_E4M3, args, std::min(tiles, d->sms), st, d);
-  cudaFreeAsync(table, st);
-  return rc;
+  return BBX_OK;
 }
 
 int bbx_add_f32(const float* a, const float* b, float* c, long long n, void* stream) {
@@ -680,23 +679,24 @@ int bbx_stream_plan_destroy(bbx_stream_plan_t* p) {
 
 int bbx_stream_group(const bbx_stream_op_t* ops, int count, void* stream) {
   if (!ops || count <= 0) return set_error(BBX_ERR_INVALID, "bad stream group arguments");
-  std::vector<StreamOp> table;
-  long long total = 0;
-  int rc = build_stream_table(ops, count, &table, &total);
-  if (rc) return rc;
-  if (total == 0) return BBX_OK;
   DeviceState* d;
-  rc = device_state(&d);
+  int rc = device_state(&d);
   if (rc) return rc;
-  cudaStream_t st = (cudaStream_t)stream;
-  StreamOp* dt = nullptr;
-  BBX_CUDA(cudaMallocAsync(&dt, sizeof(StreamOp) * count, st));
-  BBX_CUDA(cudaMemcpyAsync(dt, table.data(), sizeof(StreamOp) * count, cudaMemcpyHostToDevice, st));
-  long long grid = std::min<long long>(total, (long long)d->sms * 8);
-  k_stream_group<<<(int)grid, 256, 0, st>>>(dt, count, total);
-  cudaError_t le = cudaGetLastError();
-  cudaFreeAsync(dt, st);
-  if (le != cudaSuccess) return set_error(BBX_ERR_CUDA, "k_stream_group: %s", cudaGetErrorString(le));
+  // Ops travel in the kernel parameters, kStreamInline per launch (capture-safe).
+  for (int i = 0; i < count; i += kStreamInline) {
+    const int c = std::min(kStreamInline, count - i);
+    std::vector<StreamOp> table;
+    long long total = 0;
+    rc = build_stream_table(ops + i, c, &table, &total);
+    if (rc) return rc;
+    if (total == 0) continue;
+    StreamInline args;
+    memset(&args, 0, sizeof(args));
+    for (int j = 0; j < c; ++j) args.ops[j] = table[j];
+    long long grid = std::min<long long>(total, (long long)d->sms * 8);
+    k_stream_group_inline<<<(int)grid, 256, 0, (cudaStream_t)stream>>>(args, c, total);
+    BBX_CHECK_LAUNCH("k_stream_group_inline");
+  }
   return BBX_OK;
 }
 

@@ -1,0 +1,309 @@
+// C ABI of the runtime (declared in include/bbts_b200.h). Exceptions never
+// cross the ABI: they become BBX_ERR_* codes with the message in bbx_last_error.
+#include <cstring>
+#include <sstream>
+#include <stdexcept>
+#include "bbts_b200.h"
+#include "common.h"
+#include "runtime.h"
+
+using namespace bbts;
+
+struct bbx_rt {
+  runtime_t rt;
+};
+struct bbx_dag {
+  dag_t* d = nullptr;
+};
+
+namespace bbts {
+void* dag_tensor(const dag_t* d, tid_t tid, tensor_meta_t* meta);
+size_t dag_payload_bytes(const dag_t* d, tid_t tid);
+runtime_t* rt_of(bbx_rt* rt) { return &rt->rt; }
+}
+
+#define RT_TRY(...)                                                      \
+  try {                                                                  \
+    __VA_ARGS__;                                                         \
+    return BBX_OK;                                                       \
+  } catch (const std::exception& e) {                                    \
+    return bbx::set_error(BBX_ERR_INVALID, "%s", e.what());              \
+  } catch (...) {                                                        \
+    return bbx::set_error(BBX_ERR_INVALID, "unknown exception");         \
+  }
+
+static std::vector<std::string> split_types(const char* s) {
+  std::vector<std::string> out;
+  if (!s) return out;
+  std::stringstream ss(s);
+  std::string item;
+  while (std::getline(ss, item, ','))
+    if (!item.empty()) out.push_back(item);
+  return out;
+}
+
+static std::vector<command_param_t> to_params(const uint32_t* p, int n) {
+  std::vector<command_param_t> out(n);
+  for (int i = 0; i < n; ++i) out[i].u = p[i];
+  return out;
+}
+
+extern "C" {
+
+int bbx_rt_create(bbx_rt_t** out) {
+  if (!out) return bbx::set_error(BBX_ERR_INVALID, "null out");
+  RT_TRY(*out = new bbx_rt());
+}
+
+int bbx_rt_destroy(bbx_rt_t* rt) {
+  RT_TRY(delete rt);
+}
+
+int bbx_rt_stream(bbx_rt_t* rt, void** s) {
+  if (!rt || !s) return bbx::set_error(BBX_ERR_INVALID, "null argument");
+  *s = (void*)rt->rt.stream;
+  return BBX_OK;
+}
+
+int bbx_rt_fmt_id(bbx_rt_t* rt, const char* name) {
+  if (!rt || !name) return bbx::set_error(BBX_ERR_INVALID, "null argument");
+  return rt->rt.tf->get_tensor_ftm(name);
+}
+
+int bbx_rt_find_impl(bbx_rt_t* rt, const char* ud_name, const char* in_types, const char* out_types,
+                     int require_gpu, int* ud_id, int* impl_id) {
+  if (!rt || !ud_name || !ud_id || !impl_id) return bbx::set_error(BBX_ERR_INVALID, "null argument");
+  auto m = rt->rt.udm->get_matcher_for(ud_name);
+  if (!m) return bbx::set_error(BBX_ERR_NOT_FOUND, "no ud function named %s", ud_name);
+  ud_impl_t* impl = m->findMatch(split_types(in_types), split_types(out_types), require_gpu != 0);
+  if (!impl) return bbx::set_error(BBX_ERR_NOT_FOUND, "no impl of %s for (%s) -> (%s)", ud_name, in_types, out_types);
+  *ud_id = impl->impl_id.ud_id;
+  *impl_id = impl->impl_id.impl_id;
+  return BBX_OK;
+}
+
+int bbx_rt_impl_name(bbx_rt_t* rt, int ud_id, int impl_id, char* buf, size_t len) {
+  if (!rt) return bbx::set_error(BBX_ERR_INVALID, "null runtime");
+  ud_impl_t* impl = rt->rt.udm->get_fn_impl({ud_id, impl_id});
+  if (!impl) return bbx::set_error(BBX_ERR_NOT_FOUND, "unknown impl (%d,%d)", ud_id, impl_id);
+  if (buf && len) {
+    size_t n = std::min(len - 1, impl->impl_name.size());
+    memcpy(buf, impl->impl_name.data(), n);
+    buf[n] = 0;
+  }
+  return BBX_OK;
+}
+
+int bbx_rt_complexity(bbx_rt_t* rt, int ud_id, int impl_id, const uint32_t* params, int n_params,
+                      const void* in_metas, int n_in, unsigned long long* hint) {
+  if (!rt || !hint) return bbx::set_error(BBX_ERR_INVALID, "null argument");
+  ud_impl_t* impl = rt->rt.udm->get_fn_impl({ud_id, impl_id});
+  if (!impl) return bbx::set_error(BBX_ERR_NOT_FOUND, "unknown impl (%d,%d)", ud_id, impl_id);
+  RT_TRY({
+    std::vector<tensor_meta_t> metas(n_in);
+    for (int i = 0; i < n_in; ++i) memcpy(&metas[i], (const char*)in_metas + i * sizeof(tensor_meta_t), sizeof(tensor_meta_t));
+    auto p = to_params(params, n_params);
+    ud_impl_t::tensor_params_t tp;
+    tp._params = command_param_list_t{p.data(), p.size()};
+    ud_impl_t::meta_args_t ma(metas);
+    *hint = impl->get_complexity_hint(tp, ma);
+  });
+}
+
+int bbx_rt_tensor_put(bbx_rt_t* rt, int tid, const void* meta, const void* src, size_t bytes,
+                      int src_on_device) {
+  if (!rt || !meta) return bbx::set_error(BBX_ERR_INVALID, "null argument");
+  RT_TRY({
+    tensor_meta_t m;
+    memcpy(&m, meta, sizeof(m));
+    tensor_t* t = rt->rt.storage->create(tid, m);
+    size_t need = rt->rt.tf->get_payload_size(m);
+    if (src && bytes) {
+      if (bytes > need) throw std::runtime_error("tensor_put: more bytes than the meta describes");
+      cudaError_t e = cudaMemcpyAsync(t->_meta.payload(), src, bytes,
+                                      src_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                      rt->rt.stream);
+      if (e != cudaSuccess) throw std::runtime_error(std::string("tensor_put copy: ") + cudaGetErrorString(e));
+      e = cudaStreamSynchronize(rt->rt.stream);
+      if (e != cudaSuccess) throw std::runtime_error(std::string("tensor_put sync: ") + cudaGetErrorString(e));
+    }
+  });
+}
+
+int bbx_rt_tensor_get(bbx_rt_t* rt, int tid, void* meta_out, void* dst, size_t cap, int dst_on_device) {
+  if (!rt) return bbx::set_error(BBX_ERR_INVALID, "null runtime");
+  tensor_t* t = rt->rt.storage->get(tid);
+  if (!t) return bbx::set_error(BBX_ERR_NOT_FOUND, "no tensor %d", tid);
+  RT_TRY({
+    if (meta_out) memcpy(meta_out, &t->_meta, sizeof(tensor_meta_t));
+    size_t have = rt->rt.tf->get_payload_size(t->_meta);
+    size_t n = std::min(have, cap);
+    if (dst && n) {
+      cudaError_t e = cudaMemcpyAsync(dst, t->_meta.payload(), n,
+                                      dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                      rt->rt.stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(rt->rt.stream);
+      if (e != cudaSuccess) throw std::runtime_error(std::string("tensor_get copy: ") + cudaGetErrorString(e));
+    }
+  });
+}
+
+int bbx_rt_tensor_payload(bbx_rt_t* rt, int tid, void** ptr, size_t* bytes) {
+  if (!rt) return bbx::set_error(BBX_ERR_INVALID, "null runtime");
+  block_t* b = rt->rt.storage->block(tid);
+  if (!b) return bbx::set_error(BBX_ERR_NOT_FOUND, "no tensor %d", tid);
+  if (ptr) *ptr = b->payload;
+  if (bytes) *bytes = b->bytes;
+  return BBX_OK;
+}
+
+int bbx_rt_tensor_count(bbx_rt_t* rt) { return rt ? (int)rt->rt.storage->size() : -1; }
+
+int bbx_rt_tensor_remove(bbx_rt_t* rt, int tid) {
+  if (!rt) return bbx::set_error(BBX_ERR_INVALID, "null runtime");
+  return rt->rt.storage->remove(tid) ? BBX_OK : bbx::set_error(BBX_ERR_NOT_FOUND, "no tensor %d", tid);
+}
+
+static int check_order(bbx_rt_t* rt, int cmd_id) {
+  if (!rt->rt.commands.empty() && rt->rt.commands.back()->id >= cmd_id)
+    return bbx::set_error(BBX_ERR_INVALID, "command ids must increase (got %d after %d)", cmd_id,
+                          rt->rt.commands.back()->id);
+  return BBX_OK;
+}
+
+int bbx_rt_queue_apply(bbx_rt_t* rt, int cmd_id, int ud_id, int impl_id, const uint32_t* params,
+                       int n_params, const int* in_tids, int n_in, const int* out_tids, int n_out) {
+  if (!rt || n_in < 0 || n_out < 1) return bbx::set_error(BBX_ERR_INVALID, "bad apply");
+  if (int rc = check_order(rt, cmd_id)) return rc;
+  if (!rt->rt.udm->get_fn_impl({ud_id, impl_id})) return bbx::set_error(BBX_ERR_NOT_FOUND, "unknown impl (%d,%d)", ud_id, impl_id);
+  RT_TRY({
+    std::vector<command_t::tid_node_id_t> in, out;
+    for (int i = 0; i < n_in; ++i) in.push_back({in_tids[i], 0});
+    for (int i = 0; i < n_out; ++i) out.push_back({out_tids[i], 0});
+    rt->rt.commands.push_back(command_t::create_apply(cmd_id, {ud_id, impl_id}, true, to_params(params, n_params), in, out));
+  });
+}
+
+int bbx_rt_queue_reduce(bbx_rt_t* rt, int cmd_id, int ud_id, int impl_id, const uint32_t* params,
+                        int n_params, const int* in_tids, int n_in, int out_tid) {
+  if (!rt || n_in < 1) return bbx::set_error(BBX_ERR_INVALID, "bad reduce");
+  if (int rc = check_order(rt, cmd_id)) return rc;
+  ud_func_t* f = rt->rt.udm->get_udf(ud_id);
+  if (!f || !rt->rt.udm->get_fn_impl({ud_id, impl_id})) return bbx::set_error(BBX_ERR_NOT_FOUND, "unknown impl (%d,%d)", ud_id, impl_id);
+  // REDUCE needs an associative and commutative ud (src/commands/command_loader.h:146)
+  if (!f->is_ass || !f->is_com) return bbx::set_error(BBX_ERR_INVALID, "REDUCE needs an associative, commutative ud (%s is not)", f->ud_name.c_str());
+  RT_TRY({
+    std::vector<command_t::tid_node_id_t> in;
+    for (int i = 0; i < n_in; ++i) in.push_back({in_tids[i], 0});
+    rt->rt.commands.push_back(command_t::create_reduce(cmd_id, {ud_id, impl_id}, true, to_params(params, n_params), in, {out_tid, 0}));
+  });
+}
+
+int bbx_rt_queue_delete(bbx_rt_t* rt, int cmd_id, const int* tids, int n) {
+  if (!rt || n < 1) return bbx::set_error(BBX_ERR_INVALID, "bad delete");
+  if (int rc = check_order(rt, cmd_id)) return rc;
+  RT_TRY({
+    std::vector<command_t::tid_node_id_t> in;
+    for (int i = 0; i < n; ++i) in.push_back({tids[i], 0});
+    rt->rt.commands.push_back(command_t::create_delete(cmd_id, in));
+  });
+}
+
+int bbx_rt_clear_commands(bbx_rt_t* rt) {
+  if (!rt) return bbx::set_error(BBX_ERR_INVALID, "null runtime");
+  rt->rt.commands.clear();
+  return BBX_OK;
+}
+
+int bbx_rt_num_commands(bbx_rt_t* rt) { return rt ? (int)rt->rt.commands.size() : -1; }
+
+int bbx_rt_run(bbx_rt_t* rt, int policy) {
+  if (!rt) return bbx::set_error(BBX_ERR_INVALID, "null runtime");
+  RT_TRY({
+    rt->rt.run_per_op(policy, nullptr);
+    cudaError_t e = cudaStreamSynchronize(rt->rt.stream);
+    if (e != cudaSuccess) throw std::runtime_error(std::string("run: ") + cudaGetErrorString(e));
+  });
+}
+
+int bbx_rt_record(bbx_rt_t* rt, int policy, float* features, float* latency_us, int cap, int* n_out) {
+  if (!rt) return bbx::set_error(BBX_ERR_INVALID, "null runtime");
+  RT_TRY({
+    std::vector<std::pair<op_features_t, float>> rec;
+    rt->rt.run_per_op(policy, &rec);
+    int n = std::min<int>(cap, (int)rec.size());
+    for (int i = 0; i < n; ++i) {
+      if (features) memcpy(features + 12 * i, rec[i].first.f, 12 * sizeof(float));
+      if (latency_us) latency_us[i] = rec[i].second;
+    }
+    if (n_out) *n_out = (int)rec.size();
+  });
+}
+
+int bbx_dag_build(bbx_rt_t* rt, int policy, int tile_n, bbx_dag_t** out) {
+  if (!rt || !out) return bbx::set_error(BBX_ERR_INVALID, "null argument");
+  RT_TRY({
+    cudaError_t e = cudaStreamSynchronize(rt->rt.stream);
+    if (e != cudaSuccess) throw std::runtime_error(std::string("dag_build: ") + cudaGetErrorString(e));
+    auto* d = new bbx_dag();
+    try {
+      d->d = dag_build(&rt->rt, policy, tile_n);
+    } catch (...) {
+      delete d;
+      throw;
+    }
+    *out = d;
+  });
+}
+
+int bbx_dag_launch(bbx_dag_t* dag, void* stream) {
+  if (!dag) return bbx::set_error(BBX_ERR_INVALID, "null dag");
+  RT_TRY(dag_launch(dag->d, (cudaStream_t)stream));
+}
+
+int bbx_dag_destroy(bbx_dag_t* dag) {
+  if (!dag) return BBX_OK;
+  RT_TRY({
+    dag_destroy(dag->d);
+    delete dag;
+  });
+}
+
+int bbx_dag_stats(bbx_dag_t* dag, double* flops, double* bytes, int* waves, int* tc_launches,
+                  int* stream_launches, int* other_launches, size_t* arena_bytes) {
+  if (!dag) return bbx::set_error(BBX_ERR_INVALID, "null dag");
+  dag_stats_t s = dag_stats(dag->d);
+  if (flops) *flops = s.flops;
+  if (bytes) *bytes = s.bytes;
+  if (waves) *waves = s.waves;
+  if (tc_launches) *tc_launches = s.tc_launches;
+  if (stream_launches) *stream_launches = s.stream_launches;
+  if (other_launches) *other_launches = s.opaque_launches;
+  if (arena_bytes) *arena_bytes = s.arena_bytes;
+  return BBX_OK;
+}
+
+int bbx_dag_tensor(bbx_dag_t* dag, int tid, void** ptr, void* meta_out) {
+  if (!dag) return bbx::set_error(BBX_ERR_INVALID, "null dag");
+  tensor_meta_t m;
+  void* p = dag_tensor(dag->d, tid, &m);
+  if (!p && !meta_out) return bbx::set_error(BBX_ERR_NOT_FOUND, "DAG has no tensor %d", tid);
+  if (ptr) *ptr = p;
+  if (meta_out) memcpy(meta_out, &m, sizeof(m));
+  return p ? BBX_OK : bbx::set_error(BBX_ERR_NOT_FOUND, "DAG has no tensor %d", tid);
+}
+
+int bbx_dag_read(bbx_dag_t* dag, int tid, void* host_dst, size_t cap) {
+  if (!dag || !host_dst) return bbx::set_error(BBX_ERR_INVALID, "null argument");
+  tensor_meta_t m;
+  void* p = dag_tensor(dag->d, tid, &m);
+  if (!p) return bbx::set_error(BBX_ERR_NOT_FOUND, "DAG has no tensor %d", tid);
+  RT_TRY({
+    size_t n = std::min(cap, dag->d ? dag_payload_bytes(dag->d, tid) : 0);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(host_dst, p, n, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) throw std::runtime_error(std::string("dag_read: ") + cudaGetErrorString(e));
+  });
+}
+
+}  // extern "C"

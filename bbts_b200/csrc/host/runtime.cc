@@ -1,0 +1,366 @@
+// Runtime: block storage, per-op runner and the grouped DAG executor.
+#include "runtime.h"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <set>
+#include <stdexcept>
+
+namespace bbts {
+
+namespace {
+void cuda_ok(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+void bbx_ok(int rc) {
+  if (rc != 0) {
+    char buf[1024];
+    bbx_last_error(buf, sizeof(buf));
+    throw std::runtime_error(std::string("bbts_b200: ") + buf);
+  }
+}
+bool starts_with(const std::string& s, const char* p) { return s.rfind(p, 0) == 0; }
+}  // namespace
+
+// ------------------------------------------------------------------ storage
+block_storage_t::~block_storage_t() {
+  for (auto& kv : _blocks)
+    if (kv.second.owned && kv.second.payload) cudaFree(kv.second.payload);
+}
+
+tensor_t* block_storage_t::create(tid_t tid, const tensor_meta_t& meta) {
+  size_t bytes = _tf->get_payload_size(meta);
+  void* p = nullptr;
+  if (bytes) cuda_ok(cudaMallocAsync(&p, bytes, _st), "cudaMallocAsync(block)");
+  block_t b;
+  b.header.reset(new char[sizeof(tensor_meta_t)]);
+  std::memcpy(b.header.get(), &meta, sizeof(tensor_meta_t));
+  b.tensor()->_meta.set_payload(p);
+  b.payload = p;
+  b.bytes = bytes;
+  b.owned = true;
+  std::lock_guard<std::mutex> lk(_m);
+  auto it = _blocks.find(tid);
+  if (it != _blocks.end()) {
+    if (it->second.owned && it->second.payload) cudaFreeAsync(it->second.payload, _st);
+    _blocks.erase(it);
+  }
+  auto& slot = _blocks[tid];
+  slot = std::move(b);
+  return slot.tensor();
+}
+
+tensor_t* block_storage_t::create_view(tid_t tid, const tensor_meta_t& meta, void* payload, size_t bytes) {
+  block_t b;
+  b.header.reset(new char[sizeof(tensor_meta_t)]);
+  std::memcpy(b.header.get(), &meta, sizeof(tensor_meta_t));
+  b.tensor()->_meta.set_payload(payload);
+  b.payload = payload;
+  b.bytes = bytes;
+  b.owned = false;
+  std::lock_guard<std::mutex> lk(_m);
+  auto& slot = _blocks[tid];
+  if (slot.owned && slot.payload) cudaFreeAsync(slot.payload, _st);
+  slot = std::move(b);
+  return slot.tensor();
+}
+
+tensor_t* block_storage_t::get(tid_t tid) {
+  std::lock_guard<std::mutex> lk(_m);
+  auto it = _blocks.find(tid);
+  return it == _blocks.end() ? nullptr : it->second.tensor();
+}
+
+block_t* block_storage_t::block(tid_t tid) {
+  std::lock_guard<std::mutex> lk(_m);
+  auto it = _blocks.find(tid);
+  return it == _blocks.end() ? nullptr : &it->second;
+}
+
+bool block_storage_t::remove(tid_t tid) {
+  std::lock_guard<std::mutex> lk(_m);
+  auto it = _blocks.find(tid);
+  if (it == _blocks.end()) return false;
+  if (it->second.owned && it->second.payload) cudaFreeAsync(it->second.payload, _st);  // stream-ordered
+  _blocks.erase(it);
+  return true;
+}
+
+bool block_storage_t::assign_tid(tid_t from, tid_t to) {
+  std::lock_guard<std::mutex> lk(_m);
+  auto it = _blocks.find(from);
+  if (it == _blocks.end() || _blocks.count(to)) return false;
+  block_t b = std::move(it->second);
+  _blocks.erase(it);
+  _blocks[to] = std::move(b);
+  return true;
+}
+
+std::vector<tid_t> block_storage_t::tids() const {
+  std::vector<tid_t> out;
+  for (auto& kv : _blocks) out.push_back(kv.first);
+  return out;
+}
+
+// ------------------------------------------------------------------ runtime
+runtime_t::runtime_t() {
+  tf = std::make_shared<tensor_factory_t>();
+  register_b200_formats(*tf);
+  udm = std::make_shared<udf_manager_t>(tf);
+  register_b200_udfs(*udm);
+  cuda_ok(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  storage = std::make_unique<block_storage_t>(tf, stream);
+}
+
+runtime_t::~runtime_t() {
+  if (stream) cudaStreamSynchronize(stream);
+  storage.reset();
+  if (stream) cudaStreamDestroy(stream);
+}
+
+// The ud kinds the executor understands natively.
+node_kind_t classify(const ud_impl_t* impl, bool is_reduce) {
+  const std::string& n = impl->impl_name;
+  if (starts_with(n, "b200_dense_mult_bf16") || starts_with(n, "b200_dense_mult_e4m3")) return NK_TC;
+  if (n == "b200_dense_mult_f32") return NK_SIMT;
+  if (n == "b200_dense_add" || n == "b200_dense_bf16_add") return NK_SUM;
+  if (is_reduce) return NK_OPAQUE;
+  if (starts_with(n, "b200_dense_relu") || starts_with(n, "b200_dense_sigmoid")) return NK_UNARY;
+  if (starts_with(n, "b200_dense_hadamard") || starts_with(n, "b200_dense_weighted")) return NK_BINARY;
+  if (starts_with(n, "b200_contraction")) return NK_CONTRACT;
+  return NK_OPAQUE;
+}
+
+int elem_of(const tensor_factory_t& tf, tfid_t id) {
+  const std::string& n = tf.fmt_name(id);
+  if (n == "dense_bf16") return ELEM_BF16;
+  if (n == "dense_e4m3") return ELEM_E4M3;
+  return ELEM_F32;
+}
+
+op_features_t runtime_t::features(const command_t& cmd, size_t* hint_out) {
+  std::vector<tensor_meta_t> metas(cmd.get_num_inputs());
+  for (size_t i = 0; i < cmd.get_num_inputs(); ++i) {
+    tensor_t* t = storage->get(cmd.get_input(i).tid);
+    if (t) metas[i] = t->_meta;
+  }
+  return features_of(*tf, cmd, udm->get_fn_impl(cmd.fun_id), metas, hint_out);
+}
+
+// 12 features: op-kind one-hot (matmul, add, reduce, contraction), log2 m, n, k,
+// dtype (0 f32 / 1 bf16 / 2 e4m3), transpose flags, input count, log2 of the
+// elements touched.
+op_features_t features_of(const tensor_factory_t& tfac, const command_t& cmd, ud_impl_t* impl,
+                          std::vector<tensor_meta_t> metas, size_t* hint_out) {
+  const tensor_factory_t* tf = &tfac;
+  op_features_t f{};
+  ud_impl_t::meta_args_t margs(metas);
+  ud_impl_t::tensor_params_t params;
+  params._params = cmd.get_parameters();
+  node_kind_t k = impl ? classify(impl, cmd.is_reduce()) : NK_OPAQUE;
+  double m = 1, n = 1, kk = 1;
+  int ta = 0, tb = 0, dtype = 0;
+  if (impl && (k == NK_TC || k == NK_SIMT)) {
+    const auto& ma = metas[0].as<dense_tensor_meta_t>().m();
+    const auto& mb = metas[1].as<dense_tensor_meta_t>().m();
+    ta = params.get_bool_or_default<0>(false);
+    tb = params.get_bool_or_default<1>(false);
+    m = ta ? ma.num_cols : ma.num_rows;
+    kk = ta ? ma.num_rows : ma.num_cols;
+    n = tb ? mb.num_rows : mb.num_cols;
+    dtype = elem_of(*tf, metas[0].fmt_id);
+  } else if (impl && k == NK_CONTRACT) {
+    // lowered GEMM sizes: product of lhs-only+batch..., approximated by cube root split of the hint
+    size_t h = impl->get_complexity_hint(params, margs);
+    double c = std::cbrt((double)h);
+    m = n = kk = c;
+    dtype = impl->impl_name == "b200_contraction_bf16" ? 1 : 0;
+  } else if (!metas.empty()) {
+    const auto& ma = metas[0].as<dense_tensor_meta_t>().m();
+    m = ma.num_rows;
+    n = ma.num_cols;
+    dtype = elem_of(*tf, metas[0].fmt_id);
+  }
+  int kind_slot = (k == NK_TC || k == NK_SIMT) ? 0 : (k == NK_SUM && !cmd.is_reduce()) ? 1 : cmd.is_reduce() ? 2 : k == NK_CONTRACT ? 3 : 1;
+  f.f[kind_slot] = 1.f;
+  f.f[4] = (float)std::log2(std::max(1.0, m));
+  f.f[5] = (float)std::log2(std::max(1.0, n));
+  f.f[6] = (float)std::log2(std::max(1.0, kk));
+  f.f[7] = (float)dtype;
+  f.f[8] = (float)ta;
+  f.f[9] = (float)tb;
+  f.f[10] = (float)cmd.get_num_inputs();
+  f.f[11] = (float)std::log2(std::max(1.0, m * n * (double)std::max<size_t>(1, cmd.get_num_inputs())));
+  if (hint_out) *hint_out = impl ? impl->get_complexity_hint(params, margs) : 0;
+  return f;
+}
+
+// Executes one APPLY / REDUCE on the runtime stream (the per-op path).
+void execute_command(runtime_t& rt, command_t& cmd) {
+  ud_impl_t* impl = rt.udm->get_fn_impl(cmd.fun_id);
+  if (!impl) throw std::runtime_error("command " + std::to_string(cmd.id) + ": unknown ud impl");
+  ud_impl_t::tensor_params_t params;
+  params._params = cmd.get_parameters();
+  params.stream = rt.stream;
+  if (cmd.is_apply()) {
+    const size_t ni = cmd.get_num_inputs(), no = cmd.get_num_outputs();
+    std::vector<tensor_meta_t> in_meta(ni), out_meta(no);
+    ud_impl_t::tensor_args_t in_args(ni);
+    for (size_t i = 0; i < ni; ++i) {
+      tensor_t* t = rt.storage->get(cmd.get_input(i).tid);
+      if (!t) throw std::runtime_error("APPLY " + std::to_string(cmd.id) + ": input tensor missing");
+      in_meta[i] = t->_meta;
+      in_args.set(i, *t);
+    }
+    ud_impl_t::meta_args_t im(in_meta), om(out_meta);
+    for (size_t i = 0; i < no; ++i) std::memset(&out_meta[i], 0, sizeof(tensor_meta_t));
+    impl->get_out_meta(params, im, om);
+    ud_impl_t::tensor_args_t out_args(no);
+    for (size_t i = 0; i < no; ++i) {
+      out_meta[i].fmt_id = rt.tf->get_tensor_ftm(impl->outputTypes[i]);
+      tensor_t* t = rt.storage->create(cmd.get_output(i).tid, out_meta[i]);
+      out_args.set(i, *t);
+    }
+    impl->call_ud(params, in_args, out_args);
+  } else if (cmd.is_reduce()) {
+    // n-ary reduce: a native matrix_add reduce reads every input once in one
+    // launch; any other associative ud is folded pairwise left to right with
+    // a temporary per step, as local_reduce_op_t::apply does.
+    const size_t ni = cmd.get_num_inputs();
+    std::vector<tensor_t*> ins(ni);
+    for (size_t i = 0; i < ni; ++i) {
+      ins[i] = rt.storage->get(cmd.get_input(i).tid);
+      if (!ins[i]) throw std::runtime_error("REDUCE " + std::to_string(cmd.id) + ": input tensor missing");
+    }
+    tid_t out_tid = cmd.get_output(0).tid;
+    const tensor_meta_t& m0 = ins[0]->_meta;
+    if (impl->impl_name == "b200_dense_add" || impl->impl_name == "b200_dense_bf16_add") {
+      tensor_t* out = rt.storage->create(out_tid, m0);
+      const auto& dm = m0.as<dense_tensor_meta_t>().m();
+      const long long n = (long long)dm.num_rows * dm.num_cols;
+      const int dt = impl->impl_name == "b200_dense_add" ? BBX_F32 : BBX_BF16;
+      if (dt == BBX_F32) {
+        std::vector<const float*> ptrs(ni);
+        for (size_t i = 0; i < ni; ++i) ptrs[i] = (const float*)ins[i]->_meta.payload();
+        bbx_ok(bbx_reduce_f32(ptrs.data(), (int)ni, (float*)out->_meta.payload(), n, 1, rt.stream));
+      } else {
+        // bf16 blocks: chain grouped-stream sums of up to 16 inputs (f32 math)
+        std::vector<const void*> pend;
+        for (size_t i = 0; i < ni; ++i) pend.push_back(ins[i]->_meta.payload());
+        while (!pend.empty()) {
+          bbx_stream_op_t s{};
+          s.kind = BBX_S_SUM; s.in_dtype = BBX_BF16; s.out_dtype = BBX_BF16; s.kahan = 1; s.n = n;
+          int c = 0;
+          if (pend.size() != ni) s.in[c++] = out->_meta.payload();
+          while (c < BBX_STREAM_MAX_IN && !pend.empty()) { s.in[c++] = pend.front(); pend.erase(pend.begin()); }
+          s.n_in = c;
+          s.out = out->_meta.payload();
+          bbx_ok(bbx_stream_group(&s, 1, rt.stream));
+        }
+      }
+    } else {
+      tid_t tmp_base = -1000000000;
+      tensor_t* lhs = ins[0];
+      tid_t lhs_tid = cmd.get_input(0).tid;
+      for (size_t i = 1; i < ni; ++i) {
+        std::vector<tensor_meta_t> im{lhs->_meta, ins[i]->_meta}, om(1);
+        std::memset(&om[0], 0, sizeof(tensor_meta_t));
+        ud_impl_t::meta_args_t ima(im), oma(om);
+        impl->get_out_meta(params, ima, oma);
+        om[0].fmt_id = rt.tf->get_tensor_ftm(impl->outputTypes[0]);
+        tid_t t = (i + 1 == ni) ? out_tid : tmp_base - (tid_t)i;
+        tensor_t* o = rt.storage->create(t, om[0]);
+        ud_impl_t::tensor_args_t ia(std::vector<tensor_t*>{lhs, ins[i]}), oa(std::vector<tensor_t*>{o});
+        impl->call_ud(params, ia, oa);
+        if (i > 1) rt.storage->remove(lhs_tid);  // drop the previous intermediate
+        lhs = o;
+        lhs_tid = t;
+      }
+      if (ni == 1) {
+        tensor_t* o = rt.storage->create(out_tid, m0);
+        cuda_ok(cudaMemcpyAsync(o->_meta.payload(), m0.payload(), rt.tf->get_payload_size(m0),
+                                cudaMemcpyDeviceToDevice, rt.stream), "reduce copy");
+      }
+    }
+  }
+}
+
+void runtime_t::run_per_op(int policy, std::vector<std::pair<op_features_t, float>>* record) {
+  reservation_station_t rs(0, 1);
+  for (tid_t t : storage->tids()) rs.register_tensor(t);
+  std::unordered_map<command_id_t, double> prio;
+  if (policy == SCHED_LEARNED && predictor) {
+    // critical-path priority: predicted latency + the longest predicted path to a sink
+    std::unordered_map<tid_t, std::vector<size_t>> readers;
+    for (size_t i = 0; i < commands.size(); ++i)
+      for (size_t j = 0; j < commands[i]->get_num_inputs(); ++j) readers[commands[i]->get_input(j).tid].push_back(i);
+    std::vector<double> up(commands.size(), 0.0);
+    for (size_t ii = commands.size(); ii-- > 0;) {
+      auto& c = *commands[ii];
+      if (c.is_delete()) continue;
+      double best = 0;
+      for (size_t o = 0; o < c.get_num_outputs(); ++o)
+        for (size_t r : readers[c.get_output(o).tid]) best = std::max(best, up[r]);
+      // features need input metas; approximate with the complexity hint when inputs do not exist yet
+      size_t hint = 0;
+      op_features_t f{};
+      bool have_inputs = true;
+      for (size_t j = 0; j < c.get_num_inputs(); ++j) have_inputs = have_inputs && storage->get(c.get_input(j).tid);
+      double lat = 1.0;
+      if (have_inputs) { f = features(c, &hint); lat = predictor(f); }
+      up[ii] = lat + best;
+      prio[c.id] = up[ii];
+    }
+    rs.set_priority([&prio](const command_t& c) { auto it = prio.find(c.id); return it == prio.end() ? 0.0 : it->second; });
+  }
+  for (auto& c : commands) {
+    if (!rs.queue_command(c->clone())) throw std::runtime_error("reservation station rejected command " + std::to_string(c->id));
+  }
+  rs.execute_scheduled_async();
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evs;
+  std::vector<op_features_t> feats;
+  while (true) {
+    tid_t dead;
+    while (rs.try_get_to_remove(&dead)) {
+      storage->remove(dead);
+      rs.retire_remove(dead);
+    }
+    command_ptr_t cmd = rs.try_get_next_command();
+    if (!cmd) {
+      if (rs.num_to_retire() == 0) break;
+      throw std::runtime_error("DAG stalled: commands wait for tensors nothing produces");
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (record) {
+      size_t hint;
+      feats.push_back(features(*cmd, &hint));
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      cudaEventRecord(e0, stream);
+    }
+    execute_command(*this, *cmd);
+    if (record) {
+      cudaEventRecord(e1, stream);
+      evs.push_back({e0, e1});
+    }
+    rs.retire_command(std::move(cmd));
+  }
+  tid_t dead;
+  while (rs.try_get_to_remove(&dead)) {
+    storage->remove(dead);
+    rs.retire_remove(dead);
+  }
+  if (record) {
+    cuda_ok(cudaStreamSynchronize(stream), "run_per_op sync");
+    for (size_t i = 0; i < evs.size(); ++i) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, evs[i].first, evs[i].second);
+      record->push_back({feats[i], ms * 1000.f});
+      cudaEventDestroy(evs[i].first);
+      cudaEventDestroy(evs[i].second);
+    }
+  }
+}
+
+}  // namespace bbts

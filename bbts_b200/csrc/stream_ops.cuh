@@ -417,8 +417,30 @@ __device__ __forceinline__ float stream_eval(const StreamOp& o, const float* x) 
   }
 }
 
+constexpr int kStreamInline = 8;
+struct StreamInline {
+  StreamOp ops[kStreamInline];
+};
+
+template <typename TableT>
+__device__ __forceinline__ void stream_group_body(const TableT* __restrict__ table, int count,
+                                                  long long total_chunks);
+
+// Table in global memory (plans, replayed inside CUDA graphs).
 __global__ void __launch_bounds__(256) k_stream_group(const StreamOp* __restrict__ table, int count,
                                                       long long total_chunks) {
+  stream_group_body(table, count, total_chunks);
+}
+
+// Up to kStreamInline ops carried in the kernel parameters (one-shot calls).
+__global__ void __launch_bounds__(256) k_stream_group_inline(const __grid_constant__ StreamInline args,
+                                                             int count, long long total_chunks) {
+  stream_group_body(args.ops, count, total_chunks);
+}
+
+template <typename TableT>
+__device__ __forceinline__ void stream_group_body(const TableT* __restrict__ table, int count,
+                                                  long long total_chunks) {
   for (long long c = blockIdx.x; c < total_chunks; c += gridDim.x) {
     int lo = 0, hi = count - 1;
     while (lo < hi) {

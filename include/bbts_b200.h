@@ -201,6 +201,98 @@ int bbx_contraction(const float* lhs, int rank_l, const long long* dims_l, const
                     float* out, int rank_o, const int* modes_o, float alpha, int precision,
                     void* stream);
 
+/* ------------------------------------------------------------------ runtime
+ * A single-GPU runtime: the tensor factory + ud registry (with this library's
+ * B200 impls registered through the reference's register_tensors /
+ * register_udfs entry points), device-resident block storage, a command list,
+ * the reservation station and the executors.
+ * Tensor metas are the reference's 260-byte tensor_meta_t (4-byte format id +
+ * 256-byte blob, src/tensor/tensor.h:20-34); the last 8 blob bytes carry the
+ * payload's device address. */
+typedef struct bbx_rt bbx_rt_t;
+int bbx_rt_create(bbx_rt_t** out);
+int bbx_rt_destroy(bbx_rt_t* rt);
+/* stream every launch of this runtime is ordered on */
+int bbx_rt_stream(bbx_rt_t* rt, void** stream_out);
+/* tensor_factory_t::get_tensor_ftm (src/tensor/tensor_factory.cc:60-68); -1 if unknown */
+int bbx_rt_fmt_id(bbx_rt_t* rt, const char* fmt_name);
+/* udf_manager_t::get_matcher_for + udf_matcher::findMatch
+ * (src/ud_functions/udf_manager.cc:10-37,114-125) with REAL type matching;
+ * type lists are comma separated, e.g. "dense,dense". */
+int bbx_rt_find_impl(bbx_rt_t* rt, const char* ud_name, const char* in_types, const char* out_types,
+                     int require_gpu, int* ud_id, int* impl_id);
+int bbx_rt_impl_name(bbx_rt_t* rt, int ud_id, int impl_id, char* buf, size_t len);
+/* complexity hint of an impl on the given input metas (get_complexity_hint) */
+int bbx_rt_complexity(bbx_rt_t* rt, int ud_id, int impl_id, const uint32_t* params, int n_params,
+                      const void* in_metas, int n_in, unsigned long long* hint);
+/* Creates / replaces tensor `tid` from a 260-byte meta and `bytes` of payload
+ * (src on the host, or on the device when src_on_device). */
+int bbx_rt_tensor_put(bbx_rt_t* rt, int tid, const void* meta, const void* src, size_t bytes,
+                      int src_on_device);
+/* Copies tensor `tid`'s meta (260 bytes) and up to `cap` payload bytes out. */
+int bbx_rt_tensor_get(bbx_rt_t* rt, int tid, void* meta_out, void* dst, size_t cap, int dst_on_device);
+int bbx_rt_tensor_payload(bbx_rt_t* rt, int tid, void** ptr, size_t* bytes);
+int bbx_rt_tensor_count(bbx_rt_t* rt);
+int bbx_rt_tensor_remove(bbx_rt_t* rt, int tid);
+/* command_t::create_apply / create_reduce / create_delete (src/commands/command.h:228-457);
+ * params are the raw 4-byte command_param_t words. Commands are appended to the
+ * runtime's command list in increasing id order. */
+int bbx_rt_queue_apply(bbx_rt_t* rt, int cmd_id, int ud_id, int impl_id, const uint32_t* params,
+                       int n_params, const int* in_tids, int n_in, const int* out_tids, int n_out);
+int bbx_rt_queue_reduce(bbx_rt_t* rt, int cmd_id, int ud_id, int impl_id, const uint32_t* params,
+                        int n_params, const int* in_tids, int n_in, int out_tid);
+int bbx_rt_queue_delete(bbx_rt_t* rt, int cmd_id, const int* tids, int n);
+int bbx_rt_clear_commands(bbx_rt_t* rt);
+int bbx_rt_num_commands(bbx_rt_t* rt);
+/* The per-op path: the command list runs through the reservation station
+ * (LIFO, or learned priority with policy 1) with one stream-ordered launch per
+ * command, like command_runner_t::local_command_runner
+ * (src/commands/command_runner.cc:18-259). Synchronous. */
+int bbx_rt_run(bbx_rt_t* rt, int policy);
+/* Same, recording each command's (12 features, latency in us) as training data
+ * for the cost model; returns the number of records in *n_out. */
+int bbx_rt_record(bbx_rt_t* rt, int policy, float* features, float* latency_us, int cap, int* n_out);
+
+#define BBX_SCHED_HEURISTIC 0
+#define BBX_SCHED_LEARNED 1
+/* The grouped path: lower the command list into waves of grouped launches with
+ * a static arena, captured in one CUDA graph. No reference counterpart (the
+ * reference issues one call per command). */
+typedef struct bbx_dag bbx_dag_t;
+int bbx_dag_build(bbx_rt_t* rt, int policy, int tile_n, bbx_dag_t** out);
+int bbx_dag_launch(bbx_dag_t* dag, void* stream);
+int bbx_dag_destroy(bbx_dag_t* dag);
+int bbx_dag_stats(bbx_dag_t* dag, double* flops, double* bytes, int* waves, int* tc_launches,
+                  int* stream_launches, int* other_launches, size_t* arena_bytes);
+/* device address and meta of a tensor the DAG reads or produces */
+int bbx_dag_tensor(bbx_dag_t* dag, int tid, void** ptr, void* meta_out);
+/* copies up to `cap` payload bytes of a DAG tensor to host memory (synchronous) */
+int bbx_dag_read(bbx_dag_t* dag, int tid, void* host_dst, size_t cap);
+
+/* ------------------------------------------------------------------ learned cost model
+ * MLP 12 -> 128 -> 128 -> 128 -> 1 (ReLU, FP32) predicting log latency from op
+ * features; trained and evaluated on the GPU by this library's kernels. */
+typedef struct bbx_mlp bbx_mlp_t;
+#define BBX_MLP_IN 12
+#define BBX_MLP_HIDDEN 128
+int bbx_mlp_create(unsigned long long seed, bbx_mlp_t** out);
+int bbx_mlp_destroy(bbx_mlp_t* mlp);
+/* standardisation of the inputs (per-feature mean / std), applied inside */
+int bbx_mlp_set_norm(bbx_mlp_t* mlp, const float* mean, const float* std);
+/* Adam on MSE; x host (n x 12), y host (n) = log latency. Returns final loss. */
+int bbx_mlp_train(bbx_mlp_t* mlp, const float* x, const float* y, int n, int epochs, int batch,
+                  float lr, float* loss_out);
+int bbx_mlp_predict(bbx_mlp_t* mlp, const float* x, int n, float* y_out);
+/* loss and all gradients for one batch (for gradient checks); grads laid out
+ * as W1,b1,W2,b2,W3,b3,W4,b4 (Wi row-major in x out) */
+int bbx_mlp_loss_grad(bbx_mlp_t* mlp, const float* x, const float* y, int n, float* loss,
+                      float* grads);
+int bbx_mlp_num_params(void);
+int bbx_mlp_get_params(bbx_mlp_t* mlp, float* out);
+int bbx_mlp_set_params(bbx_mlp_t* mlp, const float* in);
+/* install the MLP as the runtime's latency predictor (policy BBX_SCHED_LEARNED) */
+int bbx_rt_set_predictor(bbx_rt_t* rt, bbx_mlp_t* mlp);
+
 #ifdef __cplusplus
 }
 #endif

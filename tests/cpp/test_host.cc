@@ -1,0 +1,245 @@
+// Host-side tests of the runtime's C++ layer, no GPU needed: tensor factory,
+// ud registry with real type matching, command records, reservation station.
+// Modelled on the reference's tests/test_builtin_dense.cc,
+// tests/test_builtin_ud.cc, tests/test_parsed_command.cc and
+// tests/test_reservation_station.cc (FewLocalCommands*, the deferred-delete
+// scenarios). Built and run by tests/test_host_cpp.py.
+#include <algorithm>
+#include <atomic>
+#include <mutex>
+#include <cstdio>
+#include <cstdlib>
+#include <set>
+#include <thread>
+#include "command.h"
+#include "reservation_station.h"
+#include "tensor.h"
+#include "ud_function.h"
+
+using namespace bbts;
+
+static int g_fail = 0;
+#define EXPECT(c)                                                              \
+  do {                                                                         \
+    if (!(c)) {                                                                \
+      std::printf("FAIL %s:%d: %s\n", __FILE__, __LINE__, #c);                 \
+      ++g_fail;                                                                \
+    }                                                                          \
+  } while (0)
+
+struct fake_impl : ud_impl_t {
+  fake_impl(const char* ud, const char* name, std::vector<std::string> in, std::vector<std::string> out, bool gpu) {
+    ud_name = ud;
+    impl_name = name;
+    inputTypes = std::move(in);
+    outputTypes = std::move(out);
+    is_gpu = gpu;
+    fn = [](const tensor_params_t&, const tensor_args_t&, tensor_args_t&) {};
+  }
+  size_t get_complexity_hint(const tensor_params_t&, const meta_args_t&) override { return 1; }
+  void get_out_meta(const tensor_params_t&, const meta_args_t&, meta_args_t&) const override {}
+};
+
+static void test_dense_format() {
+  tensor_factory_t tf;
+  tfid_t id = tf.get_tensor_ftm("dense");
+  EXPECT(id == 0);
+  EXPECT(tf.get_tensor_ftm("nope") == -1);
+  dense_tensor_meta_t m(id, 100, 200);
+  // builtin_formats.cc:18-21: header + rows*cols*4
+  EXPECT(tf.get_tensor_size(m) == sizeof(tensor_meta_t) + 100 * 200 * 4);
+  EXPECT(sizeof(tensor_meta_t) == 260);
+  // reference layout on the host: payload right after the header
+  std::vector<char> mem(tf.get_tensor_size(m));
+  auto& t = tf.init_tensor((tensor_t*)mem.data(), m).as<dense_tensor_t>();
+  EXPECT((char*)t.data() == mem.data() + sizeof(tensor_meta_t));
+  EXPECT(t.meta().m().num_rows == 100 && t.meta().m().num_cols == 200);
+  // register_fmt returns the new id, and the first one on re-registration
+  tfid_t f2 = tf.register_fmt("ffnn_dense", ffnn_dense_creation_fs());
+  EXPECT(f2 == tf.get_tensor_ftm("ffnn_dense"));
+  EXPECT(tf.register_fmt("ffnn_dense", ffnn_dense_creation_fs()) == f2);
+  ffnn_dense_meta_t fm(f2, true, 10, 20);
+  EXPECT(tf.get_tensor_size(fm) == sizeof(tensor_meta_t) + (10 * 20 + 20) * 4);
+  tfid_t bf = tf.get_tensor_ftm("dense_bf16");
+  dense_tensor_meta_t mb(bf, 64, 32);
+  EXPECT(tf.get_payload_size(mb) == 64 * 32 * 2);
+}
+
+static void test_matcher_types() {
+  auto tf = std::make_shared<tensor_factory_t>();
+  udf_manager_t udm(tf);
+  auto f = std::make_unique<ud_func_t>();
+  f->ud_name = "matrix_add";
+  f->is_ass = f->is_com = true;
+  f->num_in = 2;
+  f->num_out = 1;
+  EXPECT(udm.register_udf(std::move(f)) == 0);
+  auto dup = std::make_unique<ud_func_t>();
+  dup->ud_name = "matrix_add";
+  EXPECT(udm.register_udf(std::move(dup)) == -1);
+  auto a = udm.register_udf_impl(std::make_unique<fake_impl>("matrix_add", "cpu_dense", std::vector<std::string>{"dense", "dense"}, std::vector<std::string>{"dense"}, false));
+  auto b = udm.register_udf_impl(std::make_unique<fake_impl>("matrix_add", "gpu_bf16", std::vector<std::string>{"dense_bf16", "dense_bf16"}, std::vector<std::string>{"dense_bf16"}, true));
+  auto c = udm.register_udf_impl(std::make_unique<fake_impl>("matrix_add", "gpu_dense", std::vector<std::string>{"dense", "dense"}, std::vector<std::string>{"dense"}, true));
+  EXPECT(a.impl_id == 0 && b.impl_id == 1 && c.impl_id == 2);
+  // wrong arity is refused
+  auto bad = udm.register_udf_impl(std::make_unique<fake_impl>("matrix_add", "bad", std::vector<std::string>{"dense"}, std::vector<std::string>{"dense"}, true));
+  EXPECT(bad.ud_id == -1);
+  auto m = udm.get_matcher_for("matrix_add");
+  EXPECT(m != nullptr);
+  // the reference's matcher returns the first GPU impl regardless of types; here types decide
+  ud_impl_t* g = m->findMatch({"dense", "dense"}, {"dense"}, true);
+  EXPECT(g && g->impl_name == "gpu_dense");
+  ud_impl_t* h = m->findMatch({"dense_bf16", "dense_bf16"}, {"dense_bf16"}, true);
+  EXPECT(h && h->impl_name == "gpu_bf16");
+  EXPECT(m->findMatch({"dense", "dense_bf16"}, {"dense"}, true) == nullptr);
+  EXPECT(m->findMatch({"dense", "dense"}, {"dense"}, false)->impl_name == "cpu_dense");
+  EXPECT(udm.get_matcher_for("nope") == nullptr);
+  EXPECT(udm.get_matcher_for("matrix_add", true, true) != nullptr);
+  EXPECT(udm.get_fn_impl({0, 2})->impl_name == "gpu_dense");
+  EXPECT(udm.get_fn_impl({0, 9}) == nullptr);
+}
+
+static void test_command_layout() {
+  std::vector<command_param_t> p(3);
+  p[0].i = 7;
+  p[1].f = 2.5f;
+  p[2].b = true;
+  auto c = command_t::create_apply(5, {1, 2}, true, p, {{10, 0}, {11, 0}}, {{12, 0}});
+  EXPECT(c->id == 5 && c->is_apply() && c->get_num_inputs() == 2 && c->get_num_outputs() == 1);
+  EXPECT(c->get_input(1).tid == 11 && c->get_output(0).tid == 12);
+  EXPECT(c->get_parameters()[1].f == 2.5f && c->get_parameters()[0].i == 7);
+  auto d = c->clone();  // flat, memcpy-able (command.h:459-542)
+  EXPECT(d->num_bytes() == c->num_bytes() && d->get_input(0).tid == 10 && d->get_parameters()[2].b);
+  auto r = command_t::create_reduce(6, {0, 0}, true, {}, {{1, 0}, {2, 0}, {3, 0}}, {4, 0});
+  EXPECT(r->is_reduce() && r->is_local_reduce(0) && !r->is_local_reduce(1) && r->get_num_inputs() == 3);
+  auto del = command_t::create_delete(7, {{1, 0}, {2, 0}});
+  EXPECT(del->is_delete() && del->get_num_outputs() == 0);
+  auto mv = command_t::create_move(8, {3, 0}, {3, 1});
+  EXPECT(mv->is_move() && mv->get_nodes().size() == 2);
+}
+
+// APPLY a, b -> c ; APPLY c -> d ; DELETE a, b, c : readiness, LIFO order and deferred deletes
+static void test_reservation_station_basic() {
+  reservation_station_t rs(0, 1);
+  std::vector<command_id_t> scheduled, retired;
+  rs.add_scheduled_hook([&](command_id_t id) { scheduled.push_back(id); });
+  rs.add_retired_hook([&](command_id_t id) { retired.push_back(id); });
+  rs.register_tensor(0);
+  rs.register_tensor(1);
+  EXPECT(rs.queue_command(command_t::create_apply(0, {0, 0}, true, {}, {{0, 0}, {1, 0}}, {{2, 0}})));
+  EXPECT(rs.queue_command(command_t::create_apply(1, {0, 0}, true, {}, {{2, 0}}, {{3, 0}})));
+  EXPECT(rs.queue_command(command_t::create_delete(2, {{0, 0}, {1, 0}, {2, 0}})));
+  EXPECT(!rs.queue_command(command_t::create_apply(1, {0, 0}, true, {}, {{0, 0}}, {{9, 0}})));  // id order
+  rs.execute_scheduled_async();
+  auto c0 = rs.try_get_next_command();
+  EXPECT(c0 && c0->id == 0);
+  EXPECT(rs.try_get_next_command() == nullptr);  // command 1 waits for tensor 2
+  tid_t t;
+  EXPECT(!rs.try_get_to_remove(&t));             // a, b still have a reader
+  rs.retire_command(std::move(c0));
+  std::set<tid_t> removed;
+  while (rs.try_get_to_remove(&t)) { removed.insert(t); rs.retire_remove(t); }
+  EXPECT(removed == std::set<tid_t>({0, 1}));   // deleted as soon as their reader retired
+  auto c1 = rs.try_get_next_command();
+  EXPECT(c1 && c1->id == 1);
+  rs.retire_command(std::move(c1));
+  while (rs.try_get_to_remove(&t)) { removed.insert(t); rs.retire_remove(t); }
+  EXPECT(removed.count(2) == 1);
+  EXPECT(rs.num_to_retire() == 0);
+  rs.wait_until_finished();
+  EXPECT(scheduled == std::vector<command_id_t>({0, 1}));
+  EXPECT(retired == std::vector<command_id_t>({0, 1}));
+}
+
+// Ready commands pop LIFO (reservation_station.cc:213-214), or by priority when installed.
+static void test_reservation_station_order() {
+  for (int prio = 0; prio < 2; ++prio) {
+    reservation_station_t rs(0, 1);
+    rs.register_tensor(0);
+    for (int i = 0; i < 5; ++i)
+      rs.queue_command(command_t::create_apply(i, {0, 0}, true, {}, {{0, 0}}, {{100 + i, 0}}));
+    if (prio) rs.set_priority([](const command_t& c) { return (double)((c.id * 3) % 5); });
+    rs.execute_scheduled_async();
+    std::vector<command_id_t> order;
+    while (auto c = rs.try_get_next_command()) {
+      order.push_back(c->id);
+      rs.retire_command(std::move(c));
+    }
+    if (!prio) EXPECT(order == std::vector<command_id_t>({4, 3, 2, 1, 0}));
+    else EXPECT(order == std::vector<command_id_t>({3, 1, 4, 2, 0}));  // priorities 4,3,2,1,0
+  }
+}
+
+// A delete queued before the readers of a not-yet-created tensor waits for them;
+// reading a tensor after its delete was queued is refused.
+static void test_reservation_station_delete_rules() {
+  reservation_station_t rs(0, 1);
+  rs.register_tensor(0);
+  EXPECT(rs.queue_command(command_t::create_apply(0, {0, 0}, true, {}, {{0, 0}}, {{1, 0}})));
+  EXPECT(rs.queue_command(command_t::create_delete(1, {{1, 0}})));
+  EXPECT(!rs.queue_command(command_t::create_apply(2, {0, 0}, true, {}, {{1, 0}}, {{2, 0}})));
+  rs.execute_scheduled_async();
+  auto c = rs.try_get_next_command();
+  tid_t t;
+  EXPECT(!rs.try_get_to_remove(&t));
+  rs.retire_command(std::move(c));
+  EXPECT(rs.try_get_to_remove(&t) && t == 1);  // created with no readers and scheduled: dropped
+  rs.retire_remove(t);
+}
+
+// A diamond of 100 commands run by 4 worker threads; every tensor is deleted
+// exactly once and every command retires (the shape of the reference's
+// threaded reservation-station scenarios).
+static void test_reservation_station_threads() {
+  reservation_station_t rs(0, 1);
+  rs.register_tensor(0);
+  const int N = 100;
+  int id = 0;
+  for (int i = 0; i < N; ++i)
+    rs.queue_command(command_t::create_apply(id++, {0, 0}, true, {}, {{0, 0}}, {{1 + i, 0}}));
+  std::vector<command_t::tid_node_id_t> ins;
+  for (int i = 0; i < N; ++i) ins.push_back({1 + i, 0});
+  rs.queue_command(command_t::create_reduce(id++, {0, 0}, true, {}, ins, {1000, 0}));
+  rs.queue_command(command_t::create_delete(id++, ins));
+  std::atomic<int> executed{0};
+  std::mutex rm_mu;
+  std::set<tid_t> removed;
+  rs.execute_scheduled_async();
+  std::vector<std::thread> th;
+  for (int w = 0; w < 4; ++w)
+    th.emplace_back([&] {
+      while (auto c = rs.get_next_command()) {
+        ++executed;
+        rs.retire_command(std::move(c));
+      }
+    });
+  std::thread deleter([&] {
+    tid_t t;
+    while ((t = rs.get_to_remove()) != -1) {
+      { std::lock_guard<std::mutex> lk(rm_mu); removed.insert(t); }
+      rs.retire_remove(t);
+    }
+  });
+  rs.wait_until_finished();
+  rs.shutdown();
+  for (auto& x : th) x.join();
+  deleter.join();
+  EXPECT(executed == N + 1);
+  EXPECT((int)removed.size() == N);
+}
+
+int main() {
+  test_dense_format();
+  test_matcher_types();
+  test_command_layout();
+  test_reservation_station_basic();
+  test_reservation_station_order();
+  test_reservation_station_delete_rules();
+  test_reservation_station_threads();
+  if (g_fail) {
+    std::printf("%d failure(s)\n", g_fail);
+    return 1;
+  }
+  std::printf("all host tests passed\n");
+  return 0;
+}

@@ -1,0 +1,279 @@
+"""The native runtime on the GPU: ud registry + per-op path + grouped DAG path +
+learned cost model, checked against the CPU oracle."""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import golden, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def R(cuda):
+    from bbts_b200 import runtime, workloads
+    return runtime, workloads
+
+
+def bf16_round(x):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(x, np.float32)).to(torch.bfloat16).float().numpy()
+
+
+def read_dense(rt, tid, dag=None):
+    """f32 / bf16 dense block back to the host as float32 (from the runtime or a DAG)."""
+    import torch
+    from bbts_b200.runtime import parse_meta
+    if dag is not None:
+        _, meta = dag.tensor(tid)
+        m = parse_meta(meta)
+        name = {rt.fmt("dense"): "f32", rt.fmt("dense_bf16"): "bf16"}[m["fmt_id"]]
+        buf = dag.read_bytes(tid, m["rows"] * m["cols"] * (4 if name == "f32" else 2))
+    else:
+        m = parse_meta(rt.meta(tid))
+        name = {rt.fmt("dense"): "f32", rt.fmt("dense_bf16"): "bf16"}[m["fmt_id"]]
+        buf = rt.get_bytes(tid)
+    if name == "f32":
+        return buf.view(np.float32).reshape(m["rows"], m["cols"])
+    return torch.from_numpy(buf.view(np.int16).copy()).view(torch.bfloat16).float().numpy().reshape(m["rows"], m["cols"])
+
+
+# ------------------------------------------------------------------ ud API
+def test_matrix_add_ud_known_answer(R):
+    # tests/test_builtin_ud_gpu.cu:16-124 of the reference, through the ud registry
+    runtime, _ = R
+    rt = runtime.Runtime()
+    impl = rt.impl("matrix_add", ["dense", "dense"], ["dense"], gpu=True)
+    assert rt.impl_name(impl) == "b200_dense_add"
+    g = golden("add_kat.npz")
+    rt.put_dense(0, g["a"])
+    rt.put_dense(1, g["b"])
+    rt.apply(impl, [0, 1], [2])
+    rt.run()
+    out = rt.get_dense(2)
+    assert out.shape == (100, 200)
+    assert np.max(np.abs(out - g["expect"])) <= 1e-4
+    # the inputs are untouched
+    assert np.array_equal(rt.get_dense(1), g["b"])
+
+
+def test_type_matching_picks_the_format(R):
+    runtime, _ = R
+    rt = runtime.Runtime()
+    assert rt.impl_name(rt.impl("matrix_mult", ["dense", "dense"], ["dense"])) == "b200_dense_mult_f32"
+    assert rt.impl_name(rt.impl("matrix_mult", ["dense_bf16", "dense_bf16"], ["dense"])) == "b200_dense_mult_bf16"
+    assert rt.impl_name(rt.impl("matrix_mult", ["dense_bf16", "dense_bf16"], ["dense_bf16"])) == "b200_dense_mult_bf16_out_bf16"
+    with pytest.raises(Exception):
+        rt.impl("matrix_mult", ["dense", "dense_bf16"], ["dense"])
+
+
+@pytest.mark.parametrize("ta,tb", [(0, 0), (1, 0), (0, 1), (1, 1)])
+def test_matrix_mult_transpose_params(R, ta, tb):
+    runtime, _ = R
+    rt = runtime.Runtime()
+    rng = np.random.default_rng(ta * 2 + tb)
+    a = rng.standard_normal((192, 256)).astype(np.float32)
+    b = rng.standard_normal((256, 192)).astype(np.float32)
+    rt.put_dense(0, a)
+    rt.put_dense(1, b)
+    rt.apply(rt.impl("matrix_mult", ["dense", "dense"], ["dense"]), [0, 1], [2], params=[bool(ta), bool(tb)])
+    rt.run()
+    ref = oracle.matmul_f64(a, b, bool(ta), bool(tb))
+    assert rel_err(rt.get_dense(2), ref) <= 1e-5
+
+
+# ------------------------------------------------------------------ blocked matmul (config-1 shape)
+def _bmm_ref(info):
+    split = info["split"]
+    A = np.block([[info["hostA"][(i, j)] for j in range(split)] for i in range(split)])
+    B = np.block([[info["hostB"][(i, j)] for j in range(split)] for i in range(split)])
+    return A, B
+
+
+def test_bmm_per_op_f32_vs_f64(R):
+    runtime, workloads = R
+    rt = runtime.Runtime()
+    info = workloads.bmm(rt, n=1024, split=4, dtype="f32", seed=1)
+    n_inputs = rt.count()
+    rt.run()
+    A, B = _bmm_ref(info)
+    ref = oracle.matmul_f64(A, B)
+    bs = info["bs"]
+    for (i, j), t in info["C"].items():
+        assert rel_err(rt.get_dense(t), ref[i * bs:(i + 1) * bs, j * bs:(j + 1) * bs]) <= 1e-5
+    # the 64 partial products were deleted after their reduce retired
+    assert rt.count() == n_inputs + 16
+
+
+@pytest.mark.parametrize("dtype", ["f32", "bf16"])
+@pytest.mark.parametrize("policy", [0, 1])
+def test_bmm_dag_vs_f64(R, dtype, policy):
+    runtime, workloads = R
+    rt = runtime.Runtime()
+    info = workloads.bmm(rt, n=1024, split=4, dtype=dtype, seed=2)
+    dag = rt.build_dag(policy)
+    st = dag.stats()
+    assert st["waves"] == 2 and st["flops"] == info["flops"]
+    A, B = _bmm_ref(info)
+    if dtype == "bf16":
+        ref_q = oracle.matmul_f64(bf16_round(A), bf16_round(B))
+    ref = oracle.matmul_f64(A, B)
+    bs = info["bs"]
+    first = {}
+    for rep in range(2):
+        dag.launch()
+        for (i, j), t in info["C"].items():
+            got = read_dense(rt, t, dag)
+            blk = (slice(i * bs, (i + 1) * bs), slice(j * bs, (j + 1) * bs))
+            if dtype == "f32":
+                assert rel_err(got, ref[blk]) <= 1e-5
+            else:
+                assert rel_err(got, ref_q[blk]) <= 1e-5      # accumulation error only
+                assert rel_err(got, ref[blk]) <= 1e-2        # the bf16 budget vs FP64
+            if rep == 0:
+                first[t] = got.copy()
+            else:
+                assert np.array_equal(first[t], got)          # graph replay is deterministic
+    dag.close()
+
+
+# ------------------------------------------------------------------ random DAGs
+def _small_dag(workloads, rt, dtype, seed, with_contraction):
+    mix = (0.6, 0.15, 0.15, 0.10) if with_contraction else (0.6, 0.2, 0.2, 0.0)
+    return workloads.random_dag(rt, n_ops=48, depth=4, seed=seed, dtype=dtype, lo=128, hi=384, step=64,
+                                contraction_dims=(16, 48), mix=mix, host=True, max_inputs=6)
+
+
+def _host_eval(info, dtype):
+    vals = {}
+    for t, x in info["host_inputs"].items():
+        if x.ndim == 2:
+            vals[t] = (bf16_round(x) if dtype == "bf16" else x).astype(np.float64)
+    for kind, ins, out in info["ops"]:
+        if kind == 0:
+            vals[out] = vals[ins[0]] @ vals[ins[1]]
+        elif kind in (1, 2):
+            vals[out] = sum(vals[t] for t in ins)
+    return vals
+
+
+@pytest.mark.parametrize("dtype,tol", [("f32", 1e-5), ("bf16", 3e-2)])
+@pytest.mark.parametrize("path", ["per_op", "dag_heuristic", "dag_learned"])
+def test_random_dag_vs_f64(R, dtype, tol, path):
+    runtime, workloads = R
+    rt = runtime.Runtime()
+    info = _small_dag(workloads, rt, dtype, seed=5, with_contraction=False)
+    ref = _host_eval(info, dtype)
+    dag = None
+    if path == "per_op":
+        rt.run()
+    else:
+        if path == "dag_learned":
+            mlp = runtime.Mlp(seed=3)  # untrained predictor: the schedule changes, results must not
+            rt.set_predictor(mlp)
+        dag = rt.build_dag(runtime.LEARNED if path == "dag_learned" else runtime.HEURISTIC)
+        dag.launch()
+    for t in info["finals"]:
+        got = read_dense(rt, t, dag)
+        assert rel_err(got, ref[t]) <= tol, (t, rel_err(got, ref[t]))
+
+
+def test_random_dag_with_contractions_dag_equals_per_op(R):
+    runtime, workloads = R
+    rt1 = runtime.Runtime()
+    info = _small_dag(workloads, rt1, "f32", seed=9, with_contraction=True)
+    rt1.run()
+    rt2 = runtime.Runtime()
+    info2 = _small_dag(workloads, rt2, "f32", seed=9, with_contraction=True)
+    dag = rt2.build_dag(runtime.HEURISTIC)
+    dag.launch()
+    assert info["finals"] == info2["finals"]
+    for t in info["finals"]:
+        a = rt1.get_bytes(t).view(np.float32)
+        b = dag.read_bytes(t, a.nbytes).view(np.float32)
+        assert rel_err(b, a) <= 1e-5
+
+
+# ------------------------------------------------------------------ FNN and contraction uds
+def test_ffnn_uds(R):
+    runtime, _ = R
+    rt = runtime.Runtime()
+    f = rt.fmt("ffnn_dense")
+    rng = np.random.default_rng(0)
+    X = rng.standard_normal((96, 64)).astype(np.float32)
+    W = rng.standard_normal((64, 80)).astype(np.float32)
+    bias = rng.standard_normal(80).astype(np.float32)
+    rt.put(0, runtime.ffnn_meta(f, 96, 64, False), X)
+    rt.put(1, runtime.ffnn_meta(f, 64, 80, True), np.concatenate([W.ravel(), bias]))
+    rt.apply(rt.impl("ffnn_act_mult", ["ffnn_dense", "ffnn_dense"], ["ffnn_dense"]), [0, 1], [2])
+    rt.apply(rt.impl("ffnn_relu", ["ffnn_dense"], ["ffnn_dense"]), [2], [3])
+    G = rng.standard_normal((96, 80)).astype(np.float32)
+    rt.put(4, runtime.ffnn_meta(f, 96, 80, False), G)
+    rt.apply(rt.impl("ffnn_back_mult", ["ffnn_dense", "ffnn_dense"], ["ffnn_dense"]), [0, 4], [5])
+    labels = rng.integers(0, 80, 96).astype(np.int32)
+    rt.put(6, runtime.dense_meta(rt.fmt("labels"), 96, 1), labels)
+    rt.apply(rt.impl("ffnn_softmax_ce", ["ffnn_dense", "labels"], ["ffnn_dense", "ffnn_dense"]), [2, 6], [7, 8],
+             params=[1.0 / 96])
+    rt.run()
+    z = oracle.matmul_f64(X, W) + bias
+    got_z = rt.get_bytes(2).view(np.float32).reshape(96, 80)
+    assert rel_err(got_z, z) <= 1e-5
+    assert np.array_equal(rt.get_bytes(3).view(np.float32).reshape(96, 80), np.maximum(got_z, 0))
+    bw = rt.get_bytes(5).view(np.float32)
+    assert rel_err(bw[:64 * 80].reshape(64, 80), oracle.matmul_f64(X, G, trans_a=True)) <= 1e-5
+    assert np.array_equal(bw[64 * 80:], oracle.colsum(G))  # bias = column sums, zero-initialised
+    loss, grad = oracle.softmax_ce_f64(got_z, labels, grad_scale=1.0 / 96)
+    assert rel_err(rt.get_bytes(8).view(np.float32), loss) <= 1e-5
+    assert rel_err(rt.get_bytes(7).view(np.float32).reshape(96, 80), grad) <= 1e-5
+
+
+@pytest.mark.parametrize("impl_name", ["b200_contraction", "b200_contraction_bf16"])
+def test_contraction_ud(R, impl_name):
+    runtime, _ = R
+    rt = runtime.Runtime()
+    g = golden("contraction_int.npz")
+    I, J, K, L = [int(v) for v in g["c1_dims"]]
+    cf = rt.fmt("cutensor")
+    rt.put(0, runtime.cutensor_meta(cf, [I, J, K]), g["c1_lhs"])
+    rt.put(1, runtime.cutensor_meta(cf, [K, L]), g["c1_rhs"])
+    impl = rt.impl_named("contraction", impl_name)
+    rt.apply(impl, [0, 1], [2], params=[3, 2, 3, 0, 1, 2, 2, 3, 0, 1, 3, 1.0])
+    rt.run()
+    assert np.array_equal(rt.get_bytes(2).view(np.float32), g["c1_out"])
+
+
+# ------------------------------------------------------------------ learned cost model
+def test_mlp_gradients_match_oracle(R):
+    runtime, _ = R
+    import oracle.mlp as om
+    mlp = runtime.Mlp(seed=11)
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal((64, 12)).astype(np.float32)
+    y = rng.standard_normal(64).astype(np.float32)
+    p = mlp.get_params()
+    loss, g = mlp.loss_grad(x, y)
+    loss64, g64 = om.loss_grad(p.astype(np.float64), x, y)
+    assert abs(loss - loss64) <= 1e-5 * max(1.0, abs(loss64))
+    assert rel_err(g, g64) <= 1e-4
+    # and the finite-difference slope of the FP64 oracle agrees with its analytic gradient
+    i = int(np.argmax(np.abs(g64)))
+    e = np.zeros_like(g64); e[i] = 1e-6
+    fd = (om.loss_grad(p + e, x, y)[0] - om.loss_grad(p - e, x, y)[0]) / 2e-6
+    assert abs(fd - g64[i]) <= 1e-4 * max(1.0, abs(g64[i]))
+
+
+def test_mlp_training_fits(R):
+    runtime, _ = R
+    import oracle.mlp as om
+    rng = np.random.default_rng(1)
+    x = rng.uniform(-1, 1, (4096, 12)).astype(np.float32)
+    y = (np.sin(x[:, 0] * 2) + x[:, 1] * x[:, 2] + 0.5 * x[:, 3]).astype(np.float32)
+    mlp = runtime.Mlp(seed=2)
+    mlp.set_norm(np.zeros(12), np.ones(12))
+    l0 = float(np.mean((mlp.predict(x) - y) ** 2))
+    loss = mlp.train(x, y, epochs=30, batch=256, lr=2e-3)
+    pred = mlp.predict(x)
+    assert float(np.mean((pred - y) ** 2)) < 0.1 * l0
+    # GPU inference equals the FP64 oracle's forward pass on the trained weights
+    assert rel_err(pred, om.predict(mlp.get_params(), x)) <= 1e-4
+    assert loss < 0.1 * l0
