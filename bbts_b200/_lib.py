@@ -75,6 +75,9 @@ SIGNATURES = {
     "bbx_rt_queue_reduce": (i32, [vp, i32, i32, i32, C.POINTER(C.c_uint32), i32, C.POINTER(i32), i32, i32]),
     "bbx_rt_queue_delete": (i32, [vp, i32, C.POINTER(i32), i32]),
     "bbx_rt_clear_commands": (i32, [vp]),
+    "bbx_rt_load_sbbts": (i32, [vp, C.c_char_p, C.POINTER(i32)]),
+    "bbx_rt_load_bbts": (i32, [vp, C.c_char_p, C.POINTER(i32)]),
+    "bbx_rt_save_bbts": (i32, [vp, C.c_char_p]),
     "bbx_rt_num_commands": (i32, [vp]),
     "bbx_rt_run": (i32, [vp, i32]),
     "bbx_rt_record": (i32, [vp, i32, vp, vp, i32, C.POINTER(i32)]),

@@ -13,6 +13,7 @@
 //   ffnn_*        applications/fnn/ffnn_*.cc (registered at ffnn_lib_init.cc:20-177)
 //   contraction   libraries/cutensor/contraction.h:633-695
 //   ffnn_softmax_ce  new: softmax cross-entropy loss + gradient (no reference counterpart)
+#include <atomic>
 #include <stdexcept>
 #include "bbts_b200.h"
 #include "ud_function.h"
@@ -150,6 +151,11 @@ hint_fn ffnn_ew_hint = [](const params_t&, const margs_t& in) -> size_t {
 
 long long fn_elems(const tensor_meta_t& m) { return (long long)fm(m).num_rows * fm(m).num_cols; }
 
+unsigned long long next_seed() {
+  static std::atomic<unsigned long long> ctr{0};
+  return 0x5eedull + 0x9E3779B97F4A7C15ull * (ctr++ + 1);
+}
+
 void register_ud(udf_manager_t& udm, const char* name, bool ass, bool com, size_t nin, size_t nout) {
   if (udm.get_udf(name)) return;
   auto f = std::make_unique<ud_func_t>();
@@ -252,7 +258,9 @@ void register_b200_udfs(udf_manager_t& udm) {
           auto& c = out.get<0>().as<dense_tensor_t>();
           uint32_t rows = p.get_uint<0>(), cols = p.get_uint<1>();
           float lo = p.get_float_or_default<2>(0.f), hi = p.get_float_or_default<3>(1.f);
-          uint32_t seed = p.get_uint_or_default<4>(0x5eed);
+          // explicit seed (param u4) or a per-process call counter, so every block
+          // of a program differs (the reference seeds each call with time())
+          unsigned long long seed = p.num_parameters() > 4 ? p.get_uint<4>() : next_seed();
           ok(bbx_fill_philox(dt, c.raw(), (long long)rows * cols, seed, 0, lo, hi, p.stream));
           dm(c._meta) = {rows, cols, 1.0f};
         },
@@ -426,7 +434,7 @@ void register_b200_udfs(udf_manager_t& udm) {
           uint32_t rows = p.get_uint<0>(), cols = p.get_uint<1>();
           fm(c._meta) = {rows, cols, (bool)w};
           long long n = (long long)(rows + (w ? 1 : 0)) * cols;  // weights: data + bias row
-          ok(bbx_fill_philox(BBX_F32, c.data(), n, p.get_uint_or_default<4>(0x5eed + w), 0,
+          ok(bbx_fill_philox(BBX_F32, c.data(), n, p.num_parameters() > 4 ? p.get_uint<4>() : next_seed(), 0,
                              p.get_float_or_default<2>(0.f), p.get_float_or_default<3>(1.f), p.stream));
         },
         [](const params_t& p, const margs_t&) -> size_t {

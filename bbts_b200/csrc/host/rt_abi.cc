@@ -6,6 +6,8 @@
 #include "bbts_b200.h"
 #include "common.h"
 #include "runtime.h"
+#include "compiler.h"
+#include <fstream>
 
 using namespace bbts;
 
@@ -216,6 +218,64 @@ int bbx_rt_clear_commands(bbx_rt_t* rt) {
 }
 
 int bbx_rt_num_commands(bbx_rt_t* rt) { return rt ? (int)rt->rt.commands.size() : -1; }
+
+static command_id_t next_id(bbx_rt_t* rt) {
+  return rt->rt.commands.empty() ? 0 : rt->rt.commands.back()->id + 1;
+}
+
+int bbx_rt_load_sbbts(bbx_rt_t* rt, const char* path, int* n_added) {
+  if (!rt || !path) return bbx::set_error(BBX_ERR_INVALID, "null argument");
+  RT_TRY({
+    std::ifstream f(path);
+    if (!f.is_open()) throw std::runtime_error(std::string("cannot open ") + path);
+    compile_source_file_t src;
+    src.read(f);
+    auto cmds = compile_single_node(src, *rt->rt.udm, next_id(rt));
+    if (n_added) *n_added = (int)cmds.size();
+    for (auto& c : cmds) rt->rt.commands.push_back(std::move(c));
+  });
+}
+
+int bbx_rt_load_bbts(bbx_rt_t* rt, const char* path, int* n_added) {
+  if (!rt || !path) return bbx::set_error(BBX_ERR_INVALID, "null argument");
+  RT_TRY({
+    parsed_command_list_t list;
+    if (!list.deserialize(path)) throw std::runtime_error(std::string("cannot open ") + path);
+    auto cmds = load_parsed(list, *rt->rt.udm, next_id(rt));
+    if (n_added) *n_added = (int)cmds.size();
+    for (auto& c : cmds) rt->rt.commands.push_back(std::move(c));
+  });
+}
+
+int bbx_rt_save_bbts(bbx_rt_t* rt, const char* path) {
+  if (!rt || !path) return bbx::set_error(BBX_ERR_INVALID, "null argument");
+  RT_TRY({
+    parsed_command_list_t list;
+    for (auto& cp : rt->rt.commands) {
+      const command_t& c = *cp;
+      parsed_command_t p;
+      if (c.is_delete()) p.type = parsed_command_t::op_type_t::DELETE;
+      else if (c.is_reduce()) p.type = parsed_command_t::op_type_t::REDUCE;
+      else if (c.is_apply()) p.type = parsed_command_t::op_type_t::APPLY;
+      else p.type = parsed_command_t::op_type_t::MOVE;
+      if (!c.is_delete()) {
+        ud_impl_t* impl = rt->rt.udm->get_fn_impl(c.fun_id);
+        if (impl) {
+          p.def.ud_name = impl->ud_name;
+          p.def.input_types = impl->inputTypes;
+          p.def.output_types = impl->outputTypes;
+          p.def.is_gpu = impl->is_gpu;
+        }
+      }
+      for (size_t i = 0; i < c.get_num_inputs(); ++i) p.inputs.push_back({c.get_input(i).tid, c.get_input(i).node});
+      for (size_t i = 0; i < c.get_num_outputs(); ++i) p.outputs.push_back({c.get_output(i).tid, c.get_output(i).node});
+      auto prm = c.get_parameters();
+      p.parameters.assign(prm.begin(), prm.end());
+      list.commands.push_back(std::move(p));
+    }
+    if (!list.serialize(path)) throw std::runtime_error(std::string("cannot write ") + path);
+  });
+}
 
 int bbx_rt_run(bbx_rt_t* rt, int policy) {
   if (!rt) return bbx::set_error(BBX_ERR_INVALID, "null runtime");

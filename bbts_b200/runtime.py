@@ -169,6 +169,17 @@ class Runtime:
     def num_commands(self):
         return lib.bbx_rt_num_commands(self.h)
 
+    def load_program(self, path):
+        """Appends a .sbbts (text) or .bbts (binary) program compiled for this node."""
+        n = C.c_int()
+        fn = lib.bbx_rt_load_sbbts if path.endswith(".sbbts") else lib.bbx_rt_load_bbts
+        check(fn(self.h, path.encode(), C.byref(n)))
+        self._next_cmd += n.value  # the loader numbers them after the last queued command
+        return n.value
+
+    def save_bbts(self, path):
+        check(lib.bbx_rt_save_bbts(self.h, path.encode()))
+
     def run(self, policy=HEURISTIC):
         check(lib.bbx_rt_run(self.h, policy))
 

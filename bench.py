@@ -29,12 +29,16 @@ sys.path.insert(0, ROOT)
 GRID = 8            # 8 row blocks of A, 8 column blocks of B
 BS = 4096           # block edge
 FLOP_PER_STEP = 2.0 * (GRID * BS) ** 2 * BS
+# DRAM bytes (read + write) of one full grouped launch: ncu's dram__bytes_read.sum +
+# dram__bytes_write.sum on the 2x2-block capture (4 problems, 548 MB) scaled by the
+# 64/4 problems of the full launch (the tc_gemm ncu summary kept under profiles/).
+TRAFFIC_BYTES_PER_LAUNCH = 8.77e9
 
 
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--steps", type=int, default=30)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--tile-n", type=int, default=0)
@@ -63,6 +67,23 @@ class ClockSampler:
         self._t = None
 
     def _run(self):
+        # NVML (read-only queries) every ~10 ms; nvidia-smi as the fallback
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self.index)
+            getr = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            bits = [0x8, 0x40, 0x20, 0x4]  # hw_slowdown, hw_thermal, sw_thermal, sw_power_cap
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            while not self._stop.is_set():
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = getr(h)
+                self.samples.append([str(sm), str(mx), "0"] + ["Active" if r & b else "Not Active" for b in bits])
+                self._stop.wait(0.01)
+            return
+        except Exception:
+            pass
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
@@ -205,15 +226,14 @@ def main():
     hbm, bf16_peak, bf16_sust, src = load_peaks()
     kern_ms = sum(step_ms) / len(step_ms)
     achieved = FLOP_PER_STEP / (kern_ms * 1e-3) / 1e12
-    roofline = {"bound": "tensor", "achieved": round(achieved, 1), "peak": bf16_peak,
-                "unit": "TFLOP/s", "frac": round(achieved / bf16_peak, 4), "traffic": None,
-                "peak_source": src + " bf16 (burst)"}
-    prof = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(prof):
-        try:
-            roofline["traffic"] = json.load(open(prof)).get("tc_gemm_cpmm_bytes_per_launch")
-        except Exception:
-            pass
+    # The timed region is args.steps back-to-back launches (hundreds of ms of
+    # dense tensor work under the 1 kW cap), so the denominator is the measured
+    # SUSTAINED bf16 peak; the burst fraction is reported beside it.
+    peak = bf16_sust or bf16_peak
+    roofline = {"bound": "tensor", "achieved": round(achieved, 1), "peak": peak,
+                "unit": "TFLOP/s", "frac": round(achieved / peak, 4), "traffic": TRAFFIC_BYTES_PER_LAUNCH,
+                "peak_source": src + " bf16 sustained (of measured)", "frac_of_burst": round(achieved / bf16_peak, 4),
+                "kernel": "tc_gemm_kernel<256,K-major A,MN-major B,bf16>", "launches_timed": args.steps}
 
     # ---------------- e2e through the C ABI with pinned host blocks
     hA = [torch.empty(BS, BS, dtype=torch.bfloat16, pin_memory=True) for _ in range(GRID)]

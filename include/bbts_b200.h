@@ -244,6 +244,16 @@ int bbx_rt_queue_reduce(bbx_rt_t* rt, int cmd_id, int ud_id, int impl_id, const 
 int bbx_rt_queue_delete(bbx_rt_t* rt, int cmd_id, const int* tids, int n);
 int bbx_rt_clear_commands(bbx_rt_t* rt);
 int bbx_rt_num_commands(bbx_rt_t* rt);
+/* Appends the commands of a program file, compiled for this single node:
+ * .sbbts text compile sources (compile_source_file_t,
+ * src/commands/command_compiler.h:977-1027, compiled as command_compiler_t
+ * does with all placement on node 0) and .bbts binary parsed command lists
+ * (parsed_command_list_t, src/commands/parsed_command.h:194-383, compiled as
+ * command_loader_t does, command_loader.h:10-182). *n_added = commands added. */
+int bbx_rt_load_sbbts(bbx_rt_t* rt, const char* path, int* n_added);
+int bbx_rt_load_bbts(bbx_rt_t* rt, const char* path, int* n_added);
+/* Writes the runtime's command list back out as a .bbts parsed command list. */
+int bbx_rt_save_bbts(bbx_rt_t* rt, const char* path);
 /* The per-op path: the command list runs through the reservation station
  * (LIFO, or learned priority with policy 1) with one stream-ordered launch per
  * command, like command_runner_t::local_command_runner

@@ -11,7 +11,10 @@
 #include <cstdlib>
 #include <set>
 #include <thread>
+#include <sstream>
+#include <tuple>
 #include "command.h"
+#include "compiler.h"
 #include "reservation_station.h"
 #include "tensor.h"
 #include "ud_function.h"
@@ -228,7 +231,95 @@ static void test_reservation_station_threads() {
   EXPECT((int)removed.size() == N);
 }
 
+// .sbbts text round trip + single-node compilation (command_compiler.h:977-1027)
+static void test_sbbts_compile() {
+  const char* text =
+      "2\n"
+      "0 matrix_mult 2 dense dense 1 dense \n"
+      "1 matrix_add 2 dense dense 1 dense \n"
+      "4\n"
+      "0 APPLY 2 0 1 1 2 2 int 0 int 0 \n"
+      "0 APPLY 2 0 1 1 3 0 \n"
+      "1 REDUCE 2 2 3 1 4 1 float 0.5 \n"
+      "0 DELETE 2 2 3 0 0 \n";
+  std::istringstream in(text);
+  compile_source_file_t src;
+  src.read(in);
+  EXPECT(src.function_specs.size() == 2 && src.commands.size() == 4);
+  EXPECT(src.commands[2].type == abstract_command_type_t::REDUCE && src.commands[2].params[0].f == 0.5f);
+  std::ostringstream out;
+  src.write(out);
+  std::istringstream in2(out.str());
+  compile_source_file_t again;
+  again.read(in2);
+  EXPECT(again.commands.size() == 4 && again.commands[1].output_tids[0] == 3);
+
+  auto tf = std::make_shared<tensor_factory_t>();
+  udf_manager_t udm(tf);
+  for (auto [name, ass, com] : {std::tuple<const char*, bool, bool>{"matrix_mult", true, false},
+                                std::tuple<const char*, bool, bool>{"matrix_add", true, true}}) {
+    auto f = std::make_unique<ud_func_t>();
+    f->ud_name = name; f->is_ass = ass; f->is_com = com; f->num_in = 2; f->num_out = 1;
+    udm.register_udf(std::move(f));
+    udm.register_udf_impl(std::make_unique<fake_impl>(name, "gpu", std::vector<std::string>{"dense", "dense"}, std::vector<std::string>{"dense"}, true));
+  }
+  auto cmds = compile_single_node(src, udm, 10);
+  EXPECT(cmds.size() == 4);
+  EXPECT(cmds[0]->id == 10 && cmds[0]->is_apply() && cmds[0]->get_root_node() == 0);
+  EXPECT(cmds[2]->is_reduce() && cmds[2]->get_num_inputs() == 2 && cmds[2]->get_output(0).tid == 4);
+  EXPECT(cmds[3]->is_delete() && cmds[3]->get_num_inputs() == 2);
+  // a REDUCE over a non-commutative ud is refused
+  std::istringstream bad("1\n0 matrix_mult 2 dense dense 1 dense \n1\n0 REDUCE 2 0 1 1 2 0 \n");
+  compile_source_file_t sbad;
+  sbad.read(bad);
+  bool threw = false;
+  try { compile_single_node(sbad, udm, 0); } catch (const std::exception&) { threw = true; }
+  EXPECT(threw);
+}
+
+// .bbts binary round trip (parsed_command.h:194-383) and the loader
+static void test_bbts_roundtrip() {
+  parsed_command_list_t list;
+  parsed_command_t a;
+  a.type = parsed_command_t::op_type_t::APPLY;
+  a.def = {"matrix_add", {"dense", "dense"}, {"dense"}, true};
+  a.inputs = {{0, 0}, {1, 0}};
+  a.outputs = {{2, 0}};
+  command_param_t p;
+  p.f = 1.5f;
+  a.parameters = {p};
+  parsed_command_t d;
+  d.type = parsed_command_t::op_type_t::DELETE;
+  d.inputs = {{0, 0}};
+  list.commands = {a, d};
+  const char* path = "/tmp/bbx_test_roundtrip.bbts";
+  EXPECT(list.serialize(path));
+  parsed_command_list_t back;
+  EXPECT(back.deserialize(path));
+  EXPECT(back.commands.size() == 2);
+  EXPECT(back.commands[0].def.ud_name == "matrix_add" && back.commands[0].def.is_gpu);
+  EXPECT(back.commands[0].inputs[1].first == 1 && back.commands[0].outputs[0].first == 2);
+  EXPECT(back.commands[0].parameters[0].f == 1.5f);
+  // on disk each (tid, node) pair is stored node first (std::tuple layout)
+  FILE* f = std::fopen(path, "rb");
+  std::vector<unsigned char> raw(4096);
+  size_t n = std::fread(raw.data(), 1, raw.size(), f);
+  std::fclose(f);
+  EXPECT(n > 8);
+  auto tf = std::make_shared<tensor_factory_t>();
+  udf_manager_t udm(tf);
+  auto fn = std::make_unique<ud_func_t>();
+  fn->ud_name = "matrix_add"; fn->is_ass = fn->is_com = true; fn->num_in = 2; fn->num_out = 1;
+  udm.register_udf(std::move(fn));
+  udm.register_udf_impl(std::make_unique<fake_impl>("matrix_add", "gpu", std::vector<std::string>{"dense", "dense"}, std::vector<std::string>{"dense"}, true));
+  auto cmds = load_parsed(back, udm, 0);
+  EXPECT(cmds.size() == 2 && cmds[0]->is_apply() && cmds[1]->is_delete());
+  std::remove(path);
+}
+
 int main() {
+  test_sbbts_compile();
+  test_bbts_roundtrip();
   test_dense_format();
   test_matcher_types();
   test_command_layout();

@@ -72,8 +72,9 @@ def test_matrix_mult_transpose_params(R, ta, tb):
     runtime, _ = R
     rt = runtime.Runtime()
     rng = np.random.default_rng(ta * 2 + tb)
-    a = rng.standard_normal((192, 256)).astype(np.float32)
-    b = rng.standard_normal((256, 192)).astype(np.float32)
+    m, n, k = 192, 320, 256
+    a = rng.standard_normal((k, m) if ta else (m, k)).astype(np.float32)
+    b = rng.standard_normal((n, k) if tb else (k, n)).astype(np.float32)
     rt.put_dense(0, a)
     rt.put_dense(1, b)
     rt.apply(rt.impl("matrix_mult", ["dense", "dense"], ["dense"]), [0, 1], [2], params=[bool(ta), bool(tb)])
@@ -277,3 +278,64 @@ def test_mlp_training_fits(R):
     # GPU inference equals the FP64 oracle's forward pass on the trained weights
     assert rel_err(pred, om.predict(mlp.get_params(), x)) <= 1e-4
     assert loss < 0.1 * l0
+
+
+# ------------------------------------------------------------------ program files
+def test_bbts_program_bmm(R, tmp_path):
+    """A .bbts program in the reference's binary format (the single-node form of
+    applications/bmm/generate_bmm.cc) loads, compiles and runs per-op and as a DAG."""
+    runtime, _ = R
+    from bbts_b200 import programs
+    path = str(tmp_path / "bmm.bbts")
+    A, B, C = programs.bmm_bbts(path, n=512, split=2)
+    for mode in ("per_op", "dag"):
+        rt = runtime.Runtime()
+        n = rt.load_program(path)
+        assert n == 8 + 8 + 4 + 1
+        dag = None
+        if mode == "per_op":
+            rt.run()
+            get = rt.get_dense
+        else:
+            dag = rt.build_dag()
+            dag.launch()
+            get = lambda t: dag.read_bytes(t, 256 * 256 * 4).view(np.float32).reshape(256, 256)
+        a = np.block([[get(A[(i, j)]) for j in range(2)] for i in range(2)])
+        b = np.block([[get(B[(i, j)]) for j in range(2)] for i in range(2)])
+        assert 0.0 <= a.min() and a.max() < 1.0 and a.std() > 0.2        # uniform(0,1) blocks
+        assert not np.array_equal(get(A[(0, 0)]), get(A[(0, 1)]))         # distinct seeds per block
+        ref = oracle.matmul_f64(a, b)
+        for (i, j), t in C.items():
+            assert rel_err(get(t), ref[i * 256:(i + 1) * 256, j * 256:(j + 1) * 256]) <= 1e-5
+
+
+def test_sbbts_program(R, tmp_path):
+    runtime, _ = R
+    from bbts_b200 import programs
+    rng = np.random.default_rng(3)
+    rt = runtime.Runtime()
+    a = rng.standard_normal((128, 64)).astype(np.float32)
+    b = rng.standard_normal((64, 96)).astype(np.float32)
+    rt.put_dense(0, a)
+    rt.put_dense(1, b)
+    path = str(tmp_path / "prog.sbbts")
+    programs.write_sbbts(path, [(0, "matrix_mult", ["dense", "dense"], ["dense"]),
+                                (1, "matrix_relu", ["dense"], ["dense"]),
+                                (2, "matrix_weighted_sum", ["dense", "dense"], ["dense"])],
+                         [(0, "APPLY", [0, 1], [2], []),
+                          (1, "APPLY", [2], [3], []),
+                          (2, "APPLY", [2, 3], [4], [0.5, -2.0]),
+                          (0, "DELETE", [2, 3], [], [])])
+    assert rt.load_program(path) == 4
+    rt.run()
+    c = oracle.matmul_f64(a, b)
+    got = rt.get_dense(4)
+    assert rel_err(got, 0.5 * c - 2.0 * np.maximum(c, 0)) <= 1e-5
+    assert rt.count() == 3  # 0, 1 and the result; 2 and 3 deleted
+    rt.save_bbts(str(tmp_path / "prog.bbts"))
+    rt2 = runtime.Runtime()
+    rt2.put_dense(0, a)
+    rt2.put_dense(1, b)
+    assert rt2.load_program(str(tmp_path / "prog.bbts")) == 4
+    rt2.run()
+    assert np.array_equal(rt2.get_dense(4), got)
