@@ -39,6 +39,18 @@ def _dtype_fmt(dtype):
     return {"f32": "dense", "bf16": "dense_bf16"}[dtype]
 
 
+def fill_block(rt, tid, rows, cols, fmt, seed, dist="normal"):
+    """Registers a rows x cols block filled on the device by the seeded Philox
+    generator: N(0,1) (dist="normal") or U(-1,1) (dist="uniform")."""
+    from ._lib import lib, check
+    fid = rt.fmt(fmt)
+    rt.put(tid, dense_meta(fid, rows, cols))
+    ptr, _ = rt.payload(tid)
+    dt = 1 if fmt == "dense_bf16" else 0
+    d, a, b = (1, 0.0, 1.0) if dist == "normal" else (0, -1.0, 1.0)
+    check(lib.bbx_fill_philox(dt, ptr, rows * cols, int(seed), d, a, b, rt.stream))
+
+
 def put_block(rt, tid, arr, fmt):
     """Registers a host block in format `fmt` (dense f32 or dense_bf16)."""
     arr = np.ascontiguousarray(arr, np.float32)
@@ -122,7 +134,8 @@ def cpmm(rt, rows=8, cols=8, bs=4096, dtype="bf16", seed=0, host=False):
 
 
 def random_dag(rt, n_ops=2000, depth=8, seed=0, dtype="bf16", lo=128, hi=2048, step=64,
-               contraction_dims=(32, 256), mix=(0.60, 0.15, 0.15, 0.10), host=False, max_inputs=16):
+               contraction_dims=(32, 256), mix=(0.60, 0.15, 0.15, 0.10), host=False, max_inputs=16,
+               reuse=0.5):
     """Seeded random DAG: per level, ops drawn from the mix (matmul, add, n-ary
     reduce, contraction); every op reads at least one output of the previous
     level when one of a compatible shape exists, else fresh seeded inputs.
@@ -147,18 +160,25 @@ def random_dag(rt, n_ops=2000, depth=8, seed=0, dtype="bf16", lo=128, hi=2048, s
 
     def fresh_dense(r, c):
         t = e.tid()
-        x = rng.standard_normal((r, c)).astype(np.float32)
-        put_block(rt, t, x, fmt)
         if host:
+            x = rng.standard_normal((r, c)).astype(np.float32)
+            put_block(rt, t, x, fmt)
             host_inputs[t] = x
+        else:
+            fill_block(rt, t, r, c, fmt, seed=int(rng.integers(1 << 62)))
         return t
 
     def fresh_con(dims):
         t = e.tid()
-        x = rng.standard_normal(int(np.prod(dims))).astype(np.float32)
-        rt.put(t, cutensor_meta(cfmt, dims), x)
         if host:
+            x = rng.standard_normal(int(np.prod(dims))).astype(np.float32)
+            rt.put(t, cutensor_meta(cfmt, dims), x)
             host_inputs[t] = x
+        else:
+            from ._lib import lib, check
+            rt.put(t, cutensor_meta(cfmt, dims))
+            ptr, _ = rt.payload(t)
+            check(lib.bbx_fill_philox(0, ptr, int(np.prod(dims)), int(rng.integers(1 << 62)), 1, 0.0, 1.0, rt.stream))
         return t
 
     def pick(pool, pred):
@@ -182,7 +202,7 @@ def random_dag(rt, n_ops=2000, depth=8, seed=0, dtype="bf16", lo=128, hi=2048, s
             else:
                 xa, m, k = x
             n = int(rng.choice(sizes))
-            y = pick(earlier, lambda z: z[1] == k and z[2] == n) if rng.random() < 0.5 else None
+            y = pick(earlier, lambda z: z[1] == k and z[2] == n) if rng.random() < reuse else None
             xb = y[0] if y else fresh_dense(k, n)
             rt.apply(mm, [xa, xb], [t_out])
             dense_by_level[level].append((t_out, m, n))
@@ -198,7 +218,7 @@ def random_dag(rt, n_ops=2000, depth=8, seed=0, dtype="bf16", lo=128, hi=2048, s
             cnt = 2 if kind == 1 else int(rng.integers(2, max_inputs + 1))
             ins = [xa]
             for _ in range(cnt - 1):
-                y = pick(earlier, lambda z: z[1] == m and z[2] == n and z[0] not in ins) if rng.random() < 0.5 else None
+                y = pick(earlier, lambda z: z[1] == m and z[2] == n and z[0] not in ins) if rng.random() < reuse else None
                 ins.append(y[0] if y else fresh_dense(m, n))
             if kind == 1:
                 rt.apply(add, ins, [t_out])
