@@ -153,6 +153,20 @@ int bbx_cast(int src_dtype, const void* in, int dst_dtype, void* out, long long 
 int bbx_quantize_e4m3(int src_dtype, const void* in, void* out, int rows, int cols, int transpose,
                       float* scale_out, void* stream);
 
+/* Allocation-free batched variant of bbx_quantize_e4m3 (no counterpart in the
+ * reference). For callers that must not allocate device memory while they
+ * run -- code under a memory manager that owns all of the GPU, latency paths
+ * where cudaMalloc would synchronise, fixed-footprint deployments. It
+ * quantises `count` blocks (each rows x cols; in / out are HOST arrays of
+ * device pointers, scales_out a device array of `count` floats) and calls no
+ * cudaMalloc / cudaFree: its absmax scratch is a fixed 4 KiB __device__ array
+ * of the library, so count is at most 1024 per call (larger counts fail with
+ * BBX_ERR_INVALID). The first call on a device looks the array up
+ * (cudaGetSymbolAddress), so make it before any stream capture. All calls on
+ * a device share that array: calls that overlap on the GPU race. */
+int bbx_quantize_e4m3_batched_noalloc(int src_dtype, const void* const* in, void* const* out, int count,
+                                      int rows, int cols, int transpose, float* scales_out, void* stream);
+
 /* Seeded counter-based fill (Philox4x32-10): dist 0 = U(a,b), 1 = N(a, b^2). */
 int bbx_fill_philox(int dtype, void* out, long long n, unsigned long long seed, int dist, float a,
                     float b, void* stream);
