@@ -17,8 +17,12 @@
 //              predicted cost, longest first.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <map>
+#include <mutex>
 #include <stdexcept>
+#include <string>
 #include "runtime.h"
 
 namespace bbts {
@@ -105,6 +109,84 @@ void run_opaque(dag_t* d, opaque_t& o, cudaStream_t st) {
   for (tid_t t : o.outs) outs.push_back(header(d, t));
   ud_impl_t::tensor_args_t ia(ins), oa(outs);
   o.impl->call_ud(params, ia, oa);
+}
+
+// ---------------------------------------------------------------- tile autotuner
+// Picks the tcgen05 tile width (BN = 128 or 256) of a grouped launch by timing
+// both on the group's own problems, once per shape bucket. Buckets: input
+// dtype, operand layouts, problem count and log2 of the group's FLOPs, of its
+// largest n and of its largest m. Results persist in a text file when the
+// BBX_TUNE_CACHE environment variable names one ("key tile_n" lines).
+std::mutex g_tune_mu;
+std::map<std::string, int> g_tune;
+bool g_tune_loaded = false;
+
+std::string tune_key(int dtype, bool ta, bool tb, const std::vector<bbx_tc_problem_t>& ps) {
+  double fl = 0;
+  int maxn = 0, maxm = 0;
+  for (auto& q : ps) {
+    fl += 2.0 * q.m * q.n * (double)q.k;
+    maxn = std::max(maxn, q.n);
+    maxm = std::max(maxm, q.m);
+  }
+  char buf[128];
+  std::snprintf(buf, sizeof(buf), "d%d_a%d_b%d_p%d_f%d_n%d_m%d", dtype, (int)ta, (int)tb,
+                (int)std::ceil(std::log2((double)ps.size() + 1)), (int)std::log2(fl + 1), (int)std::log2(maxn + 1),
+                (int)std::log2(maxm + 1));
+  return buf;
+}
+
+int autotune_tile_n(int dtype, bool ta, bool tb, const std::vector<bbx_tc_problem_t>& ps) {
+  const std::string key = tune_key(dtype, ta, tb, ps);
+  const char* path = std::getenv("BBX_TUNE_CACHE");
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    if (!g_tune_loaded && path) {
+      FILE* f = std::fopen(path, "r");
+      if (f) {
+        char k[128];
+        int v;
+        while (std::fscanf(f, "%127s %d", k, &v) == 2) g_tune[k] = v;
+        std::fclose(f);
+      }
+      g_tune_loaded = true;
+    }
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) return it->second;
+  }
+  cudaStream_t st;
+  dag_cuda(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "tune stream");
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int best = 256;
+  float best_ms = 1e30f;
+  for (int tn : {256, 128}) {
+    bbx_tc_plan_t* p = nullptr;
+    if (bbx_tc_plan_create(dtype == ELEM_E4M3 ? BBX_E4M3 : BBX_BF16, ps.data(), (int)ps.size(), tn, &p) != 0) continue;
+    dag_bbx(bbx_tc_plan_launch(p, st));  // warm-up
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < 3; ++r) dag_bbx(bbx_tc_plan_launch(p, st));
+    cudaEventRecord(e1, st);
+    dag_cuda(cudaEventSynchronize(e1), "tune sync");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    bbx_tc_plan_destroy(p);
+    if (ms < best_ms) { best_ms = ms; best = tn; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamDestroy(st);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = best;
+  if (path) {
+    FILE* f = std::fopen(path, "a");
+    if (f) {
+      std::fprintf(f, "%s %d\n", key.c_str(), best);
+      std::fclose(f);
+    }
+  }
+  return best;
 }
 
 void issue(dag_t* d, cudaStream_t st) {
@@ -392,8 +474,11 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
     }
     for (auto& kv : tc_groups) {
       bbx_tc_plan_t* p = nullptr;
-      dag_bbx(bbx_tc_plan_create(kv.first / 4 == ELEM_E4M3 ? BBX_E4M3 : BBX_BF16, kv.second.data(),
-                                 (int)kv.second.size(), tile_n, &p));
+      const int dt = kv.first / 4;
+      // tile_n < 0: autotune per group; 0: size heuristic; 128 / 256: forced
+      const int tn = tile_n < 0 ? autotune_tile_n(dt, (kv.first & 2) != 0, (kv.first & 1) != 0, kv.second) : tile_n;
+      dag_bbx(bbx_tc_plan_create(dt == ELEM_E4M3 ? BBX_E4M3 : BBX_BF16, kv.second.data(),
+                                 (int)kv.second.size(), tn, &p));
       d->waves[w].tc.push_back(p);
       d->stats.tc_launches++;
     }

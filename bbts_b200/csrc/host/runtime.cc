@@ -295,6 +295,45 @@ void runtime_t::run_per_op(int policy, std::vector<std::pair<op_features_t, floa
     std::unordered_map<tid_t, std::vector<size_t>> readers;
     for (size_t i = 0; i < commands.size(); ++i)
       for (size_t j = 0; j < commands[i]->get_num_inputs(); ++j) readers[commands[i]->get_input(j).tid].push_back(i);
+    // metas of every tensor the list will create (get_out_meta propagated in
+    // command order), so each command gets real features
+    std::unordered_map<tid_t, tensor_meta_t> metas;
+    for (tid_t t : storage->tids()) metas[t] = storage->get(t)->_meta;
+    std::vector<op_features_t> fs(commands.size());
+    std::vector<bool> has(commands.size(), false);
+    for (size_t i = 0; i < commands.size(); ++i) {
+      auto& c = *commands[i];
+      if (c.is_delete()) continue;
+      ud_impl_t* impl = udm->get_fn_impl(c.fun_id);
+      std::vector<tensor_meta_t> in;
+      bool ok = impl != nullptr;
+      for (size_t j = 0; j < c.get_num_inputs() && ok; ++j) {
+        auto it = metas.find(c.get_input(j).tid);
+        ok = it != metas.end();
+        if (ok) in.push_back(it->second);
+      }
+      if (!ok) continue;
+      ud_impl_t::tensor_params_t params;
+      params._params = c.get_parameters();
+      std::vector<tensor_meta_t> out(c.get_num_outputs());
+      for (auto& m : out) std::memset(&m, 0, sizeof(m));
+      if (c.is_apply()) {
+        ud_impl_t::meta_args_t im(in), om(out);
+        impl->get_out_meta(params, im, om);
+        for (size_t o = 0; o < out.size(); ++o) out[o].fmt_id = tf->get_tensor_ftm(impl->outputTypes[o]);
+      } else {
+        out[0] = in[0];
+      }
+      for (size_t o = 0; o < out.size(); ++o) metas[c.get_output(o).tid] = out[o];
+      fs[i] = features_of(*tf, c, impl, in, nullptr);
+      has[i] = true;
+    }
+    std::vector<op_features_t> batch;
+    for (size_t i = 0; i < commands.size(); ++i) if (has[i]) batch.push_back(fs[i]);
+    std::vector<double> lat_b = batch_predictor ? batch_predictor(batch) : std::vector<double>();
+    std::vector<double> lat(commands.size(), 1.0);
+    for (size_t i = 0, k = 0; i < commands.size(); ++i)
+      if (has[i]) lat[i] = k < lat_b.size() ? lat_b[k++] : predictor(fs[i]);
     std::vector<double> up(commands.size(), 0.0);
     for (size_t ii = commands.size(); ii-- > 0;) {
       auto& c = *commands[ii];
@@ -302,14 +341,7 @@ void runtime_t::run_per_op(int policy, std::vector<std::pair<op_features_t, floa
       double best = 0;
       for (size_t o = 0; o < c.get_num_outputs(); ++o)
         for (size_t r : readers[c.get_output(o).tid]) best = std::max(best, up[r]);
-      // features need input metas; approximate with the complexity hint when inputs do not exist yet
-      size_t hint = 0;
-      op_features_t f{};
-      bool have_inputs = true;
-      for (size_t j = 0; j < c.get_num_inputs(); ++j) have_inputs = have_inputs && storage->get(c.get_input(j).tid);
-      double lat = 1.0;
-      if (have_inputs) { f = features(c, &hint); lat = predictor(f); }
-      up[ii] = lat + best;
+      up[ii] = lat[ii] + best;
       prio[c.id] = up[ii];
     }
     rs.set_priority([&prio](const command_t& c) { auto it = prio.find(c.id); return it == prio.end() ? 0.0 : it->second; });

@@ -77,11 +77,13 @@ def bmm(rt, n=4096, split=4, dtype="f32", out_dtype=None, seed=0, host=True, dis
         for i in range(split):
             for j in range(split):
                 t = e.tid()
-                x = (rng.standard_normal((bs, bs)) if dist == "normal" else rng.uniform(-1, 1, (bs, bs))).astype(np.float32)
-                put_block(rt, t, x, fmt)
                 store[(i, j)] = t
                 if host:
+                    x = (rng.standard_normal((bs, bs)) if dist == "normal" else rng.uniform(-1, 1, (bs, bs))).astype(np.float32)
+                    put_block(rt, t, x, fmt)
                     hstore[(i, j)] = x
+                else:
+                    fill_block(rt, t, bs, bs, fmt, seed=int(rng.integers(1 << 62)), dist=dist)
     mm = rt.impl("matrix_mult", [fmt, fmt], [ofmt])
     add = rt.impl("matrix_add", [ofmt, ofmt], [ofmt])
     parts, C = {}, {}

@@ -46,6 +46,11 @@ def parse():
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--grid", type=int, default=8,
                    help="blocks per side of A/B (8 = the full workload; smaller only for profiling captures)")
+    p.add_argument("--workload", default="cpmm", choices=["cpmm", "bmm", "dag", "learned"],
+                   help="cpmm: the headline line (cross-product blocked matmul); bmm / dag / learned: the "
+                        "blocked matmul, random 2000-op DAG and learned-scheduling configurations")
+    p.add_argument("--n-ops", type=int, default=0, help="DAG size override (dag: 2000, learned: 5000)")
+    p.add_argument("--train-dags", type=int, default=100, help="learned: DAGs recorded for the training set")
     return p.parse_args()
 
 
@@ -165,6 +170,147 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def _time_on(stream_ptr, fn, reps):
+    """Device time per call of fn() (ms), CUDA events on the runtime's stream."""
+    import torch
+    s = torch.cuda.ExternalStream(stream_ptr)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(s)
+    for _ in range(reps):
+        fn()
+    e1.record(s)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def run_dag_workload(args):
+    """Whole-DAG configurations through the runtime: grouped graph path vs the
+    plain FP32 per-op path, and learned vs heuristic scheduling."""
+    import numpy as np
+    import torch
+    import bbts_b200
+    from bbts_b200 import runtime, workloads
+    torch.cuda.set_device(0)
+    hbm, bf16_peak, bf16_sust, src = load_peaks()
+    line = {"n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "data": "synthetic N(0,1), seeded Philox on the device"}
+
+    def build(dtype, seed, **kw):
+        rt = runtime.Runtime()
+        if args.workload == "bmm":
+            info = workloads.bmm(rt, n=4096, split=4, dtype=dtype, seed=seed, host=False)
+        else:
+            n_ops = args.n_ops or (2000 if args.workload == "dag" else 5000)
+            hi = 2048 if args.workload == "dag" else 4096
+            info = workloads.random_dag(rt, n_ops=n_ops, depth=8, seed=seed, dtype=dtype, hi=hi, **kw)
+        torch.cuda.synchronize()
+        return rt, info
+
+    with ClockSampler(0) as clk:
+        result = {}
+        if args.workload in ("bmm", "dag"):
+            # fast path: bf16 blocks, grouped + graph, autotuned tiles, heuristic and learned-free policy
+            rt, info = build("bf16", 7)
+            dag = rt.build_dag(runtime.HEURISTIC, tile_n=-1)
+            st = dag.stats()
+            for _ in range(args.warmup):
+                dag.launch()
+            ms = _time_on(rt.stream.value, dag.launch, args.steps)
+            flops = info["flops"]
+            result["grouped_bf16"] = {"ms": round(ms, 3), "tflops": round(flops / ms / 1e9, 2), "dag": st}
+            dag.close()
+            rt.close()
+            # plain FP32 per-op path: same DAG in f32 blocks, reservation-station LIFO, one launch per op
+            rt, info32 = build("f32", 7)
+            rt.run()
+            pms = _time_on(rt.stream.value, rt.run, max(1, min(3, args.steps)))
+            result["plain_fp32_per_op"] = {"ms": round(pms, 3), "tflops": round(info32["flops"] / pms / 1e9, 3)}
+            rt.close()
+            value = flops / ms / 1e9
+            name = {"bmm": "blocked matmul 4096^2 in 1024^2 blocks (64 matrix_mult + 16 4-input reduces)",
+                    "dag": "random DAG, %d ops, depth 8 (60%% matmul 128..2048, 15%% add, 15%% reduce 2-16, "
+                           "10%% contraction ijk,kl->ijl 32..256)" % (args.n_ops or 2000)}[args.workload]
+            line.update({"metric": "block-op DAG TFLOP/s and makespan vs plain FP32 path", "value": round(value, 2),
+                         "unit": "TFLOP/s", "ms_per_step": round(ms, 3), "dtype": "bf16",
+                         "config": {"workload": name, "flops_per_step": flops},
+                         "makespan_ms": {"grouped_bf16_graph": round(ms, 3), "plain_fp32_per_op": round(pms, 3)},
+                         "speedup_vs_plain_fp32": round(pms / ms, 2), "detail": result,
+                         "gpu_launches": st["tc_launches"] + st["stream_launches"] + st["other_launches"]})
+        else:
+            # learned scheduling: train the MLP on timings the runtime records itself
+            t0 = time.perf_counter()
+            feats, lats = [], []
+            for d in range(args.train_dags):
+                rt, _ = build("bf16" if d % 2 == 0 else "f32", 1000 + d, reuse=0.8)
+                f, l = rt.record()
+                feats.append(f)
+                lats.append(l)
+                rt.close()
+            X = np.concatenate(feats)
+            y = np.log(np.maximum(np.concatenate(lats), 1e-3))
+            rec_s = time.perf_counter() - t0
+            n_hold = len(y) // 10
+            mlp = runtime.Mlp(seed=1)
+            mu, sd = X[n_hold:].mean(0), X[n_hold:].std(0) + 1e-6
+            mlp.set_norm(mu, sd)
+            t1 = time.perf_counter()
+            loss = mlp.train(X[n_hold:], y[n_hold:], epochs=20, batch=1024, lr=1e-3)
+            train_s = time.perf_counter() - t1
+            t2 = time.perf_counter()
+            pred = mlp.predict(X[:n_hold])
+            infer_s = time.perf_counter() - t2
+            hold_mse = float(np.mean((pred - y[:n_hold]) ** 2))
+            # the complexity-hint baseline predictor: log(flops-like hint) fit by least squares
+            hint = X[:, 11] * np.log(2)
+            A = np.stack([hint[n_hold:], np.ones(len(y) - n_hold)], 1)
+            coef = np.linalg.lstsq(A, y[n_hold:], rcond=None)[0]
+            hint_mse = float(np.mean((coef[0] * hint[:n_hold] + coef[1] - y[:n_hold]) ** 2))
+            # held-out DAG: makespan learned vs heuristic on the same kernels
+            rt, info = build("bf16", 4242, reuse=0.8)
+            make = {}
+            for pol, nm in ((runtime.HEURISTIC, "heuristic"), (runtime.LEARNED, "learned")):
+                if pol == runtime.LEARNED:
+                    rt.set_predictor(mlp)
+                dag = rt.build_dag(pol, tile_n=0)
+                for _ in range(args.warmup):
+                    dag.launch()
+                make[nm] = _time_on(rt.stream.value, dag.launch, args.steps)
+                make[nm + "_waves"] = dag.stats()["waves"]
+                dag.close()
+            # per-op reservation-station order: LIFO vs learned critical-path priority
+            rt.set_predictor(None)
+            rt.run(runtime.HEURISTIC)
+            lifo = _time_on(rt.stream.value, lambda: rt.run(runtime.HEURISTIC), 1)
+            rt.set_predictor(mlp)
+            rt.run(runtime.LEARNED)
+            cp = _time_on(rt.stream.value, lambda: rt.run(runtime.LEARNED), 1)
+            flops = info["flops"]
+            value = flops / make["learned"] / 1e9
+            line.update({"metric": "block-op DAG makespan, learned vs heuristic schedule", "value": round(value, 2),
+                         "unit": "TFLOP/s", "ms_per_step": round(make["learned"], 3), "dtype": "bf16",
+                         "config": {"workload": "held-out random DAG, %d ops, sizes 128..4096" % info["n_ops"],
+                                    "flops_per_step": flops, "train_timings": int(len(y) - n_hold),
+                                    "train_dags": args.train_dags},
+                         "makespan_ms": {"grouped_learned": round(make["learned"], 3),
+                                         "grouped_heuristic": round(make["heuristic"], 3),
+                                         "per_op_learned_priority": round(cp, 3), "per_op_lifo": round(lifo, 3)},
+                         "learned_gain": {"grouped": round(make["heuristic"] / make["learned"], 4),
+                                          "per_op": round(lifo / cp, 4)},
+                         "cost_model": {"holdout_mse_log_latency": round(hold_mse, 4),
+                                        "complexity_hint_mse_log_latency": round(hint_mse, 4),
+                                        "train_loss": round(loss, 4), "record_s": round(rec_s, 1),
+                                        "train_s": round(train_s, 2), "infer_s_per_%d" % n_hold: round(infer_s, 4)},
+                         "gpu_launches": None})
+            rt.close()
+            mlp.close()
+    line["clocks"] = clk.summary()
+    rc = bbts_b200.lib.bbx_check_device_status(None, None)
+    if rc != 0:
+        raise RuntimeError(bbts_b200.last_error())
+    print(json.dumps(line), flush=True)
+
+
 def main():
     global GRID, FLOP_PER_STEP
     args = parse()
@@ -172,6 +318,8 @@ def main():
     FLOP_PER_STEP = 2.0 * (GRID * BS) ** 2 * BS
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "cpmm":
+        return run_dag_workload(args)
     import torch
     import torch.distributed as dist
     import bbts_b200

@@ -283,6 +283,9 @@ int bbx_rt_record(bbx_rt_t* rt, int policy, float* features, float* latency_us, 
  * a static arena, captured in one CUDA graph. No reference counterpart (the
  * reference issues one call per command). */
 typedef struct bbx_dag bbx_dag_t;
+/* tile_n: 128 or 256 forces the tcgen05 tile width, 0 picks it from the
+ * shapes, -1 runs the autotuner (times both widths on each grouped launch's own
+ * problems once per shape bucket; cached in the file named by $BBX_TUNE_CACHE). */
 int bbx_dag_build(bbx_rt_t* rt, int policy, int tile_n, bbx_dag_t** out);
 int bbx_dag_launch(bbx_dag_t* dag, void* stream);
 int bbx_dag_destroy(bbx_dag_t* dag);
