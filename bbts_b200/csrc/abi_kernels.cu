@@ -546,15 +546,26 @@ int bbx_fill_philox(int dtype, void* out, long long n, unsigned long long seed, 
 
 int bbx_softmax_ce_f32(const float* logits, const int* labels, float* loss, float* grad, int rows,
                        int cols, long long ld, float grad_scale, void* stream) {
+  return bbx_softmax_ce(logits, labels, loss, grad, BBX_F32, rows, cols, ld, grad_scale, stream);
+}
+
+int bbx_softmax_ce(const float* logits, const int* labels, float* loss, void* grad, int grad_dtype, int rows,
+                   int cols, long long ld, float grad_scale, void* stream) {
   if (!logits || !labels || !loss || rows < 0 || cols <= 0 || ld < cols)
     return set_error(BBX_ERR_INVALID, "bad softmax_ce arguments");
+  if (grad_dtype != BBX_F32 && grad_dtype != BBX_BF16) return set_error(BBX_ERR_UNSUPPORTED, "softmax_ce grad dtype");
   if (rows == 0) return BBX_OK;
   DeviceState* d;
   int rc = device_state(&d);
   if (rc) return rc;
   const int warps = 8;
   int grid = std::min((rows + warps - 1) / warps, d->sms * 8);
-  k_softmax_ce<<<grid, warps * 32, 0, (cudaStream_t)stream>>>(logits, labels, loss, grad, rows, cols, ld, grad_scale);
+  if (grad_dtype == BBX_F32)
+    k_softmax_ce<float><<<grid, warps * 32, 0, (cudaStream_t)stream>>>(logits, labels, loss, (float*)grad, rows, cols,
+                                                                      ld, grad_scale);
+  else
+    k_softmax_ce<__nv_bfloat16><<<grid, warps * 32, 0, (cudaStream_t)stream>>>(
+        logits, labels, loss, (__nv_bfloat16*)grad, rows, cols, ld, grad_scale);
   BBX_CHECK_LAUNCH("k_softmax_ce");
   return BBX_OK;
 }

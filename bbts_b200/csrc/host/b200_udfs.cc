@@ -470,6 +470,34 @@ void register_b200_udfs(udf_manager_t& udm) {
         fm(out.get<1>()) = {mz.num_rows, 1, false};
       }));
 
+  // softmax cross-entropy over dense blocks (new ud, no reference counterpart):
+  // in (logits "dense" f32, labels) -> (grad dense / dense_bf16, loss dense rows x 1); f0 = grad scale
+  register_ud(udm, "matrix_softmax_ce", false, false, 2, 2);
+  for (int gdt : {BBX_F32, BBX_BF16}) {
+    add_impl(udm, std::make_unique<b200_impl_t>(
+        gdt == BBX_F32 ? "b200_dense_softmax_ce" : "b200_dense_softmax_ce_bf16", "matrix_softmax_ce",
+        V{"dense", "labels"}, V{gdt == BBX_F32 ? "dense" : "dense_bf16", "dense"}, std::vector<int32_t>{},
+        [gdt](const params_t& p, const targs_t& in, targs_t& out) {
+          auto& z = in.get<0>().as<dense_tensor_t>();
+          auto& y = in.get<1>().as<dense_tensor_t>();
+          auto& g = out.get<0>().as<dense_tensor_t>();
+          auto& l = out.get<1>().as<dense_tensor_t>();
+          auto& mz = dm(z._meta);
+          if (dm(y._meta).num_rows * dm(y._meta).num_cols != mz.num_rows)
+            throw std::runtime_error("matrix_softmax_ce: one label per row expected");
+          dm(g._meta) = {mz.num_rows, mz.num_cols, 1.0f};
+          dm(l._meta) = {mz.num_rows, 1, 1.0f};
+          ok(bbx_softmax_ce(z.data(), (const int*)y.raw(), l.data(), g.raw(), gdt, mz.num_rows, mz.num_cols,
+                            mz.num_cols, p.get_float_or_default<0>(1.f), p.stream));
+        },
+        ew_hint,
+        [](const params_t&, const margs_t& in, margs_t& out) {
+          auto& mz = dm(in.get<0>());
+          dm(out.get<0>()) = {mz.num_rows, mz.num_cols, 1.0f};
+          dm(out.get<1>()) = {mz.num_rows, 1, 1.0f};
+        }));
+  }
+
   // ---- contraction of the cutensor plugin (params: rank_l, rank_r, rank_o,
   // modes_l..., modes_r..., modes_o..., alpha; contraction.h:25-55)
   register_ud(udm, "contraction", false, false, 2, 1);

@@ -258,9 +258,11 @@ __global__ void k_fill_philox(T* out, long long n, unsigned long long seed, int 
 
 // Softmax cross-entropy over rows of `logits` (rows x cols, pitch ld) against
 // integer labels. Writes the per-row loss and, if grad != nullptr, the
-// gradient (softmax - onehot) * grad_scale in the same layout. One warp per row.
+// gradient (softmax - onehot) * grad_scale in the same layout (f32 or bf16).
+// One warp per row.
+template <typename TG>
 __global__ void k_softmax_ce(const float* __restrict__ logits, const int* __restrict__ labels,
-                             float* loss, float* grad, int rows, int cols, long long ld,
+                             float* loss, TG* grad, int rows, int cols, long long ld,
                              float grad_scale) {
   const int warps_per_block = blockDim.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -279,11 +281,13 @@ __global__ void k_softmax_ce(const float* __restrict__ logits, const int* __rest
     const float lse = mx + logf(se);
     if (lane == 0) loss[r] = lse - z[y];
     if (grad) {
-      float* g = grad + (long long)r * ld;
+      TG* g = grad + (long long)r * ld;
       const float inv = 1.f / se;
       for (int c = lane; c < cols; c += 32) {
         float p = expf(z[c] - mx) * inv;
-        g[c] = (p - (c == y ? 1.f : 0.f)) * grad_scale;
+        float v = (p - (c == y ? 1.f : 0.f)) * grad_scale;
+        if constexpr (sizeof(TG) == 4) g[c] = v;
+        else g[c] = __float2bfloat16_rn(v);
       }
     }
   }

@@ -135,6 +135,116 @@ def cpmm(rt, rows=8, cols=8, bs=4096, dtype="bf16", seed=0, host=False):
     return {"A": A, "B": B, "C": C, "hostA": hA, "hostB": hB, "flops": e.flops}
 
 
+def ffnn(rt, batch=16384, d_in=8192, h1=8192, h2=4096, classes=1024, bs=2048, seed=0, host=False):
+    """One forward + backward step of a blocked 3-layer network:
+    A1 = relu(X W1), A2 = relu(A1 W2), Z3 = A2 W3, loss = softmax-CE(Z3, labels);
+    backward dW3 = A2^T G3, dA2 = G3 W3^T, dZ2 = dA2 * relu'(A2), dW2 = A1^T dZ2,
+    dA1 = dZ2 W2^T, dZ1 = dA1 * relu'(A1), dW1 = X^T dZ1. Blocks are bs x bs
+    (W3 / Z3 blocks bs x classes); X, W and activations are bf16, logits and
+    weight gradients f32; every matmul over the block grid is split into block
+    products plus a matrix_add REDUCE. Weights are N(0, 1/fan_in), X N(0, 1),
+    labels uniform over the classes. Returns tids of the weights, dW blocks and
+    per-row-block losses and the algorithmic FLOPs (2 * sum m n k)."""
+    e = Emitter(rt)
+    rng = _rng(seed)
+    B16, F32 = "dense_bf16", "dense"
+    R, KI, K1, K2 = batch // bs, d_in // bs, h1 // bs, h2 // bs
+    mm_b = rt.impl("matrix_mult", [B16, B16], [B16])
+    mm_f = rt.impl("matrix_mult", [B16, B16], [F32])
+    add_b = rt.impl("matrix_add", [B16, B16], [B16])
+    add_f = rt.impl("matrix_add", [F32, F32], [F32])
+    relu = rt.impl("matrix_relu", [B16], [B16])
+    drelu = rt.impl("matrix_relu_dif", [B16], [B16])
+    had = rt.impl("matrix_matrix_hadamard", [B16, B16], [B16])
+    sce = rt.impl("matrix_softmax_ce", [F32, "labels"], [B16, F32])
+    host_vals = {}
+    dead = []
+
+    def inp(rows, cols, std):
+        t = e.tid()
+        if host:
+            x = (rng.standard_normal((rows, cols)) * std).astype(np.float32)
+            put_block(rt, t, x, B16)
+            host_vals[t] = x
+        else:
+            from ._lib import lib, check
+            rt.put(t, dense_meta(rt.fmt(B16), rows, cols))
+            ptr, _ = rt.payload(t)
+            check(lib.bbx_fill_philox(1, ptr, rows * cols, int(rng.integers(1 << 62)), 1, 0.0, float(std), rt.stream))
+        return t
+
+    X = {(i, k): inp(bs, bs, 1.0) for i in range(R) for k in range(KI)}
+    W1 = {(k, j): inp(bs, bs, 1.0 / np.sqrt(d_in)) for k in range(KI) for j in range(K1)}
+    W2 = {(k, j): inp(bs, bs, 1.0 / np.sqrt(h1)) for k in range(K1) for j in range(K2)}
+    W3 = {k: inp(bs, classes, 1.0 / np.sqrt(h2)) for k in range(K2)}
+    labels = {}
+    for i in range(R):
+        t = e.tid()
+        y = rng.integers(0, classes, bs).astype(np.int32)
+        rt.put(t, dense_meta(rt.fmt("labels"), bs, 1), y)
+        labels[i] = t
+        host_vals[("y", i)] = y
+
+    def blocked_mm(left, right, ni, nj, nk, out_impl, red_impl, ta=False, tb=False, m=bs, n=bs, k=bs,
+                   lkey=None, rkey=None):
+        """out[i,j] = sum_k op(left)[i,k] op(right)[k,j] as APPLYs + REDUCEs."""
+        out = {}
+        for i in range(ni):
+            for j in range(nj):
+                parts = []
+                for kk in range(nk):
+                    t = e.tid()
+                    rt.apply(out_impl, [left(i, kk), right(kk, j)], [t], params=[bool(ta), bool(tb)])
+                    e.flops += 2.0 * m * n * k
+                    parts.append(t)
+                if len(parts) == 1:
+                    out[(i, j)] = parts[0]
+                else:
+                    t = e.tid()
+                    rt.reduce(red_impl, parts, t)
+                    dead.extend(parts)
+                    out[(i, j)] = t
+        return out
+
+    def ew(impl, tids, params=()):
+        t = e.tid()
+        rt.apply(impl, tids, [t], params=list(params))
+        return t
+
+    # forward
+    Z1 = blocked_mm(lambda i, k: X[(i, k)], lambda k, j: W1[(k, j)], R, K1, KI, mm_b, add_b)
+    A1 = {key: ew(relu, [t]) for key, t in Z1.items()}
+    dead.extend(Z1.values())
+    Z2 = blocked_mm(lambda i, k: A1[(i, k)], lambda k, j: W2[(k, j)], R, K2, K1, mm_b, add_b)
+    A2 = {key: ew(relu, [t]) for key, t in Z2.items()}
+    dead.extend(Z2.values())
+    Z3 = blocked_mm(lambda i, k: A2[(i, k)], lambda k, j: W3[k], R, 1, K2, mm_f, add_f, n=classes)
+    G3, loss = {}, {}
+    for i in range(R):
+        g, l = e.tid(), e.tid()
+        rt.apply(sce, [Z3[(i, 0)], labels[i]], [g, l], params=[1.0 / batch])
+        G3[i], loss[i] = g, l
+    dead.extend(Z3.values())
+    # backward
+    dW3 = blocked_mm(lambda k, i: A2[(i, k)], lambda i, j: G3[i], K2, 1, R, mm_f, add_f, ta=True, n=classes)
+    dA2 = blocked_mm(lambda i, j: G3[i], lambda j, k: W3[k], R, K2, 1, mm_b, add_b, tb=True, k=classes)
+    M2 = {key: ew(drelu, [A2[key]]) for key in A2}
+    dZ2 = {key: ew(had, [dA2[key], M2[key]]) for key in A2}
+    dead.extend(list(dA2.values()) + list(M2.values()) + list(G3.values()))
+    dW2 = blocked_mm(lambda k, i: A1[(i, k)], lambda i, j: dZ2[(i, j)], K1, K2, R, mm_f, add_f, ta=True)
+    dA1 = blocked_mm(lambda i, j: dZ2[(i, j)], lambda j, k: W2[(k, j)], R, K1, K2, mm_b, add_b, tb=True)
+    dead.extend(list(A2.values()) + list(dZ2.values()))
+    M1 = {key: ew(drelu, [A1[key]]) for key in A1}
+    dZ1 = {key: ew(had, [dA1[key], M1[key]]) for key in A1}
+    dead.extend(list(dA1.values()) + list(M1.values()) + list(A1.values()))
+    dW1 = blocked_mm(lambda k, i: X[(i, k)], lambda i, j: dZ1[(i, j)], KI, K1, R, mm_f, add_f, ta=True)
+    dead.extend(dZ1.values())
+    rt.delete(sorted(set(dead)))
+    return {"X": X, "W1": W1, "W2": W2, "W3": W3, "labels": labels, "dW1": dW1, "dW2": dW2, "dW3": dW3,
+            "loss": loss, "flops": e.flops, "host": host_vals, "bs": bs,
+            "dims": (batch, d_in, h1, h2, classes)}
+
+
 def random_dag(rt, n_ops=2000, depth=8, seed=0, dtype="bf16", lo=128, hi=2048, step=64,
                contraction_dims=(32, 256), mix=(0.60, 0.15, 0.15, 0.10), host=False, max_inputs=16,
                reuse=0.5):

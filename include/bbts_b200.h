@@ -176,6 +176,9 @@ int bbx_fill_philox(int dtype, void* out, long long n, unsigned long long seed, 
  * grad = (softmax(z) - onehot(y)) * grad_scale. */
 int bbx_softmax_ce_f32(const float* logits, const int* labels, float* loss, float* grad, int rows,
                        int cols, long long ld, float grad_scale, void* stream);
+/* Same with the gradient written as BBX_F32 or BBX_BF16 (grad_dtype). */
+int bbx_softmax_ce(const float* logits, const int* labels, float* loss, void* grad, int grad_dtype, int rows,
+                   int cols, long long ld, float grad_scale, void* stream);
 
 /* Rank<=4 permutation with optional cast: out[...] = in[...] where output dim d
  * is input dim perm[d]. Dims are listed outermost-first (row-major). dst_dtype

@@ -339,3 +339,61 @@ def test_sbbts_program(R, tmp_path):
     assert rt2.load_program(str(tmp_path / "prog.bbts")) == 4
     rt2.run()
     assert np.array_equal(rt2.get_dense(4), got)
+
+
+# ------------------------------------------------------------------ blocked FFN step (config-3 shape)
+def _ffnn_reference(info, emulate_bf16):
+    """FP64 forward + backward of the blocked network from the seeded host inputs."""
+    batch, d_in, h1, h2, classes = info["dims"]
+    bs = info["bs"]
+    hv = info["host"]
+    rb = (lambda x: bf16_round(x).astype(np.float64)) if emulate_bf16 else (lambda x: x)
+    q = lambda x: bf16_round(x).astype(np.float64)  # stored inputs are bf16
+    X = np.block([[q(hv[info["X"][(i, k)]]) for k in range(d_in // bs)] for i in range(batch // bs)])
+    W1 = np.block([[q(hv[info["W1"][(k, j)]]) for j in range(h1 // bs)] for k in range(d_in // bs)])
+    W2 = np.block([[q(hv[info["W2"][(k, j)]]) for j in range(h2 // bs)] for k in range(h1 // bs)])
+    W3 = np.vstack([q(hv[info["W3"][k]]) for k in range(h2 // bs)])
+    y = np.concatenate([hv[("y", i)] for i in range(batch // bs)])
+    A1 = rb(np.maximum(rb(X @ W1), 0))
+    A2 = rb(np.maximum(rb(A1 @ W2), 0))
+    Z3 = A2 @ W3
+    P = np.exp(Z3 - Z3.max(1, keepdims=True))
+    P /= P.sum(1, keepdims=True)
+    loss = -np.log(P[np.arange(batch), y])
+    G3 = P.copy()
+    G3[np.arange(batch), y] -= 1.0
+    G3 = rb(G3 / batch)
+    dW3 = A2.T @ G3
+    dZ2 = rb(rb(G3 @ W3.T) * (A2 > 0))
+    dW2 = A1.T @ dZ2
+    dZ1 = rb(rb(dZ2 @ W2.T) * (A1 > 0))
+    dW1 = X.T @ dZ1
+    return loss, dW1, dW2, dW3
+
+
+@pytest.mark.parametrize("path", ["per_op", "dag"])
+def test_ffnn_step_vs_f64(R, path):
+    runtime, workloads = R
+    rt = runtime.Runtime()
+    info = workloads.ffnn(rt, batch=512, d_in=256, h1=256, h2=256, classes=128, bs=128, seed=4, host=True)
+    assert info["flops"] == 2.0 * 512 * (256 * 256 * 2 + 256 * 128) + 2.0 * 512 * (256 * 256 * 2 + 256 * 128) \
+        + 2.0 * 512 * (128 * 256 + 256 * 256)
+    dag = None
+    if path == "per_op":
+        rt.run()
+        get = lambda t: read_dense(rt, t)
+    else:
+        dag = rt.build_dag(runtime.HEURISTIC, tile_n=-1)
+        dag.launch()
+        get = lambda t: read_dense(rt, t, dag)
+    bs = info["bs"]
+    loss = np.concatenate([get(info["loss"][i]).ravel() for i in range(4)])
+    dW1 = np.block([[get(info["dW1"][(k, j)]) for j in range(2)] for k in range(2)])
+    dW2 = np.block([[get(info["dW2"][(k, j)]) for j in range(2)] for k in range(2)])
+    dW3 = np.vstack([get(info["dW3"][(k, 0)]) for k in range(2)])
+    for emulate, tol in ((True, 1e-2), (False, 5e-2)):
+        l64, w1, w2, w3 = _ffnn_reference(info, emulate)
+        assert rel_err(loss, l64) <= tol
+        assert rel_err(dW3, w3) <= tol
+        assert rel_err(dW2, w2) <= tol
+        assert rel_err(dW1, w1) <= tol
