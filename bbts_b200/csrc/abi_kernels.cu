@@ -65,6 +65,26 @@ static int set_tc_attr() {
   return BBX_OK;
 }
 
+template <bool AMN, bool BMN>
+static int set_tc2_attr() {
+  BBX_CUDA(cudaFuncSetAttribute(tc_gemm2_kernel<AMN, BMN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                Tc2Cfg<AMN, BMN>::SMEM_BYTES));
+  return BBX_OK;
+}
+
+static int launch_tc2(bool amn, bool bmn, const TcArgs& args, int grid, cudaStream_t st) {
+  if (grid < 2) grid = 2;
+#define TC2_CASE(A_, B_)                                                                     \
+  if (amn == A_ && bmn == B_) {                                                              \
+    tc_gemm2_kernel<A_, B_><<<grid, Tc2Cfg<A_, B_>::THREADS, Tc2Cfg<A_, B_>::SMEM_BYTES, st>>>(args); \
+    BBX_CHECK_LAUNCH("tc_gemm2_kernel");                                                     \
+    return BBX_OK;                                                                           \
+  }
+  TC2_CASE(false, false) TC2_CASE(false, true) TC2_CASE(true, false) TC2_CASE(true, true)
+#undef TC2_CASE
+  return set_error(BBX_ERR_UNSUPPORTED, "no 2-SM variant");
+}
+
 static int init_tc_attributes() {
   int rc = 0;
   rc |= set_tc_attr<256, false, false, false>(); rc |= set_tc_attr<256, false, true, false>();
@@ -75,6 +95,8 @@ static int init_tc_attributes() {
   rc |= set_tc_attr<256, true, false, true>();   rc |= set_tc_attr<256, true, true, true>();
   rc |= set_tc_attr<128, false, false, true>();  rc |= set_tc_attr<128, false, true, true>();
   rc |= set_tc_attr<128, true, false, true>();   rc |= set_tc_attr<128, true, true, true>();
+  rc |= set_tc2_attr<false, false>(); rc |= set_tc2_attr<false, true>();
+  rc |= set_tc2_attr<true, false>();  rc |= set_tc2_attr<true, true>();
   return rc ? BBX_ERR_CUDA : BBX_OK;
 }
 
@@ -188,7 +210,11 @@ static int launch_tc(int bn, bool amn, bool bmn, bool fp8, const TcArgs& args, i
 }
 
 // Validates one public problem and fills the device record (minus tile_start).
-static int build_problem(int in_dtype, const bbx_tc_problem_t& q, int bn, TcProblem* out) {
+// bn = 128 / 256: the 1-SM kernels (128 x bn tiles); bn = 512: the 2-SM pair
+// kernel (256 x 256 tiles, each CTA loading 128-row halves of A and B).
+static int build_problem(int in_dtype, const bbx_tc_problem_t& q, int bn_code, TcProblem* out) {
+  const bool pair = bn_code == 512;
+  const int bn = pair ? 128 : bn_code;  // rows of a K-major B box
   if (!q.a || !q.b || !q.c) return set_error(BBX_ERR_INVALID, "null operand pointer");
   if (q.m <= 0 || q.n <= 0 || q.k <= 0)
     return set_error(BBX_ERR_INVALID, "bad shape m=%d n=%d k=%d", q.m, q.n, q.k);
@@ -228,8 +254,8 @@ static int build_problem(int in_dtype, const bbx_tc_problem_t& q, int bn, TcProb
   out->m = q.m;
   out->n = q.n;
   out->k = q.k;
-  out->tiles_m = (q.m + 127) / 128;
-  out->tiles_n = (q.n + bn - 1) / bn;
+  out->tiles_m = pair ? (q.m + 255) / 256 : (q.m + 127) / 128;
+  out->tiles_n = pair ? (q.n + 255) / 256 : (q.n + bn - 1) / bn;
   out->alpha = q.alpha;
   out->beta = q.beta;
   out->flags = q.flags & (EPI_RELU | EPI_OUT_BF16 | EPI_BIAS | EPI_BETA);
@@ -329,7 +355,9 @@ int bbx_tc_plan_create(int in_dtype, const bbx_tc_problem_t* problems, int count
   if (in_dtype != BBX_BF16 && in_dtype != BBX_E4M3)
     return set_error(BBX_ERR_UNSUPPORTED, "tensor-core input dtype must be bf16 or e4m3");
   if (tile_n == 0) tile_n = pick_tile_n(problems, count);
-  if (tile_n != 128 && tile_n != 256) return set_error(BBX_ERR_INVALID, "tile_n must be 128 or 256");
+  if (tile_n != 128 && tile_n != 256 && tile_n != 512)
+    return set_error(BBX_ERR_INVALID, "tile_n must be 128, 256 or 512 (2-SM 256x256 pair)");
+  if (tile_n == 512 && in_dtype != BBX_BF16) return set_error(BBX_ERR_UNSUPPORTED, "the 2-SM tile is bf16 only");
   DeviceState* d;
   int rc = device_state(&d);
   if (rc) return rc;
@@ -372,6 +400,11 @@ int bbx_tc_plan_launch(bbx_tc_plan_t* p, void* stream) {
   args.status = d->status;
   if (!p->d_table)
     for (int i = 0; i < p->count; ++i) args.inline_probs[i] = p->host[i];
+  if (p->bn == 512) {
+    // one CTA pair (cluster of 2) per 256 x 256 tile, persistent over the tile list
+    const int grid = 2 * std::min(p->total_tiles, d->sms / 2);
+    return launch_tc2(p->amn, p->bmn, args, grid, (cudaStream_t)stream);
+  }
   const int grid = std::min(p->total_tiles, d->sms);
   return launch_tc(p->bn, p->amn, p->bmn, p->dtype == BBX_E4M3, args, grid,
                    (cudaStream_t)stream, d);

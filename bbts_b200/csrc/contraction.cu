@@ -2,7 +2,8 @@
 // (libraries/cutensor/contraction.h): out = alpha * sum(lhs * rhs) over the
 // modes absent from the output, on column-major rank<=4 FP32 tensors.
 //
-// Lowering (one stream, stream-ordered temporaries):
+// Lowering (stream-ordered temporaries for the per-call entry point; arena
+// slots in the DAG executor):
 //   1. classify every mode as I (lhs+out), N (rhs+out), K (lhs+rhs, summed),
 //      B (all three, batch), L (lhs only, summed) or R (rhs only, summed) --
 //      the same classes the reference's cpu_op plan uses (contraction.h:229-253);
@@ -18,59 +19,74 @@
 // I/N/B in output order and K in lhs order.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstring>
 #include <vector>
 #include "bbts_b200.h"
 #include "common.h"
+#include "contraction.h"
 
 namespace bbx {
 
-struct GatherArgs {
-  int rank_o;               // output modes, outermost first
-  long long odims[4], istride[4], ostride[4];
-  int rank_s;               // summed modes
-  long long sdims[4], sstride[4];
-};
-
-template <typename TO>
-__global__ void k_gather_sum(const float* __restrict__ in, TO* out, const __grid_constant__ GatherArgs a,
-                             long long n) {
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
-       e += (long long)gridDim.x * blockDim.x) {
-    long long rem = e, src = 0, dst = 0;
-    for (int d = a.rank_o - 1; d >= 0; --d) {
-      long long idx = rem % a.odims[d];
-      rem /= a.odims[d];
-      src += idx * a.istride[d];
-      dst += idx * a.ostride[d];
-    }
-    float v;
-    if (a.rank_s == 0) {
-      v = in[src];
-    } else {
-      long long ns = 1;
-      for (int d = 0; d < a.rank_s; ++d) ns *= a.sdims[d];
-      v = 0.f;
-      for (long long s = 0; s < ns; ++s) {
-        long long r = s, off = 0;
-        for (int d = 0; d < a.rank_s; ++d) {
-          off += (r % a.sdims[d]) * a.sstride[d];
-          r /= a.sdims[d];
-        }
-        v += in[src + off];
+__device__ __forceinline__ void gather_one(const float* __restrict__ in, void* out, int out_bf16,
+                                           const GatherArgs& a, long long e) {
+  long long rem = e, src = 0, dst = 0;
+  for (int d = a.rank_o - 1; d >= 0; --d) {
+    long long idx = rem % a.odims[d];
+    rem /= a.odims[d];
+    src += idx * a.istride[d];
+    dst += idx * a.ostride[d];
+  }
+  float v;
+  if (a.rank_s == 0) {
+    v = in[src];
+  } else {
+    long long ns = 1;
+    for (int d = 0; d < a.rank_s; ++d) ns *= a.sdims[d];
+    v = 0.f;
+    for (long long s = 0; s < ns; ++s) {
+      long long r = s, off = 0;
+      for (int d = 0; d < a.rank_s; ++d) {
+        off += (r % a.sdims[d]) * a.sstride[d];
+        r /= a.sdims[d];
       }
+      v += in[src + off];
     }
-    if constexpr (sizeof(TO) == 4) out[dst] = v;
-    else out[dst] = __float2bfloat16_rn(v);
+  }
+  if (out_bf16) ((__nv_bfloat16*)out)[dst] = __float2bfloat16_rn(v);
+  else ((float*)out)[dst] = v;
+}
+
+__global__ void k_gather_sum(const float* __restrict__ in, void* out, int out_bf16,
+                             const __grid_constant__ GatherArgs a, long long n) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x)
+    gather_one(in, out, out_bf16, a, e);
+}
+
+constexpr long long kGatherChunk = 4096;
+
+// Many gathers in one launch: chunk c belongs to the record whose
+// [chunk_start, next chunk_start) range holds it.
+__global__ void k_gather_group(const GatherRec* __restrict__ recs, int count, long long total_chunks) {
+  for (long long c = blockIdx.x; c < total_chunks; c += gridDim.x) {
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (recs[mid].chunk_start <= c) lo = mid; else hi = mid - 1;
+    }
+    const GatherRec& r = recs[lo];
+    const long long e0 = (c - r.chunk_start) * kGatherChunk;
+    const long long e1 = min(e0 + kGatherChunk, r.n);
+    for (long long e = e0 + threadIdx.x; e < e1; e += blockDim.x) gather_one(r.src, r.dst, r.dst_bf16, r.a, e);
   }
 }
 
-template <typename TO>
-static int launch_gather(const float* in, TO* out, const GatherArgs& a, long long n, cudaStream_t st) {
+static int launch_gather(const float* in, void* out, bool bf16, const GatherArgs& a, long long n, cudaStream_t st) {
   if (n == 0) return BBX_OK;
   long long blocks = (n + 255) / 256;
   if (blocks > 148 * 16) blocks = 148 * 16;
-  k_gather_sum<TO><<<(int)blocks, 256, 0, st>>>(in, out, a, n);
+  k_gather_sum<<<(int)blocks, 256, 0, st>>>(in, out, bf16 ? 1 : 0, a, n);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_error(BBX_ERR_CUDA, "k_gather_sum: %s", cudaGetErrorString(e));
   return BBX_OK;
@@ -78,19 +94,11 @@ static int launch_gather(const float* in, TO* out, const GatherArgs& a, long lon
 
 enum { CI = 0, CN = 1, CB = 2, CK = 3, CL = 4, CR = 5 };
 
-}  // namespace bbx
-
-using namespace bbx;
-
-extern "C" int bbx_contraction(const float* lhs, int rank_l, const long long* dims_l,
-                               const int* modes_l, const float* rhs, int rank_r,
-                               const long long* dims_r, const int* modes_r, float* out, int rank_o,
-                               const int* modes_o, float alpha, int precision, void* stream) {
-  if (!lhs || !rhs || !out) return set_error(BBX_ERR_INVALID, "null tensor");
+int lower_contraction(int rank_l, const long long* dims_l, const int* modes_l, int rank_r,
+                      const long long* dims_r, const int* modes_r, int rank_o, const int* modes_o,
+                      bool bf16, ContractionLowering* L) {
   if (rank_l < 0 || rank_l > 4 || rank_r < 0 || rank_r > 4 || rank_o < 0 || rank_o > 4)
     return set_error(BBX_ERR_INVALID, "ranks must be in [0,4] (MAXRANK of the cutensor format)");
-  if (precision != BBX_F32 && precision != BBX_BF16)
-    return set_error(BBX_ERR_UNSUPPORTED, "contraction precision %d", precision);
   constexpr int MAXM = 16;
   long long ext[MAXM];
   bool inl[MAXM] = {}, inr[MAXM] = {}, ino[MAXM] = {};
@@ -134,16 +142,17 @@ extern "C" int bbx_contraction(const float* lhs, int rank_l, const long long* di
   for (int d = 0; d < rank_r; ++d)
     if (cls(modes_r[d]) == CR) gR.push_back(modes_r[d]);
   auto prod = [&](const std::vector<int>& g) { long long p = 1; for (int m : g) p *= ext[m]; return p; };
-  const long long nb = prod(gB), nm = prod(gI), nn = prod(gN), nk = prod(gK);
-  if (nb == 0 || nm == 0 || nn == 0) return BBX_OK;  // empty output
-  if (nm > (1ll << 31) - 1 || nn > (1ll << 31) - 1 || nk > (1ll << 31) - 1)
+  memset(L, 0, sizeof(*L));
+  L->nb = prod(gB);
+  L->nm = prod(gI);
+  L->nn = prod(gN);
+  const long long nk = prod(gK);
+  L->empty = L->nb == 0 || L->nm == 0 || L->nn == 0;
+  if (L->empty) return BBX_OK;
+  if (L->nm > (1ll << 31) - 1 || L->nn > (1ll << 31) - 1 || nk > (1ll << 31) - 1)
     return set_error(BBX_ERR_INVALID, "contraction group too large");
-
-  cudaStream_t st = (cudaStream_t)stream;
-  const bool bf16 = precision == BBX_BF16;
-  const long long kdim = nk > 0 ? nk : 1;  // no contracted mode: an outer product, k = 1
-  const long long pk = bf16 ? ((kdim + 7) / 8) * 8 : kdim;
-  const int esz = bf16 ? 2 : 4;
+  L->kdim = nk > 0 ? nk : 1;  // no contracted mode: an outer product, k = 1
+  L->pk = bf16 ? ((L->kdim + 7) / 8) * 8 : L->kdim;
 
   // Column-major group flattening: stride of each mode inside its group.
   auto group_strides = [&](const std::vector<int>& g, long long base, long long* st_of) {
@@ -174,86 +183,139 @@ extern "C" int bbx_contraction(const float* lhs, int rank_l, const long long* di
       a->sdims[d] = ext[summed[d]];
       a->sstride[d] = src_stride[summed[d]];
     }
+    if (a->rank_o == 0) { a->rank_o = 1; a->odims[0] = 1; }  // empty groups behave as extent 1
   };
-  // Empty groups behave as extent 1 (prod() of nothing), so rank-0 pieces work.
-  GatherArgs ga, gb;
-  make_gather(gB, gI, gK, gL, strl, nm, pk, &ga);
-  make_gather(gB, gN, gK, gR, strr, nn, pk, &gb);
-  if (ga.rank_o == 0) { ga.rank_o = 1; ga.odims[0] = 1; }
-  if (gb.rank_o == 0) { gb.rank_o = 1; gb.odims[0] = 1; }
+  make_gather(gB, gI, gK, gL, strl, L->nm, L->pk, &L->ga);
+  make_gather(gB, gN, gK, gR, strr, L->nn, L->pk, &L->gb);
+  L->nl = L->nb * L->nm * L->kdim;
+  L->nr = L->nb * L->nn * L->kdim;
 
   // Direct write when the output order is I..., N..., B...
-  bool direct = true;
+  L->direct = true;
   int last = -1;
   for (int d = 0; d < rank_o; ++d) {
     int c = cls(modes_o[d]);
     int rank_c = c == CI ? 0 : c == CN ? 1 : 2;
-    if (rank_c < last) direct = false;
+    if (rank_c < last) L->direct = false;
     last = rank_c;
   }
+  // Ct[b][n][m] -> column-major output in modes_o order
+  long long src_of[MAXM] = {};
+  group_strides(gI, 1, src_of);
+  group_strides(gN, L->nm, src_of);
+  group_strides(gB, L->nm * L->nn, src_of);
+  long long p = 1, ostr[MAXM] = {};
+  for (int d = 0; d < rank_o; ++d) { ostr[modes_o[d]] = p; p *= ext[modes_o[d]]; }
+  L->go.rank_o = rank_o;
+  for (int d = 0; d < rank_o; ++d) {
+    int m = modes_o[rank_o - 1 - d];
+    L->go.odims[d] = ext[m];
+    L->go.istride[d] = src_of[m];
+    L->go.ostride[d] = ostr[m];
+  }
+  if (L->go.rank_o == 0) { L->go.rank_o = 1; L->go.odims[0] = 1; }
+  L->no = p;
+  return BBX_OK;
+}
 
+struct GatherPlan {
+  GatherRec* d = nullptr;
+  int count = 0;
+  long long total = 0;
+};
+
+int gather_plan_create(const GatherRec* recs, int count, GatherPlan** out) {
+  if (!recs || count <= 0 || !out) return set_error(BBX_ERR_INVALID, "bad gather plan");
+  std::vector<GatherRec> h(recs, recs + count);
+  long long chunks = 0;
+  for (auto& r : h) {
+    r.chunk_start = chunks;
+    chunks += (r.n + kGatherChunk - 1) / kGatherChunk;
+  }
+  auto* p = new GatherPlan();
+  p->count = count;
+  p->total = chunks;
+  cudaError_t e = cudaMalloc(&p->d, sizeof(GatherRec) * count);
+  if (e == cudaSuccess) e = cudaMemcpy(p->d, h.data(), sizeof(GatherRec) * count, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    if (p->d) cudaFree(p->d);
+    delete p;
+    return set_error(BBX_ERR_CUDA, "gather plan upload: %s", cudaGetErrorString(e));
+  }
+  *out = p;
+  return BBX_OK;
+}
+
+int gather_plan_launch(GatherPlan* p, void* stream) {
+  if (!p || p->total == 0) return BBX_OK;
+  long long grid = std::min<long long>(p->total, 148 * 8);
+  k_gather_group<<<(int)grid, 256, 0, (cudaStream_t)stream>>>(p->d, p->count, p->total);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(BBX_ERR_CUDA, "k_gather_group: %s", cudaGetErrorString(e));
+  return BBX_OK;
+}
+
+void gather_plan_destroy(GatherPlan* p) {
+  if (!p) return;
+  if (p->d) cudaFree(p->d);
+  delete p;
+}
+
+}  // namespace bbx
+
+using namespace bbx;
+
+extern "C" int bbx_contraction(const float* lhs, int rank_l, const long long* dims_l,
+                               const int* modes_l, const float* rhs, int rank_r,
+                               const long long* dims_r, const int* modes_r, float* out, int rank_o,
+                               const int* modes_o, float alpha, int precision, void* stream) {
+  if (!lhs || !rhs || !out) return set_error(BBX_ERR_INVALID, "null tensor");
+  if (precision != BBX_F32 && precision != BBX_BF16)
+    return set_error(BBX_ERR_UNSUPPORTED, "contraction precision %d", precision);
+  const bool bf16 = precision == BBX_BF16;
+  ContractionLowering L;
+  int rc = lower_contraction(rank_l, dims_l, modes_l, rank_r, dims_r, modes_r, rank_o, modes_o, bf16, &L);
+  if (rc) return rc;
+  if (L.empty) return BBX_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int esz = bf16 ? 2 : 4;
   void *Lc = nullptr, *Rc = nullptr;
   float* Ct = nullptr;
   cudaError_t e;
-  e = cudaMallocAsync(&Lc, (size_t)(nb * nm * pk * esz + 16), st);
+  e = cudaMallocAsync(&Lc, (size_t)(L.nb * L.nm * L.pk * esz + 16), st);
   if (e != cudaSuccess) return set_error(BBX_ERR_CUDA, "cudaMallocAsync: %s", cudaGetErrorString(e));
-  e = cudaMallocAsync(&Rc, (size_t)(nb * nn * pk * esz + 16), st);
+  e = cudaMallocAsync(&Rc, (size_t)(L.nb * L.nn * L.pk * esz + 16), st);
   if (e != cudaSuccess) { cudaFreeAsync(Lc, st); return set_error(BBX_ERR_CUDA, "cudaMallocAsync: %s", cudaGetErrorString(e)); }
-  if (!direct) {
-    e = cudaMallocAsync((void**)&Ct, (size_t)(nb * nn * nm * 4), st);
+  if (!L.direct) {
+    e = cudaMallocAsync((void**)&Ct, (size_t)(L.nb * L.nn * L.nm * 4), st);
     if (e != cudaSuccess) { cudaFreeAsync(Lc, st); cudaFreeAsync(Rc, st); return set_error(BBX_ERR_CUDA, "cudaMallocAsync: %s", cudaGetErrorString(e)); }
   }
-  float* C = direct ? out : Ct;
-  int rc = BBX_OK;
-  const long long nl = nb * nm * kdim, nr = nb * nn * kdim;
-  if (bf16) {
-    rc = launch_gather<__nv_bfloat16>(lhs, (__nv_bfloat16*)Lc, ga, nl, st);
-    if (!rc) rc = launch_gather<__nv_bfloat16>(rhs, (__nv_bfloat16*)Rc, gb, nr, st);
-  } else {
-    rc = launch_gather<float>(lhs, (float*)Lc, ga, nl, st);
-    if (!rc) rc = launch_gather<float>(rhs, (float*)Rc, gb, nr, st);
-  }
+  float* C = L.direct ? out : Ct;
+  rc = launch_gather(lhs, Lc, bf16, L.ga, L.nl, st);
+  if (!rc) rc = launch_gather(rhs, Rc, bf16, L.gb, L.nr, st);
   if (!rc) {
-    const long long pitch = pk;
+    const long long pitch = L.pk;
     if (!bf16) {
-      rc = bbx_matmul_f32((const float*)Rc, (const float*)Lc, C, (int)nn, (int)nm, (int)kdim, pitch,
-                          pitch, nm, 0, 1, alpha, 0.f, nullptr, 0, (int)nb, nn * pitch, nm * pitch,
-                          nn * nm, stream);
+      rc = bbx_matmul_f32((const float*)Rc, (const float*)Lc, C, (int)L.nn, (int)L.nm, (int)L.kdim, pitch,
+                          pitch, L.nm, 0, 1, alpha, 0.f, nullptr, 0, (int)L.nb, L.nn * pitch, L.nm * pitch,
+                          L.nn * L.nm, stream);
     } else {
-      std::vector<bbx_tc_problem_t> probs((size_t)nb);
-      for (long long b = 0; b < nb; ++b) {
+      std::vector<bbx_tc_problem_t> probs((size_t)L.nb);
+      for (long long b = 0; b < L.nb; ++b) {
         bbx_tc_problem_t& q = probs[(size_t)b];
         memset(&q, 0, sizeof(q));
-        q.a = (const __nv_bfloat16*)Rc + b * nn * pitch;
-        q.b = (const __nv_bfloat16*)Lc + b * nm * pitch;
-        q.c = C + b * nn * nm;
-        q.m = (int)nn; q.n = (int)nm; q.k = (int)kdim;
+        q.a = (const __nv_bfloat16*)Rc + b * L.nn * pitch;
+        q.b = (const __nv_bfloat16*)Lc + b * L.nm * pitch;
+        q.c = C + b * L.nn * L.nm;
+        q.m = (int)L.nn; q.n = (int)L.nm; q.k = (int)L.kdim;
         q.trans_a = 0; q.trans_b = 1;
-        q.lda = pitch; q.ldb = pitch; q.ldc = nm;
+        q.lda = pitch; q.ldb = pitch; q.ldc = L.nm;
         q.alpha = alpha; q.beta = 0.f;
       }
-      rc = bbx_matmul_tc(BBX_BF16, probs.data(), (int)nb, 0, stream);
+      rc = bbx_matmul_tc(BBX_BF16, probs.data(), (int)L.nb, 0, stream);
     }
   }
-  if (!rc && !direct) {
-    // Ct[b][n][m] -> column-major output in modes_o order.
-    long long src_of[MAXM] = {};
-    group_strides(gI, 1, src_of);
-    group_strides(gN, nm, src_of);
-    group_strides(gB, nm * nn, src_of);
-    GatherArgs go;
-    memset(&go, 0, sizeof(go));
-    long long p = 1, ostr[MAXM] = {};
-    for (int d = 0; d < rank_o; ++d) { ostr[modes_o[d]] = p; p *= ext[modes_o[d]]; }
-    go.rank_o = rank_o;
-    for (int d = 0; d < rank_o; ++d) {
-      int m = modes_o[rank_o - 1 - d];
-      go.odims[d] = ext[m];
-      go.istride[d] = src_of[m];
-      go.ostride[d] = ostr[m];
-    }
-    rc = launch_gather<float>(Ct, out, go, p, st);
-  }
+  if (!rc && !L.direct) rc = launch_gather(Ct, out, false, L.go, L.no, st);
   cudaFreeAsync(Lc, st);
   cudaFreeAsync(Rc, st);
   if (Ct) cudaFreeAsync(Ct, st);

@@ -328,4 +328,259 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
   }
 }
 
+// ============================================================================
+// 2-SM variant: a cluster of two CTAs computes one 256 x 256 tile with
+// tcgen05.mma.cta_group::2 (M = 256 split over the pair's TMEM, N = 256 split
+// over the pair's shared memory). Each CTA TMA-loads only ITS half of A (128
+// rows) and of B (128 rows / columns) -- no multicast -- so the operand bytes
+// each SM pulls per FLOP are a third lower than the 1-SM 128 x 256 tile and the
+// 32 KiB stages allow a 6-deep ring. Both CTAs' loads complete on the leader's
+// full barrier; the leader's single MMA thread commits each stage back to the
+// empty barriers of both CTAs and each accumulator to both CTAs' tfull
+// barriers; both epilogues release the accumulator on the leader's tempty.
+// bf16 only.
+// ============================================================================
+template <bool A_MN, bool B_MN>
+struct Tc2Cfg {
+  static constexpr int BM = 256;  // rows per pair (128 per CTA)
+  static constexpr int BN = 256;  // columns per pair (128 B rows per CTA)
+  static constexpr int BK = 64;
+  static constexpr int UMMA_K = 16;
+  static constexpr int A_BYTES = 128 * 128;  // 128 rows x 128 B
+  static constexpr int B_BYTES = 128 * 128;
+  static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+  static constexpr int STAGES = 6;
+  static constexpr int TMEM_COLS = 512;
+  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+  static constexpr int THREADS = 192;
+};
+
+template <bool A_MN, bool B_MN>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
+    tc_gemm2_kernel(const __grid_constant__ TcArgs args) {
+  using C = Tc2Cfg<A_MN, B_MN>;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t* stage_base = smem;
+  uint64_t* bars = (uint64_t*)(smem + C::STAGES * C::STAGE_BYTES);
+  uint64_t* full_bar = bars;
+  uint64_t* empty_bar = bars + C::STAGES;
+  uint64_t* tfull_bar = bars + 2 * C::STAGES;
+  uint64_t* tempty_bar = bars + 2 * C::STAGES + 2;
+  uint32_t* tmem_slot = (uint32_t*)(bars + 2 * C::STAGES + 4);
+  volatile uint32_t* status = args.status;
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_ctarank();
+  const bool leader = rank == 0;
+  const int pair = blockIdx.x >> 1, num_pairs = gridDim.x >> 1;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < C::STAGES; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull_bar[b], 1);
+      mbar_init(&tempty_bar[b], 256);  // both CTAs' epilogue threads
+    }
+    fence_mbar_init();
+  }
+  if (warp == 1) tmem_alloc_2sm(tmem_slot, C::TMEM_COLS);
+  tc_fence_before();
+  __syncthreads();
+  __syncwarp();
+  cluster_sync();  // peer barriers initialised before any remote arrive / complete_tx
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producer (both CTAs)
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      bool ok = true;
+      for (int t = pair; t < args.total_tiles && ok; t += num_pairs) {
+        int p, tm, tn;
+        tc_locate(args, t, p, tm, tn);
+        const TcProblem* pr = tc_problem(args, p);
+        const int kb_n = (pr->k + C::BK - 1) / C::BK;
+        for (int kb = 0; kb < kb_n; ++kb) {
+          if (!mbar_wait(&empty_bar[s], ph ^ 1, status, DEV_TIMEOUT_EMPTY)) { ok = false; break; }
+          uint8_t* sa = stage_base + s * C::STAGE_BYTES;
+          uint8_t* sb = sa + C::A_BYTES;
+          if (leader) mbar_arrive_expect_tx(&full_bar[s], 2 * C::STAGE_BYTES);
+          const uint32_t bar = mapa_shared(smem_u32(&full_bar[s]), 0);
+          const int k0 = kb * C::BK;
+          const int row_a = tm * C::BM + (int)rank * 128;
+          const int row_b = tn * C::BN + (int)rank * 128;
+          if constexpr (!A_MN) {
+            tma_load_2d_2sm(sa, &pr->tmap_a, bar, k0, row_a);
+          } else {
+            tma_load_2d_2sm(sa, &pr->tmap_a, bar, row_a, k0);
+            tma_load_2d_2sm(sa + C::BK * 128, &pr->tmap_a, bar, row_a + 64, k0);
+          }
+          if constexpr (!B_MN) {
+            tma_load_2d_2sm(sb, &pr->tmap_b, bar, k0, row_b);
+          } else {
+            tma_load_2d_2sm(sb, &pr->tmap_b, bar, row_b, k0);
+            tma_load_2d_2sm(sb + C::BK * 128, &pr->tmap_b, bar, row_b + 64, k0);
+          }
+          if (++s == C::STAGES) { s = 0; ph ^= 1; }
+        }
+      }
+      for (int i = 0; i < C::STAGES; ++i) {
+        if (!mbar_wait(&empty_bar[s], ph ^ 1, status, DEV_TIMEOUT_EMPTY)) break;
+        if (++s == C::STAGES) { s = 0; ph ^= 1; }
+      }
+      if (*status != DEV_OK) {
+        const long long t0 = clock64();
+        while (clock64() - t0 < 200000) {}
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------------ MMA issuer (leader CTA only)
+    if (leader && lane == 0) {
+      constexpr uint32_t idesc = make_idesc(256, 256, 1u, A_MN, B_MN);
+      int s = 0;
+      uint32_t ph = 0;
+      int acc = 0;
+      uint32_t acc_ph = 0;
+      bool ok = true;
+      for (int t = pair; t < args.total_tiles && ok; t += num_pairs) {
+        int p, tm, tn;
+        tc_locate(args, t, p, tm, tn);
+        const TcProblem* pr = tc_problem(args, p);
+        const int kb_n = (pr->k + C::BK - 1) / C::BK;
+        if (!mbar_wait(&tempty_bar[acc], acc_ph ^ 1, status, DEV_TIMEOUT_TMEM_EMPTY)) break;
+        tc_fence_after();
+        const uint32_t d_tmem = tmem_base + acc * C::BN;
+        for (int kb = 0; kb < kb_n; ++kb) {
+          if (!mbar_wait(&full_bar[s], ph, status, DEV_TIMEOUT_FULL)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t sa = smem_u32(stage_base + s * C::STAGE_BYTES);
+          const uint32_t sb = sa + C::A_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < C::BK / C::UMMA_K; ++kk) {
+            uint64_t da, db;
+            if constexpr (!A_MN) da = smem_desc_sw128(sa + kk * 32, 16, 1024);
+            else da = smem_desc_sw128(sa + kk * (C::UMMA_K * 128), C::BK * 128, 1024);
+            if constexpr (!B_MN) db = smem_desc_sw128(sb + kk * 32, 16, 1024);
+            else db = smem_desc_sw128(sb + kk * (C::UMMA_K * 128), C::BK * 128, 1024);
+            umma_f16_2sm(d_tmem, da, db, idesc, (kb > 0 || kk > 0) ? 1u : 0u);
+          }
+          umma_commit_2sm(&empty_bar[s], 0x3);
+          if (++s == C::STAGES) { s = 0; ph ^= 1; }
+        }
+        if (!ok) break;
+        umma_commit_2sm(&tfull_bar[acc], 0x3);
+        if (++acc == 2) { acc = 0; acc_ph ^= 1; }
+      }
+    }
+  } else {
+    // ------------------------------------------------------------ epilogue (both CTAs)
+    const int lane_base = 32 * (warp & 3);
+    const uint32_t tempty_leader0 = mapa_shared(smem_u32(&tempty_bar[0]), 0);
+    const uint32_t tempty_leader1 = mapa_shared(smem_u32(&tempty_bar[1]), 0);
+    int acc = 0;
+    uint32_t acc_ph = 0;
+    for (int t = pair; t < args.total_tiles; t += num_pairs) {
+      int p, tm, tn;
+      tc_locate(args, t, p, tm, tn);
+      const TcProblem* pr = tc_problem(args, p);
+      const bool got = mbar_wait(&tfull_bar[acc], acc_ph, status, DEV_TIMEOUT_TMEM_FULL);
+      if (!__all_sync(0xffffffffu, got)) break;
+      tc_fence_after();
+      const int row = tm * C::BM + (int)rank * 128 + lane_base + lane;
+      const bool row_ok = row < pr->m;
+      const int flags = pr->flags;
+      const float alpha = pr->alpha, beta = pr->beta;
+      const long long ldc = pr->ldc;
+      const int n = pr->n;
+      const uint32_t t_row = tmem_base + acc * C::BN + ((uint32_t)lane_base << 16);
+      for (int c = 0; c < C::BN / 16; ++c) {
+        const int col0 = tn * C::BN + c * 16;
+        if (col0 >= n) break;  // warp-uniform
+        float v[16];
+        tmem_ld16(t_row + c * 16, v);
+        if (!row_ok) continue;
+        const bool full = (col0 + 16 <= n);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          float x = v[i] * alpha;
+          if ((flags & EPI_BIAS) && (full || col0 + i < n)) x += pr->bias[col0 + i];
+          v[i] = x;
+        }
+        if (flags & EPI_OUT_BF16) {
+          __nv_bfloat16* cp = (__nv_bfloat16*)pr->c + (long long)row * ldc + col0;
+          if (flags & EPI_BETA) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+              if (full || col0 + i < n) v[i] += beta * __bfloat162float(cp[i]);
+          }
+          if (flags & EPI_RELU) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i], 0.f);
+          }
+          if (full && ((((uintptr_t)cp) & 15) == 0)) {
+            uint4 pk[2];
+            __nv_bfloat162* h = (__nv_bfloat162*)pk;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) h[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+            ((uint4*)cp)[0] = pk[0];
+            ((uint4*)cp)[1] = pk[1];
+          } else {
+            for (int i = 0; i < 16; ++i)
+              if (col0 + i < n) cp[i] = __float2bfloat16_rn(v[i]);
+          }
+        } else {
+          float* cp = (float*)pr->c + (long long)row * ldc + col0;
+          const bool vec = full && ((((uintptr_t)cp) & 15) == 0);
+          if (flags & EPI_BETA) {
+            if (vec) {
+#pragma unroll
+              for (int q = 0; q < 4; ++q) {
+                float4 o = ((const float4*)cp)[q];
+                v[4 * q + 0] += beta * o.x; v[4 * q + 1] += beta * o.y;
+                v[4 * q + 2] += beta * o.z; v[4 * q + 3] += beta * o.w;
+              }
+            } else {
+              for (int i = 0; i < 16; ++i)
+                if (col0 + i < n) v[i] += beta * cp[i];
+            }
+          }
+          if (flags & EPI_RELU) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i], 0.f);
+          }
+          if (vec) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              ((float4*)cp)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+          } else {
+            for (int i = 0; i < 16; ++i)
+              if (col0 + i < n) cp[i] = v[i];
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive_cluster(acc == 0 ? tempty_leader0 : tempty_leader1);
+      if (++acc == 2) { acc = 0; acc_ph ^= 1; }
+    }
+  }
+
+  // the leader's MMAs read the peer's shared memory: neither CTA may release
+  // TMEM or exit before both are done
+  tc_fence_before();
+  __syncthreads();
+  __syncwarp();
+  cluster_sync();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc_2sm(tmem_base, C::TMEM_COLS);
+  }
+}
+
 }  // namespace bbx

@@ -118,9 +118,9 @@ meta_fn same_meta = [](const params_t&, const margs_t& in, margs_t& out) {
 
 // One grouped-stream op on a dense block of any element type (f32 / bf16).
 void dense_stream(const params_t& p, int kind, int op, const std::vector<const tensor_t*>& ins,
-                  tensor_t& out, int dtype, float p0, float p1) {
+                  tensor_t& out, int dtype, float p0, float p1, int out_dtype = -1) {
   bbx_stream_op_t s{};
-  s.kind = kind; s.op = op; s.in_dtype = dtype; s.out_dtype = dtype;
+  s.kind = kind; s.op = op; s.in_dtype = dtype; s.out_dtype = out_dtype < 0 ? dtype : out_dtype;
   s.n_in = (int)ins.size(); s.kahan = 1;
   const auto& m = dm(ins[0]->_meta);
   s.n = (long long)m.num_rows * m.num_cols;
@@ -303,6 +303,15 @@ void register_b200_udfs(udf_manager_t& udm) {
           ew_hint, same_meta));
     }
   }
+
+  // relu of an f32 block written as bf16 (the activation of a layer whose
+  // pre-activation was accumulated in f32)
+  add_impl(udm, std::make_unique<b200_impl_t>(
+      "b200_dense_relu_to_bf16", "matrix_relu", V{"dense"}, V{"dense_bf16"}, std::vector<int32_t>{},
+      [](const params_t& p, const targs_t& in, targs_t& out) {
+        dense_stream(p, BBX_S_UNARY, BBX_U_RELU, {&in.get<0>()}, out.get<0>(), BBX_F32, 0, 0, BBX_BF16);
+      },
+      ew_hint, same_meta));
 
   // ---- FNN application uds (applications/fnn/ffnn_lib_init.cc:20-177)
   register_ud(udm, "ffnn_act_mult", false, false, 2, 1);

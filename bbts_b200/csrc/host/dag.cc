@@ -1,28 +1,42 @@
 // Grouped DAG executor.
 //
 // A compiled command list (APPLY / REDUCE / DELETE) is lowered once into
-// waves. Every wave issues at most: the grouped streaming launches of its
-// add / reduce / elementwise nodes, one grouped tcgen05 launch per operand
-// layout class of its block matmuls, and direct calls of the remaining impls
-// (FP32 SIMT matmul, contraction, FNN ops). Intermediate blocks live in one
-// arena whose offsets come from a lifetime-based first-fit plan, and the whole
-// launch sequence is captured into one CUDA graph that dag_launch replays.
+// waves of launch groups:
+//   PRE     one grouped gather launch: the operand gathers of the wave's
+//           tensor-core contractions (Lc / Rc staging blocks)
+//   STREAM  grouped streaming launches: every add / n-ary reduce / elementwise
+//           node of the wave (more than 16 reduce inputs chain extra phases)
+//   OTHER   direct calls of the remaining impls (FP32 SIMT matmul, FP32
+//           contraction, FNN ops, softmax, uniform)
+//   TC      one grouped tcgen05 launch per operand-layout class: the wave's
+//           block matmuls and contraction matmuls
+//   POST    one grouped gather launch: contraction outputs whose mode order
+//           needs a final permutation
+// TC groups run on a tensor stream, everything else on a memory stream, and
+// the launches are captured into ONE CUDA graph whose edges are the true
+// tensor dependencies between groups plus a wave barrier two waves back, so a
+// wave's HBM-bound streaming work overlaps its tensor-core work and the next
+// wave's. Intermediate blocks share one arena: a slot is reused only by a block
+// defined at least two waves after the slot's last reader (the barrier makes
+// that reader finished).
 //
 // Scheduling policies (what the learned cost model changes):
-//   heuristic  waves = ASAP levels; matmul tiles in reservation-station LIFO
-//              order; costs = the ud's complexity hint.
-//   learned    nodes get the MLP's predicted latency; a node with slack is
-//              placed in the wave (within [ASAP, ALAP]) with the least
-//              predicted load, and each grouped launch orders its problems by
-//              predicted cost, longest first.
+//   heuristic  waves = ASAP levels; problems of a grouped launch in
+//              reservation-station LIFO order; costs = complexity hints.
+//   learned    nodes carry the MLP's predicted latency and a resource (tensor
+//              or memory); a node with slack goes to the wave within
+//              [ASAP, ALAP] that least increases max(tensor time, memory time)
+//              of that wave, and grouped launches order problems longest first.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <map>
 #include <mutex>
+#include <set>
 #include <stdexcept>
 #include <string>
+#include "contraction.h"
 #include "runtime.h"
 
 namespace bbts {
@@ -44,8 +58,10 @@ struct node_t {
   const command_t* cmd;
   ud_impl_t* impl;
   node_kind_t kind;
+  bool tc_contract = false;  // bf16 contraction lowered into PRE / TC / POST groups
   std::vector<tid_t> ins, outs;
   int asap = 0, height = 0, wave = 0;
+  int resource = 1;          // 0 tensor stream, 1 memory stream
   double cost = 1.0, flops = 0.0, bytes = 0.0;
   std::vector<int> preds, succs;
 };
@@ -62,20 +78,26 @@ struct opaque_t {
   ud_impl_t* impl;
   std::vector<command_param_t> params;
   std::vector<tid_t> ins, outs;
-  bool reduce = false;
 };
 
-struct wave_t {
-  std::vector<bbx_stream_plan_t*> phases;  // in order
-  std::vector<bbx_tc_plan_t*> tc;
+enum group_kind_t { G_PRE = 0, G_STREAM = 1, G_OTHER = 2, G_TC = 3, G_POST = 4 };
+
+struct group_t {
+  group_kind_t kind;
+  int wave;
+  std::vector<tid_t> reads, writes;
+  bbx_stream_plan_t* stream_plan = nullptr;
+  bbx_tc_plan_t* tc_plan = nullptr;
+  bbx::GatherPlan* gather_plan = nullptr;
   std::vector<opaque_t> opaque;
+  std::vector<int> deps;  // indices of earlier groups this one waits for
 };
 
 }  // namespace
 
 struct dag_t {
   runtime_t* rt = nullptr;
-  std::vector<wave_t> waves;
+  std::vector<group_t> groups;
   std::unordered_map<tid_t, tplan_t> tensors;
   std::unordered_map<tid_t, std::unique_ptr<char[]>> headers;
   void* arena = nullptr;
@@ -109,6 +131,18 @@ void run_opaque(dag_t* d, opaque_t& o, cudaStream_t st) {
   for (tid_t t : o.outs) outs.push_back(header(d, t));
   ud_impl_t::tensor_args_t ia(ins), oa(outs);
   o.impl->call_ud(params, ia, oa);
+}
+
+void launch_group(dag_t* d, group_t& g, cudaStream_t st) {
+  switch (g.kind) {
+    case G_PRE:
+    case G_POST: dag_bbx(bbx::gather_plan_launch(g.gather_plan, st)); break;
+    case G_STREAM: dag_bbx(bbx_stream_plan_launch(g.stream_plan, st)); break;
+    case G_TC: dag_bbx(bbx_tc_plan_launch(g.tc_plan, st)); break;
+    case G_OTHER:
+      for (auto& o : g.opaque) run_opaque(d, o, st);
+      break;
+  }
 }
 
 // ---------------------------------------------------------------- tile autotuner
@@ -189,12 +223,21 @@ int autotune_tile_n(int dtype, bool ta, bool tb, const std::vector<bbx_tc_proble
   return best;
 }
 
-void issue(dag_t* d, cudaStream_t st) {
-  for (auto& w : d->waves) {
-    for (auto* p : w.phases) dag_bbx(bbx_stream_plan_launch(p, st));
-    for (auto* p : w.tc) dag_bbx(bbx_tc_plan_launch(p, st));
-    for (auto& o : w.opaque) run_opaque(d, o, st);
-  }
+// Contraction params: rank_l, rank_r, rank_o, modes_l..., modes_r..., modes_o..., alpha.
+struct cparams_t {
+  std::vector<int> ml, mr, mo;
+  float alpha;
+};
+cparams_t parse_contraction(const command_t& c) {
+  auto p = c.get_parameters();
+  cparams_t r;
+  int rl = p[0].i, rr = p[1].i, ro = p[2].i;
+  size_t i = 3;
+  for (int d = 0; d < rl; ++d) r.ml.push_back(p[i++].i);
+  for (int d = 0; d < rr; ++d) r.mr.push_back(p[i++].i);
+  for (int d = 0; d < ro; ++d) r.mo.push_back(p[i++].i);
+  r.alpha = p[i].f;
+  return r;
 }
 
 }  // namespace
@@ -235,11 +278,15 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
     n.kind = classify(n.impl, c.is_reduce());
     if (c.is_reduce() && n.kind != NK_SUM)
       throw std::runtime_error("DAG: REDUCE is supported for matrix_add over dense / dense_bf16 blocks");
+    n.tc_contract = n.kind == NK_CONTRACT && n.impl->impl_name == "b200_contraction_bf16";
+    n.resource = (n.kind == NK_TC || n.tc_contract) ? 0 : 1;
     std::vector<tensor_meta_t> in_metas;
     for (size_t i = 0; i < c.get_num_inputs(); ++i) {
       tid_t t = c.get_input(i).tid;
       auto it = d->tensors.find(t);
-      if (it == d->tensors.end()) throw std::runtime_error("DAG: command " + std::to_string(c.id) + " reads tensor " + std::to_string(t) + " that nothing creates");
+      if (it == d->tensors.end())
+        throw std::runtime_error("DAG: command " + std::to_string(c.id) + " reads tensor " + std::to_string(t) +
+                                 " that nothing creates");
       in_metas.push_back(it->second.meta);
       n.ins.push_back(t);
       auto pit = producer.find(t);
@@ -269,7 +316,6 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
       producer[t] = idx;
       n.outs.push_back(t);
     }
-    // algorithmic work
     if (n.kind == NK_TC || n.kind == NK_SIMT) {
       const auto& ma = in_metas[0].as<dense_tensor_meta_t>().m();
       const auto& mb = in_metas[1].as<dense_tensor_meta_t>().m();
@@ -310,22 +356,59 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
   // ---- waves
   const int W = max_level + 1;
   if (policy == SCHED_LEARNED) {
-    std::vector<double> load(W, 0.0);
+    // tensor and memory streams overlap inside a wave: minimise sum_w max(tc_w, mem_w)
+    std::vector<double> load[2] = {std::vector<double>(W, 0.0), std::vector<double>(W, 0.0)};
     for (int i = 0; i < N; ++i) {  // command order is topological
       int lo = nodes[i].asap;
       for (int p : nodes[i].preds) lo = std::max(lo, nodes[p].wave + 1);
       int hi = std::max(lo, max_level - nodes[i].height);
+      const int r = nodes[i].resource;
       int best = lo;
-      for (int w = lo; w <= hi; ++w)
-        if (load[w] < load[best] - 1e-9) best = w;
+      double best_inc = 1e300;
+      for (int w = lo; w <= hi; ++w) {
+        double before = std::max(load[0][w], load[1][w]);
+        double after = std::max(load[r][w] + nodes[i].cost, load[1 - r][w]);
+        double inc = after - before;
+        if (inc < best_inc - 1e-12) { best_inc = inc; best = w; }
+      }
       nodes[i].wave = best;
-      load[best] += nodes[i].cost;
+      load[r][best] += nodes[i].cost;
     }
   } else {
     for (auto& n : nodes) n.wave = n.asap;
   }
   int nw = 0;
   for (auto& n : nodes) nw = std::max(nw, n.wave + 1);
+
+  // ---- contraction staging blocks (arena slots living for one wave)
+  struct cstage_t { tid_t lc, rc, ct; bbx::ContractionLowering L; cparams_t p; };
+  std::unordered_map<int, cstage_t> cstage;
+  tid_t next_stage = -1000000;
+  for (int i = 0; i < N; ++i) {
+    node_t& n = nodes[i];
+    if (!n.tc_contract) continue;
+    cstage_t cs;
+    cs.p = parse_contraction(*n.cmd);
+    const auto& sl = d->tensors.at(n.ins[0]).meta.as<cu_meta_t>().m();
+    const auto& sr = d->tensors.at(n.ins[1]).meta.as<cu_meta_t>().m();
+    std::vector<long long> dl(sl.dims, sl.dims + sl.rank), dr(sr.dims, sr.dims + sr.rank);
+    dag_bbx(bbx::lower_contraction((int)dl.size(), dl.data(), cs.p.ml.data(), (int)dr.size(), dr.data(),
+                                   cs.p.mr.data(), (int)cs.p.mo.size(), cs.p.mo.data(), true, &cs.L));
+    auto stage = [&](size_t bytes) {
+      tid_t t = next_stage--;
+      tplan_t tp;
+      std::memset(&tp.meta, 0, sizeof(tp.meta));
+      tp.bytes = bytes;
+      tp.def = tp.last = n.wave;
+      tp.deleted = true;
+      d->tensors[t] = tp;
+      return t;
+    };
+    cs.lc = stage((size_t)(cs.L.nb * cs.L.nm * cs.L.pk * 2 + 16));
+    cs.rc = stage((size_t)(cs.L.nb * cs.L.nn * cs.L.pk * 2 + 16));
+    cs.ct = cs.L.direct ? TID_NONE : stage((size_t)(cs.L.nb * cs.L.nn * cs.L.nm * 4));
+    cstage[i] = cs;
+  }
 
   // ---- tensor lifetimes
   for (int i = 0; i < N; ++i) {
@@ -340,8 +423,8 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
     }
   }
 
-  // ---- memory: deleted intermediates share one arena (first fit on disjoint
-  // lifetimes); results nobody deletes get their own allocations.
+  // ---- memory: deleted intermediates and staging blocks share one arena; a
+  // slot is reused only by a block defined two or more waves after its last use
   struct placed_t { size_t off, bytes; int def, last; };
   std::vector<placed_t> placed;
   std::vector<std::pair<tid_t, tplan_t*>> order;
@@ -357,7 +440,7 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
     const size_t bytes = (tp->bytes + 255) & ~(size_t)255;
     std::vector<std::pair<size_t, size_t>> busy;
     for (auto& p : placed)
-      if (!(p.last < tp->def || tp->last < p.def)) busy.push_back({p.off, p.off + p.bytes});
+      if (!(p.last + 1 < tp->def || tp->last + 1 < p.def)) busy.push_back({p.off, p.off + p.bytes});
     std::sort(busy.begin(), busy.end());
     size_t off = 0;
     for (auto& b : busy) {
@@ -381,18 +464,21 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
   }
   for (auto& kv : d->tensors) kv.second.meta.set_payload(kv.second.payload);
 
-  // ---- per-wave launch plans
+  // ---- launch groups per wave
   std::vector<std::vector<int>> by_wave(nw);
   for (int i = 0; i < N; ++i) by_wave[nodes[i].wave].push_back(i);
-  d->waves.resize(nw);
   for (int w = 0; w < nw; ++w) {
     auto& ids = by_wave[w];
     if (policy == SCHED_LEARNED)
       std::stable_sort(ids.begin(), ids.end(), [&](int a, int b) { return nodes[a].cost > nodes[b].cost; });
     else
       std::reverse(ids.begin(), ids.end());  // LIFO: the last queued ready command first
-    std::map<int, std::vector<bbx_tc_problem_t>> tc_groups;  // key: dtype | amn | bmn
+    std::map<int, std::vector<bbx_tc_problem_t>> tc_groups;  // key: dtype*4 + ta*2 + tb
+    std::map<int, std::pair<std::vector<tid_t>, std::vector<tid_t>>> tc_rw;
     std::vector<std::vector<bbx_stream_op_t>> phases(1);
+    std::vector<std::pair<std::vector<tid_t>, std::vector<tid_t>>> phase_rw(1);
+    std::vector<bbx::GatherRec> pre, post;
+    group_t gpre{G_PRE, w}, gpost{G_POST, w}, gother{G_OTHER, w};
     for (int i : ids) {
       node_t& n = nodes[i];
       const command_t& c = *n.cmd;
@@ -415,12 +501,55 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
         const int in_dt = elem_of(tf, ta_.meta.fmt_id);
         q.alpha = in_dt == ELEM_E4M3 ? ma.scale * mb.scale : 1.0f;
         q.flags = elem_of(tf, tc_.meta.fmt_id) == ELEM_BF16 ? BBX_EPI_OUT_BF16 : 0;
-        tc_groups[in_dt * 4 + (ta ? 2 : 0) + (tb ? 1 : 0)].push_back(q);
+        const int key = in_dt * 4 + (ta ? 2 : 0) + (tb ? 1 : 0);
+        tc_groups[key].push_back(q);
+        tc_rw[key].first.insert(tc_rw[key].first.end(), n.ins.begin(), n.ins.end());
+        tc_rw[key].second.push_back(n.outs[0]);
+      } else if (n.tc_contract) {
+        cstage_t& cs = cstage.at(i);
+        auto& L = cs.L;
+        if (!L.empty) {
+          auto& tl = d->tensors.at(cs.lc);
+          auto& tr = d->tensors.at(cs.rc);
+          bbx::GatherRec ra{}, rb{};
+          ra.a = L.ga; ra.src = (const float*)d->tensors.at(n.ins[0]).payload; ra.dst = tl.payload; ra.dst_bf16 = 1; ra.n = L.nl;
+          rb.a = L.gb; rb.src = (const float*)d->tensors.at(n.ins[1]).payload; rb.dst = tr.payload; rb.dst_bf16 = 1; rb.n = L.nr;
+          pre.push_back(ra);
+          pre.push_back(rb);
+          gpre.reads.insert(gpre.reads.end(), n.ins.begin(), n.ins.end());
+          gpre.writes.push_back(cs.lc);
+          gpre.writes.push_back(cs.rc);
+          void* C = L.direct ? d->tensors.at(n.outs[0]).payload : d->tensors.at(cs.ct).payload;
+          const int key = ELEM_BF16 * 4 + 0 + 1;  // A = Rc (K-major), B = Lc stored n x k (trans_b)
+          for (long long b = 0; b < L.nb; ++b) {
+            bbx_tc_problem_t q{};
+            q.a = (const char*)tr.payload + 2 * b * L.nn * L.pk;
+            q.b = (const char*)tl.payload + 2 * b * L.nm * L.pk;
+            q.c = (char*)C + 4 * b * L.nn * L.nm;
+            q.m = (int)L.nn; q.n = (int)L.nm; q.k = (int)L.kdim;
+            q.trans_a = 0; q.trans_b = 1;
+            q.lda = L.pk; q.ldb = L.pk; q.ldc = L.nm;
+            q.alpha = cs.p.alpha;
+            tc_groups[key].push_back(q);
+          }
+          tc_rw[key].first.push_back(cs.lc);
+          tc_rw[key].first.push_back(cs.rc);
+          tc_rw[key].second.push_back(L.direct ? n.outs[0] : cs.ct);
+          if (!L.direct) {
+            bbx::GatherRec ro{};
+            ro.a = L.go; ro.src = (const float*)d->tensors.at(cs.ct).payload; ro.dst = d->tensors.at(n.outs[0]).payload;
+            ro.dst_bf16 = 0; ro.n = L.no;
+            post.push_back(ro);
+            gpost.reads.push_back(cs.ct);
+            gpost.writes.push_back(n.outs[0]);
+          }
+        }
       } else if (n.kind == NK_SUM || n.kind == NK_UNARY || n.kind == NK_BINARY) {
         auto& to = d->tensors.at(n.outs[0]);
         const auto& m0 = d->tensors.at(n.ins[0]).meta.as<dense_tensor_meta_t>().m();
         const long long elems = (long long)m0.num_rows * m0.num_cols;
         const int dt = elem_of(tf, d->tensors.at(n.ins[0]).meta.fmt_id) == ELEM_BF16 ? BBX_BF16 : BBX_F32;
+        const int odt = elem_of(tf, to.meta.fmt_id) == ELEM_BF16 ? BBX_BF16 : BBX_F32;
         if (n.kind == NK_SUM) {
           size_t done = 0;
           int ph = 0;
@@ -429,10 +558,14 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
             s.kind = BBX_S_SUM; s.in_dtype = dt; s.out_dtype = dt; s.kahan = 1; s.n = elems; s.out = to.payload;
             int cnt = 0;
             if (done > 0) s.in[cnt++] = to.payload;  // keep folding into the output
+            const size_t first = done;
             while (cnt < BBX_STREAM_MAX_IN && done < n.ins.size()) s.in[cnt++] = d->tensors.at(n.ins[done++]).payload;
             s.n_in = cnt;
-            if ((int)phases.size() <= ph) phases.resize(ph + 1);
-            phases[ph++].push_back(s);
+            if ((int)phases.size() <= ph) { phases.resize(ph + 1); phase_rw.resize(ph + 1); }
+            phases[ph].push_back(s);
+            phase_rw[ph].first.insert(phase_rw[ph].first.end(), n.ins.begin() + first, n.ins.begin() + done);
+            phase_rw[ph].second.push_back(n.outs[0]);
+            ++ph;
           }
         } else {
           bbx_stream_op_t s{};
@@ -448,10 +581,12 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
             s.p0 = params.get_float_or_default<0>(1.f);
             s.p1 = params.get_float_or_default<1>(1.f);
           }
-          s.in_dtype = dt; s.out_dtype = dt; s.n = elems; s.out = to.payload;
+          s.in_dtype = dt; s.out_dtype = odt; s.n = elems; s.out = to.payload;
           s.n_in = n.kind == NK_UNARY ? 1 : 2;
           for (int j = 0; j < s.n_in; ++j) s.in[j] = d->tensors.at(n.ins[j]).payload;
           phases[0].push_back(s);
+          phase_rw[0].first.insert(phase_rw[0].first.end(), n.ins.begin(), n.ins.end());
+          phase_rw[0].second.push_back(n.outs[0]);
         }
       } else {
         opaque_t o;
@@ -460,66 +595,140 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
         o.params.assign(pl.begin(), pl.end());
         o.ins = n.ins;
         o.outs = n.outs;
-        d->waves[w].opaque.push_back(std::move(o));
+        gother.reads.insert(gother.reads.end(), n.ins.begin(), n.ins.end());
+        gother.writes.insert(gother.writes.end(), n.outs.begin(), n.outs.end());
+        gother.opaque.push_back(std::move(o));
       }
       d->stats.flops += n.flops;
       d->stats.bytes += n.bytes;
     }
-    for (auto& ph : phases) {
-      if (ph.empty()) continue;
-      bbx_stream_plan_t* p = nullptr;
-      dag_bbx(bbx_stream_plan_create(ph.data(), (int)ph.size(), &p));
-      d->waves[w].phases.push_back(p);
+    // group order inside a wave: PRE, STREAM phases, OTHER (memory stream); TC (tensor stream); POST
+    if (!pre.empty()) {
+      dag_bbx(bbx::gather_plan_create(pre.data(), (int)pre.size(), &gpre.gather_plan));
+      d->groups.push_back(std::move(gpre));
       d->stats.stream_launches++;
     }
+    for (size_t ph = 0; ph < phases.size(); ++ph) {
+      if (phases[ph].empty()) continue;
+      group_t g{G_STREAM, w};
+      dag_bbx(bbx_stream_plan_create(phases[ph].data(), (int)phases[ph].size(), &g.stream_plan));
+      g.reads = phase_rw[ph].first;
+      g.writes = phase_rw[ph].second;
+      d->groups.push_back(std::move(g));
+      d->stats.stream_launches++;
+    }
+    if (!gother.opaque.empty()) {
+      d->stats.opaque_launches += (int)gother.opaque.size();
+      d->groups.push_back(std::move(gother));
+    }
     for (auto& kv : tc_groups) {
-      bbx_tc_plan_t* p = nullptr;
+      group_t g{G_TC, w};
       const int dt = kv.first / 4;
       // tile_n < 0: autotune per group; 0: size heuristic; 128 / 256: forced
       const int tn = tile_n < 0 ? autotune_tile_n(dt, (kv.first & 2) != 0, (kv.first & 1) != 0, kv.second) : tile_n;
-      dag_bbx(bbx_tc_plan_create(dt == ELEM_E4M3 ? BBX_E4M3 : BBX_BF16, kv.second.data(),
-                                 (int)kv.second.size(), tn, &p));
-      d->waves[w].tc.push_back(p);
+      dag_bbx(bbx_tc_plan_create(dt == ELEM_E4M3 ? BBX_E4M3 : BBX_BF16, kv.second.data(), (int)kv.second.size(), tn,
+                                 &g.tc_plan));
+      g.reads = tc_rw[kv.first].first;
+      g.writes = tc_rw[kv.first].second;
+      d->groups.push_back(std::move(g));
       d->stats.tc_launches++;
     }
-    d->stats.opaque_launches += (int)d->waves[w].opaque.size();
+    if (!post.empty()) {
+      dag_bbx(bbx::gather_plan_create(post.data(), (int)post.size(), &gpost.gather_plan));
+      d->groups.push_back(std::move(gpost));
+      d->stats.stream_launches++;
+    }
   }
   d->stats.waves = nw;
   d->stats.nodes = N;
   d->stats.arena_bytes = arena;
 
-  // ---- capture the whole launch sequence in one CUDA graph
-  cudaStream_t cs;
-  dag_cuda(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "cudaStreamCreate(capture)");
-  dag_cuda(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+  // ---- dependencies between groups: producers of every read, and every group
+  // two or more waves back (the wave barrier the arena reuse rule relies on)
+  {
+    std::unordered_map<tid_t, int> writer;
+    for (int gi = 0; gi < (int)d->groups.size(); ++gi) {
+      group_t& g = d->groups[gi];
+      std::set<int> deps;
+      for (tid_t t : g.reads) {
+        auto it = writer.find(t);
+        if (it != writer.end()) deps.insert(it->second);
+      }
+      for (int gj = 0; gj < gi; ++gj)
+        if (d->groups[gj].wave <= g.wave - 2) deps.insert(gj);
+      g.deps.assign(deps.begin(), deps.end());
+      for (tid_t t : g.writes) writer[t] = gi;
+    }
+  }
+
+  // ---- capture: tensor groups on one stream, the rest on another, joined by events
+  cudaStream_t origin, s_mem, s_tc;
+  dag_cuda(cudaStreamCreateWithFlags(&origin, cudaStreamNonBlocking), "cudaStreamCreate");
+  dag_cuda(cudaStreamCreateWithFlags(&s_mem, cudaStreamNonBlocking), "cudaStreamCreate");
+  dag_cuda(cudaStreamCreateWithFlags(&s_tc, cudaStreamNonBlocking), "cudaStreamCreate");
+  std::vector<cudaEvent_t> ev(d->groups.size() + 1);
+  for (auto& e : ev) dag_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+  dag_cuda(cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+  bool ok = false;
   try {
-    issue(d.get(), cs);
+    cudaEvent_t fork = ev.back();
+    dag_cuda(cudaEventRecord(fork, origin), "fork");
+    dag_cuda(cudaStreamWaitEvent(s_mem, fork, 0), "fork mem");
+    dag_cuda(cudaStreamWaitEvent(s_tc, fork, 0), "fork tc");
+    std::vector<bool> on_tc(d->groups.size());
+    for (size_t gi = 0; gi < d->groups.size(); ++gi) {
+      group_t& g = d->groups[gi];
+      on_tc[gi] = g.kind == G_TC;
+      cudaStream_t st = on_tc[gi] ? s_tc : s_mem;
+      for (int dep : g.deps)
+        if (on_tc[dep] != on_tc[gi]) dag_cuda(cudaStreamWaitEvent(st, ev[dep], 0), "dependency");
+      launch_group(d.get(), g, st);
+      dag_cuda(cudaEventRecord(ev[gi], st), "group event");
+    }
+    // join both streams back into the origin stream
+    cudaEvent_t jm, jt;
+    dag_cuda(cudaEventCreateWithFlags(&jm, cudaEventDisableTiming), "join event");
+    dag_cuda(cudaEventCreateWithFlags(&jt, cudaEventDisableTiming), "join event");
+    dag_cuda(cudaEventRecord(jm, s_mem), "join mem");
+    dag_cuda(cudaEventRecord(jt, s_tc), "join tc");
+    dag_cuda(cudaStreamWaitEvent(origin, jm, 0), "join");
+    dag_cuda(cudaStreamWaitEvent(origin, jt, 0), "join");
+    ok = true;
+    dag_cuda(cudaStreamEndCapture(origin, &d->graph), "cudaStreamEndCapture");
+    cudaEventDestroy(jm);
+    cudaEventDestroy(jt);
   } catch (...) {
-    cudaGraph_t g;
-    cudaStreamEndCapture(cs, &g);
-    if (g) cudaGraphDestroy(g);
-    cudaStreamDestroy(cs);
+    if (!ok) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(origin, &g);
+      if (g) cudaGraphDestroy(g);
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    cudaStreamDestroy(origin);
+    cudaStreamDestroy(s_mem);
+    cudaStreamDestroy(s_tc);
     dag_destroy(d.release());
     throw;
   }
-  dag_cuda(cudaStreamEndCapture(cs, &d->graph), "cudaStreamEndCapture");
+  for (auto& e : ev) cudaEventDestroy(e);
+  cudaStreamDestroy(origin);
+  cudaStreamDestroy(s_mem);
+  cudaStreamDestroy(s_tc);
   dag_cuda(cudaGraphInstantiate(&d->exec, d->graph, 0), "cudaGraphInstantiate");
-  cudaStreamDestroy(cs);
   return d.release();
 }
 
-void dag_launch(dag_t* d, cudaStream_t st) {
-  dag_cuda(cudaGraphLaunch(d->exec, st), "cudaGraphLaunch");
-}
+void dag_launch(dag_t* d, cudaStream_t st) { dag_cuda(cudaGraphLaunch(d->exec, st), "cudaGraphLaunch"); }
 
 void dag_destroy(dag_t* d) {
   if (!d) return;
   cudaDeviceSynchronize();
   if (d->exec) cudaGraphExecDestroy(d->exec);
   if (d->graph) cudaGraphDestroy(d->graph);
-  for (auto& w : d->waves) {
-    for (auto* p : w.phases) bbx_stream_plan_destroy(p);
-    for (auto* p : w.tc) bbx_tc_plan_destroy(p);
+  for (auto& g : d->groups) {
+    if (g.stream_plan) bbx_stream_plan_destroy(g.stream_plan);
+    if (g.tc_plan) bbx_tc_plan_destroy(g.tc_plan);
+    if (g.gather_plan) bbx::gather_plan_destroy(g.gather_plan);
   }
   if (d->arena) cudaFree(d->arena);
   for (void* p : d->persistent) cudaFree(p);

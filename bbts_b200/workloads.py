@@ -135,7 +135,8 @@ def cpmm(rt, rows=8, cols=8, bs=4096, dtype="bf16", seed=0, host=False):
     return {"A": A, "B": B, "C": C, "hostA": hA, "hostB": hB, "flops": e.flops}
 
 
-def ffnn(rt, batch=16384, d_in=8192, h1=8192, h2=4096, classes=1024, bs=2048, seed=0, host=False):
+def ffnn(rt, batch=16384, d_in=8192, h1=8192, h2=4096, classes=1024, bs=2048, seed=0, host=False,
+         dtype="bf16"):
     """One forward + backward step of a blocked 3-layer network:
     A1 = relu(X W1), A2 = relu(A1 W2), Z3 = A2 W3, loss = softmax-CE(Z3, labels);
     backward dW3 = A2^T G3, dA2 = G3 W3^T, dZ2 = dA2 * relu'(A2), dW2 = A1^T dZ2,
@@ -147,13 +148,14 @@ def ffnn(rt, batch=16384, d_in=8192, h1=8192, h2=4096, classes=1024, bs=2048, se
     per-row-block losses and the algorithmic FLOPs (2 * sum m n k)."""
     e = Emitter(rt)
     rng = _rng(seed)
-    B16, F32 = "dense_bf16", "dense"
+    # dtype="f32" runs the same network on FP32 blocks (the plain path)
+    B16, F32 = ("dense_bf16" if dtype == "bf16" else "dense"), "dense"
     R, KI, K1, K2 = batch // bs, d_in // bs, h1 // bs, h2 // bs
     mm_b = rt.impl("matrix_mult", [B16, B16], [B16])
     mm_f = rt.impl("matrix_mult", [B16, B16], [F32])
     add_b = rt.impl("matrix_add", [B16, B16], [B16])
     add_f = rt.impl("matrix_add", [F32, F32], [F32])
-    relu = rt.impl("matrix_relu", [B16], [B16])
+    relu = rt.impl("matrix_relu", [F32], [B16])  # f32 pre-activation -> bf16 activation
     drelu = rt.impl("matrix_relu_dif", [B16], [B16])
     had = rt.impl("matrix_matrix_hadamard", [B16, B16], [B16])
     sce = rt.impl("matrix_softmax_ce", [F32, "labels"], [B16, F32])
@@ -170,7 +172,8 @@ def ffnn(rt, batch=16384, d_in=8192, h1=8192, h2=4096, classes=1024, bs=2048, se
             from ._lib import lib, check
             rt.put(t, dense_meta(rt.fmt(B16), rows, cols))
             ptr, _ = rt.payload(t)
-            check(lib.bbx_fill_philox(1, ptr, rows * cols, int(rng.integers(1 << 62)), 1, 0.0, float(std), rt.stream))
+            check(lib.bbx_fill_philox(1 if B16 == "dense_bf16" else 0, ptr, rows * cols, int(rng.integers(1 << 62)),
+                                      1, 0.0, float(std), rt.stream))
         return t
 
     X = {(i, k): inp(bs, bs, 1.0) for i in range(R) for k in range(KI)}
@@ -211,11 +214,12 @@ def ffnn(rt, batch=16384, d_in=8192, h1=8192, h2=4096, classes=1024, bs=2048, se
         rt.apply(impl, tids, [t], params=list(params))
         return t
 
-    # forward
-    Z1 = blocked_mm(lambda i, k: X[(i, k)], lambda k, j: W1[(k, j)], R, K1, KI, mm_b, add_b)
+    # forward: pre-activations accumulate in f32 (so the ReLU masks come from
+    # f32 values), activations are stored bf16 for the next tensor-core matmul
+    Z1 = blocked_mm(lambda i, k: X[(i, k)], lambda k, j: W1[(k, j)], R, K1, KI, mm_f, add_f)
     A1 = {key: ew(relu, [t]) for key, t in Z1.items()}
     dead.extend(Z1.values())
-    Z2 = blocked_mm(lambda i, k: A1[(i, k)], lambda k, j: W2[(k, j)], R, K2, K1, mm_b, add_b)
+    Z2 = blocked_mm(lambda i, k: A1[(i, k)], lambda k, j: W2[(k, j)], R, K2, K1, mm_f, add_f)
     A2 = {key: ew(relu, [t]) for key, t in Z2.items()}
     dead.extend(Z2.values())
     Z3 = blocked_mm(lambda i, k: A2[(i, k)], lambda k, j: W3[k], R, 1, K2, mm_f, add_f, n=classes)

@@ -46,7 +46,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--grid", type=int, default=8,
                    help="blocks per side of A/B (8 = the full workload; smaller only for profiling captures)")
-    p.add_argument("--workload", default="cpmm", choices=["cpmm", "bmm", "dag", "learned"],
+    p.add_argument("--workload", default="cpmm", choices=["cpmm", "bmm", "ffnn", "dag", "learned"],
                    help="cpmm: the headline line (cross-product blocked matmul); bmm / dag / learned: the "
                         "blocked matmul, random 2000-op DAG and learned-scheduling configurations")
     p.add_argument("--n-ops", type=int, default=0, help="DAG size override (dag: 2000, learned: 5000)")
@@ -200,6 +200,8 @@ def run_dag_workload(args):
         rt = runtime.Runtime()
         if args.workload == "bmm":
             info = workloads.bmm(rt, n=4096, split=4, dtype=dtype, seed=seed, host=False)
+        elif args.workload == "ffnn":
+            info = workloads.ffnn(rt, seed=seed, dtype=dtype)
         else:
             n_ops = args.n_ops or (2000 if args.workload == "dag" else 5000)
             hi = 2048 if args.workload == "dag" else 4096
@@ -209,7 +211,7 @@ def run_dag_workload(args):
 
     with ClockSampler(0) as clk:
         result = {}
-        if args.workload in ("bmm", "dag"):
+        if args.workload in ("bmm", "dag", "ffnn"):
             # fast path: bf16 blocks, grouped + graph, autotuned tiles, heuristic and learned-free policy
             rt, info = build("bf16", 7)
             dag = rt.build_dag(runtime.HEURISTIC, tile_n=-1)
@@ -229,6 +231,8 @@ def run_dag_workload(args):
             rt.close()
             value = flops / ms / 1e9
             name = {"bmm": "blocked matmul 4096^2 in 1024^2 blocks (64 matrix_mult + 16 4-input reduces)",
+                    "ffnn": "3-layer FFN step (fwd + bwd), X 16384x8192, W1 8192^2, W2 8192x4096, W3 4096x1024, "
+                            "2048^2 blocks, relu / relu / softmax-CE",
                     "dag": "random DAG, %d ops, depth 8 (60%% matmul 128..2048, 15%% add, 15%% reduce 2-16, "
                            "10%% contraction ijk,kl->ijl 32..256)" % (args.n_ops or 2000)}[args.workload]
             line.update({"metric": "block-op DAG TFLOP/s and makespan vs plain FP32 path", "value": round(value, 2),

@@ -379,3 +379,64 @@ def test_contraction_random_vs_f64(T, spec, precision):
     else:
         ref = oracle.contraction_f64(lhs, dl, ml, rhs, dr, mr, mo, 0.5)
         assert rel_err(host(out), ref) <= 1e-2
+
+
+# ----------------------------------------------------------------- 2-SM (cta_group::2) tile
+@pytest.mark.parametrize("key", ["128x256x64", "200x136x96", "256x512x256", "130x70x40"])
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+def test_matmul_tc_2sm_integer_exact(T, key, ta, tb):
+    torch, ops = T
+    g = golden("matmul_int.npz")
+    a, b, cref = g[key + "_a"], g[key + "_b"], g[key + "_c"]
+    A = np.ascontiguousarray(a.T) if ta else a
+    B = np.ascontiguousarray(b.T) if tb else b
+
+    def padded(x):
+        rows, cols = x.shape
+        p = (cols + 7) // 8 * 8
+        buf = torch.zeros(rows, p, dtype=torch.bfloat16, device="cuda")
+        buf[:, :cols] = dev(torch, x, torch.bfloat16)
+        return buf[:, :cols]
+    c = torch.full(cref.shape, -7.0, device="cuda")
+    ops.matmul_tc([ops.tc_problem(padded(A), padded(B), c, bool(ta), bool(tb))], tile_n=512)
+    assert np.array_equal(host(c), cref)
+
+
+@pytest.mark.parametrize("m,n,k", [(1024, 1024, 1024), (512, 768, 4096), (384, 640, 136)])
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+def test_matmul_tc_2sm_random_vs_1sm(T, m, n, k, ta, tb):
+    torch, ops = T
+    rng = np.random.default_rng(m + 3 * n + k)
+    a = rng.standard_normal((k, m) if ta else (m, k)).astype(np.float32)
+    b = rng.standard_normal((n, k) if tb else (k, n)).astype(np.float32)
+    A, B = dev(torch, a, torch.bfloat16), dev(torch, b, torch.bfloat16)
+    c2 = torch.empty(m, n, device="cuda")
+    c1 = torch.empty(m, n, device="cuda")
+    ops.matmul_tc([ops.tc_problem(A, B, c2, bool(ta), bool(tb))], tile_n=512)
+    ops.matmul_tc([ops.tc_problem(A, B, c1, bool(ta), bool(tb))], tile_n=256)
+    assert rel_err(host(c2), oracle.matmul_f64(bf16_round(a), bf16_round(b), bool(ta), bool(tb))) <= 1e-5
+    assert rel_err(host(c2), host(c1)) <= 1e-6
+
+
+def test_matmul_tc_2sm_grouped_epilogues(T):
+    torch, ops = T
+    rng = np.random.default_rng(78)
+    probs, refs, outs, keep = [], [], [], []
+    for i, (m, n, k) in enumerate([(256, 256, 128), (128, 384, 64), (300, 200, 72), (512, 128, 256),
+                                   (64, 64, 64), (200, 520, 320), (1024, 1024, 512)]):
+        a = bf16_round(rng.standard_normal((m, k)))
+        b = bf16_round(rng.standard_normal((k, n)))
+        c0 = rng.standard_normal((m, n)).astype(np.float32)
+        bias = rng.standard_normal(n).astype(np.float32)
+        A, B, Cd, Bi = dev(torch, a, torch.bfloat16), dev(torch, b, torch.bfloat16), dev(torch, c0), dev(torch, bias)
+        keep += [A, B, Bi]
+        relu = i % 2 == 1
+        probs.append(ops.tc_problem(A, B, Cd, alpha=0.5, beta=1.5, bias=Bi, relu=relu))
+        ref = 0.5 * oracle.matmul_f64(a, b) + 1.5 * c0 + bias
+        refs.append(np.maximum(ref, 0) if relu else ref)
+        outs.append(Cd)
+    plan = ops.TcPlan(probs, tile_n=512)  # 7 problems: device table
+    plan.launch()
+    for o, r in zip(outs, refs):
+        assert rel_err(host(o), r) <= 1e-5
+    plan.close()

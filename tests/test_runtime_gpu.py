@@ -354,8 +354,10 @@ def _ffnn_reference(info, emulate_bf16):
     W2 = np.block([[q(hv[info["W2"][(k, j)]]) for j in range(h2 // bs)] for k in range(h1 // bs)])
     W3 = np.vstack([q(hv[info["W3"][k]]) for k in range(h2 // bs)])
     y = np.concatenate([hv[("y", i)] for i in range(batch // bs)])
-    A1 = rb(np.maximum(rb(X @ W1), 0))
-    A2 = rb(np.maximum(rb(A1 @ W2), 0))
+    # bf16 storage is emulated exactly where the DAG stores bf16: activations,
+    # the softmax gradient, each block product of dA1 and the reduced dA1
+    A1 = rb(np.maximum(X @ W1, 0))
+    A2 = rb(np.maximum(A1 @ W2, 0))
     Z3 = A2 @ W3
     P = np.exp(Z3 - Z3.max(1, keepdims=True))
     P /= P.sum(1, keepdims=True)
@@ -364,9 +366,10 @@ def _ffnn_reference(info, emulate_bf16):
     G3[np.arange(batch), y] -= 1.0
     G3 = rb(G3 / batch)
     dW3 = A2.T @ G3
-    dZ2 = rb(rb(G3 @ W3.T) * (A2 > 0))
+    dZ2 = rb(G3 @ W3.T) * (A2 > 0)
     dW2 = A1.T @ dZ2
-    dZ1 = rb(rb(dZ2 @ W2.T) * (A1 > 0))
+    dA1 = sum(rb(dZ2[:, j * bs:(j + 1) * bs] @ W2[:, j * bs:(j + 1) * bs].T) for j in range(h2 // bs))
+    dZ1 = rb(dA1) * (A1 > 0)
     dW1 = X.T @ dZ1
     return loss, dW1, dW2, dW3
 
@@ -397,3 +400,29 @@ def test_ffnn_step_vs_f64(R, path):
         assert rel_err(dW3, w3) <= tol
         assert rel_err(dW2, w2) <= tol
         assert rel_err(dW1, w1) <= tol
+
+
+@pytest.mark.parametrize("policy", [0, 1])
+def test_random_bf16_dag_with_contractions_matches_per_op(R, policy):
+    """Grouped contraction gathers + tcgen05 groups + two-stream overlap in the
+    graph reproduce the per-op path byte for byte (same kernels, same order of
+    accumulation per output element)."""
+    runtime, workloads = R
+    mk = lambda rt: workloads.random_dag(rt, n_ops=80, depth=5, seed=21, dtype="bf16", lo=128, hi=384, step=64,
+                                         contraction_dims=(16, 72), mix=(0.45, 0.15, 0.15, 0.25), max_inputs=20)
+    rt1 = runtime.Runtime()
+    info = mk(rt1)
+    rt1.run()
+    rt2 = runtime.Runtime()
+    info2 = mk(rt2)
+    if policy == 1:
+        rt2.set_predictor(runtime.Mlp(seed=5))
+    dag = rt2.build_dag(policy)
+    st = dag.stats()
+    assert st["tc_launches"] >= 1 and st["other_launches"] == 0  # contractions are grouped, not called one by one
+    for rep in range(2):
+        dag.launch()
+        for t in info["finals"]:
+            a = rt1.get_bytes(t)
+            b = dag.read_bytes(t, a.nbytes)
+            assert np.array_equal(a, b), t
