@@ -54,6 +54,11 @@ SIGNATURES = {
     "bbx_permute": (i32, [pf, i32, C.POINTER(i64), C.POINTER(i32), i32, pf, vp]),
     "bbx_contraction": (i32, [pf, i32, C.POINTER(i64), C.POINTER(i32), pf, i32, C.POINTER(i64),
                               C.POINTER(i32), pf, i32, C.POINTER(i32), f32, i32, vp]),
+    "bbx_cu_reduction": (i32, [pf, i32, C.POINTER(i64), i32, f32, C.POINTER(i32), i32, pf, vp]),
+    "bbx_cu_ew": (i32, [pf, i32, C.POINTER(i64), i32, f32, f32, C.POINTER(i32), pf, vp]),
+    "bbx_cu_ewb": (i32, [pf, i32, C.POINTER(i64), C.POINTER(i32), pf, i32, C.POINTER(i64), C.POINTER(i32), i32,
+                         f32, f32, pf, C.POINTER(i32), C.POINTER(i64), vp]),
+    "bbx_cu_expand": (i32, [pf, C.POINTER(i32), i32, pf, vp]),
     "bbx_stream_group": (i32, [vp, i32, vp]),
     "bbx_stream_plan_create": (i32, [vp, i32, C.POINTER(vp)]),
     "bbx_stream_plan_launch": (i32, [vp, vp]),

@@ -507,6 +507,166 @@ void register_b200_udfs(udf_manager_t& udm) {
         }));
   }
 
+  // ---- reduction / ew / ewb / ewb_castable / expand of the cutensor plugin
+  // (libraries/cutensor.cc:20-28 registers them under these names)
+  auto cu_shape = [](const tensor_meta_t& m) -> const cu_shape_t& { return m.as<cu_meta_t>().m(); };
+  auto cu_elems = [](const cu_shape_t& s) { size_t n = 1; for (uint32_t r = 0; r < s.rank; ++r) n *= (size_t)s.dims[r]; return n; };
+  auto ints_from = [](const params_t& p, size_t first) {
+    std::vector<int> v;
+    for (size_t i = first; i < p.num_parameters(); ++i) v.push_back(p.get_raw(i).i);
+    return v;
+  };
+  const V CU{"cutensor"}, CU2{"cutensor", "cutensor"};
+  register_ud(udm, "reduction", false, false, 1, 1);
+  add_impl(udm, std::make_unique<b200_impl_t>(
+      "b200_reduction", "reduction", CU, CU, std::vector<int32_t>{},
+      [cu_shape, ints_from](const params_t& p, const targs_t& in, targs_t& out) {
+        const auto& si = cu_shape(in.get<0>()._meta);
+        auto ord = ints_from(p, 2);
+        auto& so = out.get<0>().as<cu_t>().meta().m();
+        so.rank = (uint32_t)ord.size();
+        for (size_t r = 0; r < ord.size(); ++r) so.dims[r] = si.dims[ord[r]];
+        std::vector<long long> d(si.dims, si.dims + si.rank);
+        ok(bbx_cu_reduction((const float*)in.get<0>()._meta.payload(), (int)si.rank, d.data(), p.get_raw(0).i,
+                            p.get_raw(1).f, ord.data(), (int)ord.size(), (float*)out.get<0>()._meta.payload(), p.stream));
+      },
+      [cu_shape, cu_elems](const params_t&, const margs_t& in) -> size_t { return cu_elems(cu_shape(in.get<0>())); },
+      [cu_shape, ints_from](const params_t& p, const margs_t& in, margs_t& out) {
+        const auto& si = cu_shape(in.get<0>());
+        auto ord = ints_from(p, 2);
+        auto& so = out.get<0>().as<cu_meta_t>().m();
+        so.rank = (uint32_t)ord.size();
+        for (size_t r = 0; r < ord.size(); ++r) so.dims[r] = si.dims[ord[r]];
+      }));
+  // ew params: uop, [scalar if uop == 6], alpha, ordering...
+  auto ew_parse = [](const params_t& p, int& uop, float& scalar, float& alpha, std::vector<int>& ord) {
+    size_t i = 0;
+    uop = p.get_raw(i++).i;
+    if (uop < 0 || uop > 6) throw std::invalid_argument("is not a valid unary op");
+    scalar = uop == 6 ? p.get_raw(i++).f : 0.f;
+    alpha = p.get_raw(i++).f;
+    ord.clear();
+    for (; i < p.num_parameters(); ++i) ord.push_back(p.get_raw(i).i);
+  };
+  register_ud(udm, "ew", false, false, 1, 1);
+  add_impl(udm, std::make_unique<b200_impl_t>(
+      "b200_ew", "ew", CU, CU, std::vector<int32_t>{},
+      [cu_shape, ew_parse](const params_t& p, const targs_t& in, targs_t& out) {
+        const auto& si = cu_shape(in.get<0>()._meta);
+        int uop; float sc, al; std::vector<int> ord;
+        ew_parse(p, uop, sc, al, ord);
+        if (ord.size() != si.rank) throw std::invalid_argument("input rank is incorrect");
+        auto& so = out.get<0>().as<cu_t>().meta().m();
+        so.rank = si.rank;
+        for (size_t r = 0; r < ord.size(); ++r) so.dims[r] = si.dims[ord[r]];
+        std::vector<long long> d(si.dims, si.dims + si.rank);
+        ok(bbx_cu_ew((const float*)in.get<0>()._meta.payload(), (int)si.rank, d.data(), uop, sc, al, ord.data(),
+                     (float*)out.get<0>()._meta.payload(), p.stream));
+      },
+      [cu_shape, cu_elems](const params_t&, const margs_t& in) -> size_t { return cu_elems(cu_shape(in.get<0>())); },
+      [cu_shape, ew_parse](const params_t& p, const margs_t& in, margs_t& out) {
+        const auto& si = cu_shape(in.get<0>());
+        int uop; float sc, al; std::vector<int> ord;
+        ew_parse(p, uop, sc, al, ord);
+        auto& so = out.get<0>().as<cu_meta_t>().m();
+        so.rank = (uint32_t)ord.size();
+        for (size_t r = 0; r < ord.size() && r < 4; ++r) so.dims[r] = si.dims[ord[r]];
+      }));
+  // ewb params: op, alpha, beta, rank_l, ord_l..., rank_r, ord_r...
+  auto ewb_parse = [](const params_t& p, int& op, float& al, float& be, std::vector<int>& ol, std::vector<int>& orr) {
+    op = p.get_raw(0).i;
+    al = p.get_raw(1).f;
+    be = p.get_raw(2).f;
+    int rl = p.get_raw(3).i;
+    size_t i = 4;
+    ol.clear();
+    orr.clear();
+    for (int r = 0; r < rl; ++r) ol.push_back(p.get_raw(i++).i);
+    int rr = p.get_raw(i++).i;
+    for (int r = 0; r < rr; ++r) orr.push_back(p.get_raw(i++).i);
+  };
+  auto ewb_meta = [cu_shape](const std::vector<int>& ol, const std::vector<int>& orr, const tensor_meta_t& l,
+                             const tensor_meta_t& r, cu_shape_t& so) {
+    const auto &sl = cu_shape(l), &sr = cu_shape(r);
+    int rank = 0;
+    for (int m : ol) rank = std::max(rank, m + 1);
+    for (int m : orr) rank = std::max(rank, m + 1);
+    so.rank = (uint32_t)rank;
+    for (int d = 0; d < 4; ++d) so.dims[d] = 0;
+    for (size_t q = 0; q < ol.size(); ++q) so.dims[ol[q]] = sl.dims[q];
+    for (size_t q = 0; q < orr.size(); ++q) so.dims[orr[q]] = sr.dims[q];
+  };
+  register_ud(udm, "ewb", false, false, 2, 1);
+  add_impl(udm, std::make_unique<b200_impl_t>(
+      "b200_ewb", "ewb", CU2, CU, std::vector<int32_t>{},
+      [cu_shape, ewb_parse, ewb_meta](const params_t& p, const targs_t& in, targs_t& out) {
+        int op; float al, be; std::vector<int> ol, orr;
+        ewb_parse(p, op, al, be, ol, orr);
+        const auto &sl = cu_shape(in.get<0>()._meta), &sr = cu_shape(in.get<1>()._meta);
+        ewb_meta(ol, orr, in.get<0>()._meta, in.get<1>()._meta, out.get<0>().as<cu_t>().meta().m());
+        std::vector<long long> dl(sl.dims, sl.dims + sl.rank), dr(sr.dims, sr.dims + sr.rank);
+        ok(bbx_cu_ewb((const float*)in.get<0>()._meta.payload(), (int)sl.rank, dl.data(), ol.data(),
+                      (const float*)in.get<1>()._meta.payload(), (int)sr.rank, dr.data(), orr.data(), op, al, be,
+                      (float*)out.get<0>()._meta.payload(), nullptr, nullptr, p.stream));
+      },
+      [cu_shape, cu_elems](const params_t&, const margs_t& in) -> size_t {
+        return std::max(cu_elems(cu_shape(in.get<0>())), cu_elems(cu_shape(in.get<1>())));
+      },
+      [ewb_parse, ewb_meta](const params_t& p, const margs_t& in, margs_t& out) {
+        int op; float al, be; std::vector<int> ol, orr;
+        ewb_parse(p, op, al, be, ol, orr);
+        ewb_meta(ol, orr, in.get<0>(), in.get<1>(), out.get<0>().as<cu_meta_t>().m());
+      }));
+  // ewb_castable: same-shape add / max / min / mul (param op), associative and commutative
+  register_ud(udm, "ewb_castable", true, true, 2, 1);
+  add_impl(udm, std::make_unique<b200_impl_t>(
+      "b200_ewb_castable", "ewb_castable", CU2, CU, std::vector<int32_t>{0, 1},
+      [cu_shape](const params_t& p, const targs_t& in, targs_t& out) {
+        const auto &sl = cu_shape(in.get<0>()._meta), &sr = cu_shape(in.get<1>()._meta);
+        if (sl.rank != sr.rank) throw std::runtime_error("ewb_castable: ranks differ");
+        std::vector<int> ord;
+        for (uint32_t r = 0; r < sl.rank; ++r) {
+          if (sl.dims[r] != sr.dims[r]) throw std::runtime_error("ewb_castable: shapes differ");
+          ord.push_back((int)r);
+        }
+        auto& so = out.get<0>().as<cu_t>().meta().m();
+        so = sl;
+        int op = p.get_raw(0).i;
+        if (op < 0 || op > 3) throw std::invalid_argument("is not a castable operator");
+        std::vector<long long> d(sl.dims, sl.dims + sl.rank);
+        ok(bbx_cu_ewb((const float*)in.get<0>()._meta.payload(), (int)sl.rank, d.data(), ord.data(),
+                      (const float*)in.get<1>()._meta.payload(), (int)sr.rank, d.data(), ord.data(), op, 1.f, 1.f,
+                      (float*)out.get<0>()._meta.payload(), nullptr, nullptr, p.stream));
+      },
+      [cu_shape, cu_elems](const params_t&, const margs_t& in) -> size_t { return cu_elems(cu_shape(in.get<0>())); },
+      [cu_shape](const params_t&, const margs_t& in, margs_t& out) {
+        out.get<0>().as<cu_meta_t>().m() = cu_shape(in.get<0>());
+      }));
+  // expand params: per mode (sz_in, sz_out, num, start_in, start_out)
+  register_ud(udm, "expand", false, false, 1, 1);
+  add_impl(udm, std::make_unique<b200_impl_t>(
+      "b200_expand", "expand", CU, CU, std::vector<int32_t>{},
+      [](const params_t& p, const targs_t& in, targs_t& out) {
+        const int rank = (int)(p.num_parameters() / 5);
+        std::vector<int> q(p.num_parameters());
+        for (size_t i = 0; i < q.size(); ++i) q[i] = p.get_raw(i).i;
+        auto& so = out.get<0>().as<cu_t>().meta().m();
+        so.rank = (uint32_t)rank;
+        for (int i = 0; i < rank; ++i) so.dims[i] = q[5 * i + 1];
+        ok(bbx_cu_expand((const float*)in.get<0>()._meta.payload(), q.data(), rank,
+                         (float*)out.get<0>()._meta.payload(), p.stream));
+      },
+      [](const params_t& p, const margs_t&) -> size_t {
+        size_t t = 1;
+        for (size_t i = 0; i + 4 < p.num_parameters(); i += 5) t *= (size_t)p.get_raw(i + 1).i;
+        return t;
+      },
+      [](const params_t& p, const margs_t&, margs_t& out) {
+        auto& so = out.get<0>().as<cu_meta_t>().m();
+        so.rank = (uint32_t)(p.num_parameters() / 5);
+        for (uint32_t i = 0; i < so.rank; ++i) so.dims[i] = p.get_raw(5 * i + 1).i;
+      }));
+
   // ---- contraction of the cutensor plugin (params: rank_l, rank_r, rank_o,
   // modes_l..., modes_r..., modes_o..., alpha; contraction.h:25-55)
   register_ud(udm, "contraction", false, false, 2, 1);

@@ -145,6 +145,43 @@ def permute(x, perm, out):
     return out
 
 
+def _ints(v, ctype=C.c_int):
+    return (ctype * max(1, len(v)))(*v)
+
+
+def cu_reduction(x, dims, op, alpha, ordering, out):
+    """out (dims[ordering]...) = alpha * fold_op over the modes not in ordering
+    (op 0 add, 1 max, 2 min, 3 mul); column-major FP32."""
+    check(lib.bbx_cu_reduction(_p(x), len(dims), _ints(dims, C.c_longlong), op, alpha, _ints(ordering),
+                               len(ordering), _p(out), _stream()))
+    return out
+
+
+def cu_ew(x, dims, uop, alpha, ordering, out, scalar=0.0):
+    """out = alpha * uop(x) with output mode r = input mode ordering[r]."""
+    check(lib.bbx_cu_ew(_p(x), len(dims), _ints(dims, C.c_longlong), uop, scalar, alpha, _ints(ordering), _p(out),
+                        _stream()))
+    return out
+
+
+def cu_ewb(lhs, dims_l, ord_l, rhs, dims_r, ord_r, op, alpha, beta, out):
+    """out = op(alpha * lhs, beta * rhs), broadcast over the output modes each
+    side lacks; returns the output dims."""
+    ro = C.c_int()
+    do = (C.c_longlong * 4)()
+    check(lib.bbx_cu_ewb(_p(lhs), len(dims_l), _ints(dims_l, C.c_longlong), _ints(ord_l), _p(rhs), len(dims_r),
+                         _ints(dims_r, C.c_longlong), _ints(ord_r), op, alpha, beta, _p(out), C.byref(ro), do,
+                         _stream()))
+    return [do[i] for i in range(ro.value)]
+
+
+def cu_expand(x, params5, out):
+    """Zero `out`, then copy the box given per mode as (sz_in, sz_out, num,
+    start_in, start_out)."""
+    check(lib.bbx_cu_expand(_p(x), _ints(params5), len(params5) // 5, _p(out), _stream()))
+    return out
+
+
 def contraction(lhs, dims_l, modes_l, rhs, dims_r, modes_r, out, modes_o, alpha=1.0, precision=F32):
     """Column-major einsum (the cutensor format): tensors are flat device buffers."""
     dl = (C.c_longlong * len(dims_l))(*dims_l)

@@ -194,7 +194,10 @@ class Runtime:
         return feats[:k].copy(), lat[:k].copy()
 
     def set_predictor(self, mlp):
+        """The runtime calls into `mlp` whenever it schedules, so it holds a
+        reference: a temporary passed here stays alive as long as the runtime."""
         check(lib.bbx_rt_set_predictor(self.h, mlp.h if mlp is not None else None))
+        self._predictor = mlp
 
     def build_dag(self, policy=HEURISTIC, tile_n=0):
         return Dag(self, policy, tile_n)

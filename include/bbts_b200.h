@@ -218,6 +218,29 @@ int bbx_contraction(const float* lhs, int rank_l, const long long* dims_l, const
                     float* out, int rank_o, const int* modes_o, float alpha, int precision,
                     void* stream);
 
+/* The other block ops of the cutensor plugin, on column-major FP32 tensors of
+ * rank <= 4 (dims listed mode 0 first):
+ * reduction.h:13-21,42-111: out = alpha * fold(op: 0 add, 1 max, 2 min, 3 mul)
+ *   over the modes not in `ordering`; output mode r = input mode ordering[r]. */
+int bbx_cu_reduction(const float* in, int rank, const long long* dims, int op, float alpha, const int* ordering,
+                     int rank_out, float* out, void* stream);
+/* ew.h:13-21,131-190: out = permute(alpha * uop(in)), uop 0 e^v/(1+e^v), 1 exp,
+ *   2 square, 3 max(v,0), 4 (v<0 ? 0 : 1), 5 sqrt, 6 v + scalar; output mode r =
+ *   input mode ordering[r]. */
+int bbx_cu_ew(const float* in, int rank, const long long* dims, int uop, float scalar, float alpha,
+              const int* ordering, float* out, void* stream);
+/* ewb.h:13-46,122-204: out[i] = op(alpha * lhs[i|lhs], beta * rhs[i|rhs]) with
+ *   op 0 add, 1 max, 2 min, 3 mul, 4 sub, 5 div; lhs mode r is output mode
+ *   ord_l[r] (likewise rhs), output modes absent from an input broadcast it.
+ *   ewb_castable (ewb_castable.h:24-91) is the same-shape case with
+ *   alpha = beta = 1. The output rank / dims are returned. */
+int bbx_cu_ewb(const float* lhs, int rank_l, const long long* dims_l, const int* ord_l, const float* rhs,
+               int rank_r, const long long* dims_r, const int* ord_r, int op, float alpha, float beta, float* out,
+               int* rank_out, long long* dims_out, void* stream);
+/* expand.h:1-110: params5 = per mode (sz_in, sz_out, num, start_in, start_out);
+ *   out (sz_out...) = 0, then out[start_out + i] = in[start_in + i] for i < num. */
+int bbx_cu_expand(const float* in, const int* params5, int rank, float* out, void* stream);
+
 /* ------------------------------------------------------------------ runtime
  * A single-GPU runtime: the tensor factory + ud registry (with this library's
  * B200 impls registered through the reference's register_tensors /
