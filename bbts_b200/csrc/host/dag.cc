@@ -195,7 +195,8 @@ int autotune_tile_n(int dtype, bool ta, bool tb, const std::vector<bbx_tc_proble
   cudaEventCreate(&e1);
   int best = 256;
   float best_ms = 1e30f;
-  for (int tn : {256, 128}) {
+  for (int tn : {512, 256, 128}) {
+    if (tn == 512 && dtype == ELEM_E4M3) continue;  // the 2-SM pair tile is bf16 only
     bbx_tc_plan_t* p = nullptr;
     if (bbx_tc_plan_create(dtype == ELEM_E4M3 ? BBX_E4M3 : BBX_BF16, ps.data(), (int)ps.size(), tn, &p) != 0) continue;
     dag_bbx(bbx_tc_plan_launch(p, st));  // warm-up

@@ -70,6 +70,18 @@ class TcPlan:
     def launch(self, stream=None):
         check(lib.bbx_tc_plan_launch(self.h, stream if stream is not None else _stream()))
 
+    @property
+    def tile_n(self):
+        """128 / 256 (1-SM 128 x tile_n tiles) or 512 (2-SM 256 x 256 pair)."""
+        return lib.bbx_tc_plan_tile_n(self.h)
+
+    @property
+    def kernel_name(self):
+        tn = self.tile_n
+        if tn == 512:
+            return "tc_gemm2_kernel<K-major A,MN-major B> (2-SM 256x256 pair, cta_group::2)"
+        return "tc_gemm_kernel<%d,K-major A,MN-major B,bf16>" % tn
+
     def close(self):
         if self.h:
             lib.bbx_tc_plan_destroy(self.h)

@@ -29,10 +29,11 @@ sys.path.insert(0, ROOT)
 GRID = 8            # 8 row blocks of A, 8 column blocks of B
 BS = 4096           # block edge
 FLOP_PER_STEP = 2.0 * (GRID * BS) ** 2 * BS
-# DRAM bytes (read + write) of one full grouped launch: ncu's dram__bytes_read.sum +
-# dram__bytes_write.sum on the 2x2-block capture (4 problems, 548 MB) scaled by the
-# 64/4 problems of the full launch (the tc_gemm ncu summary kept under profiles/).
-TRAFFIC_BYTES_PER_LAUNCH = 8.77e9
+# DRAM bytes (read + write) of one full grouped launch per tile: ncu's
+# dram__bytes_read.sum + dram__bytes_write.sum on the 2x2-block capture (4 problems:
+# 548 MB with the 1-SM 128x256 tile, 627 MB with the 2-SM 256x256 pair) scaled by the
+# 64/4 problems of the full launch (the tc_gemm ncu summaries kept under profiles/).
+TRAFFIC_BYTES_PER_LAUNCH = {256: 8.77e9, 512: 10.03e9}
 
 
 def parse():
@@ -383,9 +384,10 @@ def main():
     # SUSTAINED bf16 peak; the burst fraction is reported beside it.
     peak = bf16_sust or bf16_peak
     roofline = {"bound": "tensor", "achieved": round(achieved, 1), "peak": peak,
-                "unit": "TFLOP/s", "frac": round(achieved / peak, 4), "traffic": TRAFFIC_BYTES_PER_LAUNCH,
+                "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
+                "traffic": TRAFFIC_BYTES_PER_LAUNCH.get(plan.tile_n) if GRID == 8 else None,
                 "peak_source": src + " bf16 sustained (of measured)", "frac_of_burst": round(achieved / bf16_peak, 4),
-                "kernel": "tc_gemm_kernel<256,K-major A,MN-major B,bf16>", "launches_timed": args.steps}
+                "kernel": plan.kernel_name, "launches_timed": args.steps}
 
     # ---------------- e2e through the C ABI with pinned host blocks
     hA = [torch.empty(BS, BS, dtype=torch.bfloat16, pin_memory=True) for _ in range(GRID)]

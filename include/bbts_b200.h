@@ -119,6 +119,9 @@ int bbx_tc_plan_create(int in_dtype, const bbx_tc_problem_t* problems, int count
                        bbx_tc_plan_t** out);
 int bbx_tc_plan_launch(bbx_tc_plan_t* plan, void* stream);
 int bbx_tc_plan_destroy(bbx_tc_plan_t* plan);
+/* The tile the plan runs (128, 256, or 512 = the 2-SM 256 x 256 pair); the
+ * choice made for tile_n = 0. Returns 0 for a null plan. */
+int bbx_tc_plan_tile_n(const bbx_tc_plan_t* plan);
 
 /* ------------------------------------------------------------------ streaming ops */
 /* c = a + b (dense_matrix_add.cc:67-73, dense_matrix_gpu_add.cu:47-55); c may alias a or b. */

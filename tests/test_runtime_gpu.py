@@ -394,12 +394,17 @@ def test_ffnn_step_vs_f64(R, path):
     dW1 = np.block([[get(info["dW1"][(k, j)]) for j in range(2)] for k in range(2)])
     dW2 = np.block([[get(info["dW2"][(k, j)]) for j in range(2)] for k in range(2)])
     dW3 = np.vstack([get(info["dW3"][(k, 0)]) for k in range(2)])
-    for emulate, tol in ((True, 1e-2), (False, 5e-2)):
-        l64, w1, w2, w3 = _ffnn_reference(info, emulate)
-        assert rel_err(loss, l64) <= tol
-        assert rel_err(dW3, w3) <= tol
-        assert rel_err(dW2, w2) <= tol
-        assert rel_err(dW1, w1) <= tol
+    got = (loss, dW1, dW2, dW3)
+    emul = _ffnn_reference(info, True)
+    pure = _ffnn_reference(info, False)
+    for name, g, e, p in zip(("loss", "dW1", "dW2", "dW3"), got, emul, pure):
+        # the kernels: within 1e-2 of FP64 arithmetic on the same bf16 storage points
+        assert rel_err(g, e) <= 1e-2, name
+        # against the all-FP64 network the gap is the bf16 storage itself (bf16
+        # activations move pre-activations near 0 across the ReLU, which shows
+        # up in the max norm of dW2 at ~0.15 for these seeded inputs); the
+        # kernels add at most 1e-2 on top of it
+        assert rel_err(g, p) <= rel_err(e, p) + 1e-2, name
 
 
 @pytest.mark.parametrize("policy", [0, 1])
