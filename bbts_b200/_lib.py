@@ -87,7 +87,9 @@ SIGNATURES = {
     "bbx_rt_save_bbts": (i32, [vp, C.c_char_p]),
     "bbx_rt_num_commands": (i32, [vp]),
     "bbx_rt_run": (i32, [vp, i32]),
-    "bbx_rt_record": (i32, [vp, i32, vp, vp, i32, C.POINTER(i32)]),
+    "bbx_rt_record": (i32, [vp, i32, vp, vp, vp, i32, C.POINTER(i32)]),
+    "bbx_rt_set_workers": (i32, [vp, i32]),
+    "bbx_rt_set_hint_predictor": (i32, [vp, C.c_double, C.c_double]),
     "bbx_dag_build": (i32, [vp, i32, i32, C.POINTER(vp)]),
     "bbx_dag_launch": (i32, [vp, vp]),
     "bbx_dag_destroy": (i32, [vp]),

@@ -52,8 +52,7 @@ struct DeviceState {
   bool ready = false;
   int sms = 148;
   uint32_t* status = nullptr;       // kernel status word
-  unsigned int* scratch = nullptr;  // absmax word for FP8 quantisation
-  uint32_t attr_done = 0;           // bitmask of tcgen05 kernels with smem attribute set
+  uint32_t attr_done = 0;          // bitmask of tcgen05 kernels with smem attribute set
 };
 static std::mutex g_dev_mu;
 static DeviceState g_dev[64];
@@ -110,7 +109,6 @@ int device_state(DeviceState** out) {
     BBX_CUDA(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
     BBX_CUDA(cudaMalloc(&d.status, 256));
     BBX_CUDA(cudaMemset(d.status, 0, 256));
-    d.scratch = (unsigned int*)(d.status + 16);
     // Dynamic shared-memory opt-in for every tcgen05 variant, once, here: never
     // inside a stream capture.
     int rc = init_tc_attributes();
@@ -563,15 +561,21 @@ int bbx_quantize_e4m3(int src_dtype, const void* in, void* out, int rows, int co
   cudaStream_t st = (cudaStream_t)stream;
   const long long n = (long long)rows * cols;
   const int grid = grid_for(n, 256, d->sms);
-  BBX_CUDA(cudaMemsetAsync(d->scratch, 0, 4, st));
+  // the absmax word is stream-ordered scratch of this call, so quantisations
+  // on different streams never share it
+  unsigned int* amax = nullptr;
+  BBX_CUDA(cudaMallocAsync((void**)&amax, 4, st));
+  BBX_CUDA(cudaMemsetAsync(amax, 0, 4, st));
   if (src_dtype == BBX_F32) {
-    k_absmax<float><<<grid, 256, 0, st>>>((const float*)in, n, d->scratch);
-    k_quant_e4m3<float><<<grid, 256, 0, st>>>((const float*)in, (__nv_fp8_e4m3*)out, rows, cols, d->scratch, scale_out, transpose);
+    k_absmax<float><<<grid, 256, 0, st>>>((const float*)in, n, amax);
+    k_quant_e4m3<float><<<grid, 256, 0, st>>>((const float*)in, (__nv_fp8_e4m3*)out, rows, cols, amax, scale_out, transpose);
   } else {
-    k_absmax<__nv_bfloat16><<<grid, 256, 0, st>>>((const __nv_bfloat16*)in, n, d->scratch);
-    k_quant_e4m3<__nv_bfloat16><<<grid, 256, 0, st>>>((const __nv_bfloat16*)in, (__nv_fp8_e4m3*)out, rows, cols, d->scratch, scale_out, transpose);
+    k_absmax<__nv_bfloat16><<<grid, 256, 0, st>>>((const __nv_bfloat16*)in, n, amax);
+    k_quant_e4m3<__nv_bfloat16><<<grid, 256, 0, st>>>((const __nv_bfloat16*)in, (__nv_fp8_e4m3*)out, rows, cols, amax, scale_out, transpose);
   }
-  BBX_CHECK_LAUNCH("quantize_e4m3");
+  cudaError_t le = cudaGetLastError();
+  cudaFreeAsync(amax, st);
+  if (le != cudaSuccess) return set_error(BBX_ERR_CUDA, "quantize_e4m3: %s", cudaGetErrorString(le));
   return BBX_OK;
 }
 

@@ -328,3 +328,18 @@ extern "C" int bbx_rt_set_predictor(bbx_rt_t* rt, bbx_mlp_t* mlp) {
   r->predictor = [r](const bbts::op_features_t& f) { return r->batch_predictor({f})[0]; };
   return BBX_OK;
 }
+
+// The heuristic cost, calibrated: the ud's get_complexity_hint mapped to
+// microseconds by a fit of log latency on log hint.
+extern "C" int bbx_rt_set_hint_predictor(bbx_rt_t* rt, double a, double b) {
+  if (!rt) return bbx::set_error(BBX_ERR_INVALID, "null runtime");
+  if (!std::isfinite(a) || !std::isfinite(b)) return bbx::set_error(BBX_ERR_INVALID, "non-finite hint model");
+  bbts::runtime_t* r = bbts::rt_of(rt);
+  r->batch_predictor = [a, b](const std::vector<bbts::op_features_t>& fs) {
+    std::vector<double> out(fs.size());
+    for (size_t i = 0; i < fs.size(); ++i) out[i] = std::exp(a * std::log(std::max(1.0, fs[i].hint)) + b);
+    return out;
+  };
+  r->predictor = [a, b](const bbts::op_features_t& f) { return std::exp(a * std::log(std::max(1.0, f.hint)) + b); };
+  return BBX_OK;
+}

@@ -286,7 +286,15 @@ int bbx_rt_run(bbx_rt_t* rt, int policy) {
   });
 }
 
-int bbx_rt_record(bbx_rt_t* rt, int policy, float* features, float* latency_us, int cap, int* n_out) {
+int bbx_rt_set_workers(bbx_rt_t* rt, int workers) {
+  if (!rt) return bbx::set_error(BBX_ERR_INVALID, "null runtime");
+  if (workers < 1 || workers > 16) return bbx::set_error(BBX_ERR_INVALID, "workers must be in [1, 16]");
+  rt->rt.workers = workers;
+  return BBX_OK;
+}
+
+int bbx_rt_record(bbx_rt_t* rt, int policy, float* features, float* latency_us, double* hints, int cap,
+                  int* n_out) {
   if (!rt) return bbx::set_error(BBX_ERR_INVALID, "null runtime");
   RT_TRY({
     std::vector<std::pair<op_features_t, float>> rec;
@@ -295,6 +303,7 @@ int bbx_rt_record(bbx_rt_t* rt, int policy, float* features, float* latency_us, 
     for (int i = 0; i < n; ++i) {
       if (features) memcpy(features + 12 * i, rec[i].first.f, 12 * sizeof(float));
       if (latency_us) latency_us[i] = rec[i].second;
+      if (hints) hints[i] = rec[i].first.hint;
     }
     if (n_out) *n_out = (int)rec.size();
   });

@@ -24,15 +24,31 @@ bool starts_with(const std::string& s, const char* p) { return s.rfind(p, 0) == 
 }  // namespace
 
 // ------------------------------------------------------------------ storage
-block_storage_t::~block_storage_t() {
-  for (auto& kv : _blocks)
-    if (kv.second.owned && kv.second.payload) cudaFree(kv.second.payload);
+block_storage_t::block_storage_t(tensor_factory_ptr_t tf, cudaStream_t st) : _tf(std::move(tf)), _st(st) {
+  int dev = 0;
+  cuda_ok(cudaGetDevice(&dev), "cudaGetDevice");
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cuda_ok(cudaMemPoolCreate(&_pool, &props), "cudaMemPoolCreate(blocks)");
+  unsigned long long keep = ~0ULL;  // never trim at synchronisation points
+  cuda_ok(cudaMemPoolSetAttribute(_pool, cudaMemPoolAttrReleaseThreshold, &keep), "pool release threshold");
 }
 
-tensor_t* block_storage_t::create(tid_t tid, const tensor_meta_t& meta) {
+block_storage_t::~block_storage_t() {
+  for (auto& kv : _blocks)
+    if (kv.second.owned && kv.second.payload) cudaFreeAsync(kv.second.payload, _st);
+  cudaStreamSynchronize(_st);
+  _blocks.clear();
+  if (_pool) cudaMemPoolDestroy(_pool);
+}
+
+tensor_t* block_storage_t::create(tid_t tid, const tensor_meta_t& meta, cudaStream_t st) {
+  if (!st) st = _st;
   size_t bytes = _tf->get_payload_size(meta);
   void* p = nullptr;
-  if (bytes) cuda_ok(cudaMallocAsync(&p, bytes, _st), "cudaMallocAsync(block)");
+  if (bytes) cuda_ok(cudaMallocFromPoolAsync(&p, bytes, _pool, st), "cudaMallocFromPoolAsync(block)");
   block_t b;
   b.header.reset(new char[sizeof(tensor_meta_t)]);
   std::memcpy(b.header.get(), &meta, sizeof(tensor_meta_t));
@@ -43,7 +59,7 @@ tensor_t* block_storage_t::create(tid_t tid, const tensor_meta_t& meta) {
   std::lock_guard<std::mutex> lk(_m);
   auto it = _blocks.find(tid);
   if (it != _blocks.end()) {
-    if (it->second.owned && it->second.payload) cudaFreeAsync(it->second.payload, _st);
+    if (it->second.owned && it->second.payload) cudaFreeAsync(it->second.payload, st);
     _blocks.erase(it);
   }
   auto& slot = _blocks[tid];
@@ -78,11 +94,11 @@ block_t* block_storage_t::block(tid_t tid) {
   return it == _blocks.end() ? nullptr : &it->second;
 }
 
-bool block_storage_t::remove(tid_t tid) {
+bool block_storage_t::remove(tid_t tid, cudaStream_t st) {
   std::lock_guard<std::mutex> lk(_m);
   auto it = _blocks.find(tid);
   if (it == _blocks.end()) return false;
-  if (it->second.owned && it->second.payload) cudaFreeAsync(it->second.payload, _st);  // stream-ordered
+  if (it->second.owned && it->second.payload) cudaFreeAsync(it->second.payload, st ? st : _st);  // stream-ordered
   _blocks.erase(it);
   return true;
 }
@@ -114,8 +130,10 @@ runtime_t::runtime_t() {
 }
 
 runtime_t::~runtime_t() {
+  for (cudaStream_t s : worker_streams) cudaStreamSynchronize(s);
   if (stream) cudaStreamSynchronize(stream);
   storage.reset();
+  for (cudaStream_t s : worker_streams) cudaStreamDestroy(s);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -192,17 +210,19 @@ op_features_t features_of(const tensor_factory_t& tfac, const command_t& cmd, ud
   f.f[9] = (float)tb;
   f.f[10] = (float)cmd.get_num_inputs();
   f.f[11] = (float)std::log2(std::max(1.0, m * n * (double)std::max<size_t>(1, cmd.get_num_inputs())));
-  if (hint_out) *hint_out = impl ? impl->get_complexity_hint(params, margs) : 0;
+  const size_t hint = impl ? impl->get_complexity_hint(params, margs) : 0;
+  f.hint = (double)hint;
+  if (hint_out) *hint_out = hint;
   return f;
 }
 
 // Executes one APPLY / REDUCE on the runtime stream (the per-op path).
-void execute_command(runtime_t& rt, command_t& cmd) {
+void execute_command(runtime_t& rt, command_t& cmd, cudaStream_t st) {
   ud_impl_t* impl = rt.udm->get_fn_impl(cmd.fun_id);
   if (!impl) throw std::runtime_error("command " + std::to_string(cmd.id) + ": unknown ud impl");
   ud_impl_t::tensor_params_t params;
   params._params = cmd.get_parameters();
-  params.stream = rt.stream;
+  params.stream = st;
   if (cmd.is_apply()) {
     const size_t ni = cmd.get_num_inputs(), no = cmd.get_num_outputs();
     std::vector<tensor_meta_t> in_meta(ni), out_meta(no);
@@ -219,7 +239,7 @@ void execute_command(runtime_t& rt, command_t& cmd) {
     ud_impl_t::tensor_args_t out_args(no);
     for (size_t i = 0; i < no; ++i) {
       out_meta[i].fmt_id = rt.tf->get_tensor_ftm(impl->outputTypes[i]);
-      tensor_t* t = rt.storage->create(cmd.get_output(i).tid, out_meta[i]);
+      tensor_t* t = rt.storage->create(cmd.get_output(i).tid, out_meta[i], st);
       out_args.set(i, *t);
     }
     impl->call_ud(params, in_args, out_args);
@@ -236,14 +256,14 @@ void execute_command(runtime_t& rt, command_t& cmd) {
     tid_t out_tid = cmd.get_output(0).tid;
     const tensor_meta_t& m0 = ins[0]->_meta;
     if (impl->impl_name == "b200_dense_add" || impl->impl_name == "b200_dense_bf16_add") {
-      tensor_t* out = rt.storage->create(out_tid, m0);
+      tensor_t* out = rt.storage->create(out_tid, m0, st);
       const auto& dm = m0.as<dense_tensor_meta_t>().m();
       const long long n = (long long)dm.num_rows * dm.num_cols;
       const int dt = impl->impl_name == "b200_dense_add" ? BBX_F32 : BBX_BF16;
       if (dt == BBX_F32) {
         std::vector<const float*> ptrs(ni);
         for (size_t i = 0; i < ni; ++i) ptrs[i] = (const float*)ins[i]->_meta.payload();
-        bbx_ok(bbx_reduce_f32(ptrs.data(), (int)ni, (float*)out->_meta.payload(), n, 1, rt.stream));
+        bbx_ok(bbx_reduce_f32(ptrs.data(), (int)ni, (float*)out->_meta.payload(), n, 1, st));
       } else {
         // bf16 blocks: chain grouped-stream sums of up to 16 inputs (f32 math)
         std::vector<const void*> pend;
@@ -256,7 +276,7 @@ void execute_command(runtime_t& rt, command_t& cmd) {
           while (c < BBX_STREAM_MAX_IN && !pend.empty()) { s.in[c++] = pend.front(); pend.erase(pend.begin()); }
           s.n_in = c;
           s.out = out->_meta.payload();
-          bbx_ok(bbx_stream_group(&s, 1, rt.stream));
+          bbx_ok(bbx_stream_group(&s, 1, st));
         }
       }
     } else {
@@ -270,17 +290,17 @@ void execute_command(runtime_t& rt, command_t& cmd) {
         impl->get_out_meta(params, ima, oma);
         om[0].fmt_id = rt.tf->get_tensor_ftm(impl->outputTypes[0]);
         tid_t t = (i + 1 == ni) ? out_tid : tmp_base - (tid_t)i;
-        tensor_t* o = rt.storage->create(t, om[0]);
+        tensor_t* o = rt.storage->create(t, om[0], st);
         ud_impl_t::tensor_args_t ia(std::vector<tensor_t*>{lhs, ins[i]}), oa(std::vector<tensor_t*>{o});
         impl->call_ud(params, ia, oa);
-        if (i > 1) rt.storage->remove(lhs_tid);  // drop the previous intermediate
+        if (i > 1) rt.storage->remove(lhs_tid, st);  // drop the previous intermediate
         lhs = o;
         lhs_tid = t;
       }
       if (ni == 1) {
-        tensor_t* o = rt.storage->create(out_tid, m0);
+        tensor_t* o = rt.storage->create(out_tid, m0, st);
         cuda_ok(cudaMemcpyAsync(o->_meta.payload(), m0.payload(), rt.tf->get_payload_size(m0),
-                                cudaMemcpyDeviceToDevice, rt.stream), "reduce copy");
+                                cudaMemcpyDeviceToDevice, st), "reduce copy");
       }
     }
   }
@@ -289,7 +309,7 @@ void execute_command(runtime_t& rt, command_t& cmd) {
 void runtime_t::run_per_op(int policy, std::vector<std::pair<op_features_t, float>>* record) {
   reservation_station_t rs(0, 1);
   for (tid_t t : storage->tids()) rs.register_tensor(t);
-  std::unordered_map<command_id_t, double> prio;
+  std::unordered_map<command_id_t, double> prio, lat_of;
   if (policy == SCHED_LEARNED && predictor) {
     // critical-path priority: predicted latency + the longest predicted path to a sink
     std::unordered_map<tid_t, std::vector<size_t>> readers;
@@ -343,6 +363,7 @@ void runtime_t::run_per_op(int policy, std::vector<std::pair<op_features_t, floa
         for (size_t r : readers[c.get_output(o).tid]) best = std::max(best, up[r]);
       up[ii] = lat[ii] + best;
       prio[c.id] = up[ii];
+      lat_of[c.id] = lat[ii];
     }
     rs.set_priority([&prio](const command_t& c) { auto it = prio.find(c.id); return it == prio.end() ? 0.0 : it->second; });
   }
@@ -350,12 +371,62 @@ void runtime_t::run_per_op(int policy, std::vector<std::pair<op_features_t, floa
     if (!rs.queue_command(c->clone())) throw std::runtime_error("reservation station rejected command " + std::to_string(c->id));
   }
   rs.execute_scheduled_async();
+
+  // ---- worker streams (one = the runtime stream itself)
+  const int K = record ? 1 : std::max(1, std::min(workers, 16));
+  while ((int)worker_streams.size() < K && K > 1) {
+    cudaStream_t s;
+    cuda_ok(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate(worker)");
+    worker_streams.push_back(s);
+  }
+  std::vector<cudaStream_t> ws;
+  if (K == 1) ws.push_back(stream);
+  else ws.assign(worker_streams.begin(), worker_streams.begin() + K);
+  std::vector<cudaEvent_t> events;
+  auto new_event = [&]() {
+    cudaEvent_t e;
+    cuda_ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+    events.push_back(e);
+    return e;
+  };
+  std::unordered_map<tid_t, cudaEvent_t> ready;                              // producer's completion
+  std::unordered_map<tid_t, std::vector<std::pair<cudaEvent_t, int>>> reads;  // readers' completions + stream
+  if (K > 1) {
+    cudaEvent_t start = new_event();  // everything queued on the runtime stream so far comes first
+    cuda_ok(cudaEventRecord(start, stream), "record start");
+    for (cudaStream_t s : ws) cuda_ok(cudaStreamWaitEvent(s, start, 0), "wait start");
+  }
+  // a deleted block is freed on the stream of its last reader, after the other
+  // readers' completions, so its memory returns to the pool only when unused
+  auto free_block = [&](tid_t t) {
+    if (K == 1) {
+      storage->remove(t);
+      return;
+    }
+    cudaStream_t s = stream;
+    auto it = reads.find(t);
+    if (it != reads.end() && !it->second.empty()) {
+      const int si = it->second.back().second;
+      s = ws[si];
+      for (auto& er : it->second)
+        if (er.second != si) cuda_ok(cudaStreamWaitEvent(s, er.first, 0), "wait reader");
+    } else {
+      auto r = ready.find(t);
+      if (r != ready.end()) cuda_ok(cudaStreamWaitEvent(s, r->second, 0), "wait producer");
+    }
+    storage->remove(t, s);
+    reads.erase(t);
+    ready.erase(t);
+  };
+  std::vector<double> avail(K, 0.0);             // predicted time each stream frees up
+  std::unordered_map<tid_t, double> t_ready;     // predicted time each block is written
+  int rr = 0;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evs;
   std::vector<op_features_t> feats;
   while (true) {
     tid_t dead;
     while (rs.try_get_to_remove(&dead)) {
-      storage->remove(dead);
+      free_block(dead);
       rs.retire_remove(dead);
     }
     command_ptr_t cmd = rs.try_get_next_command();
@@ -363,26 +434,64 @@ void runtime_t::run_per_op(int policy, std::vector<std::pair<op_features_t, floa
       if (rs.num_to_retire() == 0) break;
       throw std::runtime_error("DAG stalled: commands wait for tensors nothing produces");
     }
+    int si = 0;
+    if (K > 1) {
+      auto lit = lat_of.find(cmd->id);
+      if (policy == SCHED_LEARNED && lit != lat_of.end()) {
+        // list scheduling: the stream on which the command is predicted to finish first
+        double rdy = 0;
+        for (size_t j = 0; j < cmd->get_num_inputs(); ++j) {
+          auto r = t_ready.find(cmd->get_input(j).tid);
+          if (r != t_ready.end()) rdy = std::max(rdy, r->second);
+        }
+        for (int k = 1; k < K; ++k)
+          if (std::max(avail[k], rdy) < std::max(avail[si], rdy)) si = k;
+        avail[si] = std::max(avail[si], rdy) + lit->second;
+        for (size_t o = 0; o < cmd->get_num_outputs(); ++o) t_ready[cmd->get_output(o).tid] = avail[si];
+      } else {
+        si = rr++ % K;  // the reference's workers take commands as they come
+      }
+      for (size_t j = 0; j < cmd->get_num_inputs(); ++j) {
+        auto r = ready.find(cmd->get_input(j).tid);
+        if (r != ready.end()) cuda_ok(cudaStreamWaitEvent(ws[si], r->second, 0), "wait input");
+      }
+    }
+    cudaStream_t s = ws[si];
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (record) {
       size_t hint;
       feats.push_back(features(*cmd, &hint));
       cudaEventCreate(&e0);
       cudaEventCreate(&e1);
-      cudaEventRecord(e0, stream);
+      cudaEventRecord(e0, s);
     }
-    execute_command(*this, *cmd);
+    execute_command(*this, *cmd, s);
     if (record) {
-      cudaEventRecord(e1, stream);
+      cudaEventRecord(e1, s);
       evs.push_back({e0, e1});
+    }
+    if (K > 1) {
+      cudaEvent_t done = new_event();
+      cuda_ok(cudaEventRecord(done, s), "record done");
+      for (size_t o = 0; o < cmd->get_num_outputs(); ++o) ready[cmd->get_output(o).tid] = done;
+      for (size_t j = 0; j < cmd->get_num_inputs(); ++j) reads[cmd->get_input(j).tid].push_back({done, si});
     }
     rs.retire_command(std::move(cmd));
   }
   tid_t dead;
   while (rs.try_get_to_remove(&dead)) {
-    storage->remove(dead);
+    free_block(dead);
     rs.retire_remove(dead);
   }
+  if (K > 1) {
+    // join: the runtime stream continues after every worker's last command
+    for (cudaStream_t s : ws) {
+      cudaEvent_t e = new_event();
+      cuda_ok(cudaEventRecord(e, s), "record join");
+      cuda_ok(cudaStreamWaitEvent(stream, e, 0), "wait join");
+    }
+  }
+  for (cudaEvent_t e : events) cudaEventDestroy(e);  // released once the device has passed them
   if (record) {
     cuda_ok(cudaStreamSynchronize(stream), "run_per_op sync");
     for (size_t i = 0; i < evs.size(); ++i) {

@@ -29,15 +29,19 @@ struct block_t {
 };
 
 // tid -> block. Payload allocations are stream-ordered on the runtime stream.
+// Payloads come from a memory pool the storage owns, stream-ordered on the
+// stream each call names (the runtime stream by default). The pool keeps freed
+// memory for reuse instead of returning it to the driver at every
+// synchronisation, so a block freed and re-created costs no new mapping.
 class block_storage_t {
  public:
-  block_storage_t(tensor_factory_ptr_t tf, cudaStream_t st) : _tf(std::move(tf)), _st(st) {}
+  block_storage_t(tensor_factory_ptr_t tf, cudaStream_t st);
   ~block_storage_t();
-  tensor_t* create(tid_t tid, const tensor_meta_t& meta);                  // allocates the payload
+  tensor_t* create(tid_t tid, const tensor_meta_t& meta, cudaStream_t st = nullptr);  // allocates the payload
   tensor_t* create_view(tid_t tid, const tensor_meta_t& meta, void* payload, size_t bytes);
   tensor_t* get(tid_t tid);
   block_t* block(tid_t tid);
-  bool remove(tid_t tid);
+  bool remove(tid_t tid, cudaStream_t st = nullptr);
   bool assign_tid(tid_t from, tid_t to);
   size_t size() const { return _blocks.size(); }
   std::vector<tid_t> tids() const;
@@ -45,13 +49,16 @@ class block_storage_t {
  private:
   tensor_factory_ptr_t _tf;
   cudaStream_t _st;
+  cudaMemPool_t _pool = nullptr;
   std::mutex _m;
   std::unordered_map<tid_t, block_t> _blocks;
 };
 
-// Op features for the learned cost model (12 values, see cost_model.h).
+// Op features for the learned cost model: the 12 MLP inputs, plus the ud's
+// own get_complexity_hint (the heuristic cost), which is not an MLP input.
 struct op_features_t {
   float f[12];
+  double hint = 0.0;
 };
 
 // A compiled DAG: every launch of a whole command list, captured in a CUDA graph.
@@ -77,9 +84,19 @@ class runtime_t {
   std::function<double(const op_features_t&)> predictor;
   std::function<std::vector<double>(const std::vector<op_features_t>&)> batch_predictor;
 
-  // Per-op execution of `commands` through the reservation station, one
-  // worker, stream-ordered launches (the plain path). With record != null the
-  // launches of each command are bracketed by CUDA events and their
+  // Worker streams of the per-op path: the reference pulls ready commands from
+  // the reservation station with num_threads workers (src/server/node.cc:67-69);
+  // here each worker is a CUDA stream and a command waits only on the events
+  // of the commands that produced its inputs. 1 = the plain path (one stream,
+  // one launch after another).
+  int workers = 1;
+  std::vector<cudaStream_t> worker_streams;
+
+  // Per-op execution of `commands` through the reservation station with
+  // `workers` streams. Heuristic: LIFO pop, round-robin streams. Learned:
+  // critical-path pop by predicted latency, each command on the stream with
+  // the earliest predicted finish. With record != null (always one stream)
+  // the launches of each command are bracketed by CUDA events and their
   // (features, latency) pairs appended.
   void run_per_op(int policy, std::vector<std::pair<op_features_t, float>>* record);
 
@@ -92,7 +109,7 @@ node_kind_t classify(const ud_impl_t* impl, bool is_reduce);
 op_features_t features_of(const tensor_factory_t& tf, const command_t& cmd, ud_impl_t* impl,
                           std::vector<tensor_meta_t> in_metas, size_t* hint_out);
 int elem_of(const tensor_factory_t& tf, tfid_t id);
-void execute_command(runtime_t& rt, command_t& cmd);
+void execute_command(runtime_t& rt, command_t& cmd, cudaStream_t st);
 
 dag_t* dag_build(runtime_t* rt, int policy, int tile_n);
 void dag_launch(dag_t* d, cudaStream_t st);

@@ -183,15 +183,30 @@ class Runtime:
     def run(self, policy=HEURISTIC):
         check(lib.bbx_rt_run(self.h, policy))
 
-    def record(self, policy=HEURISTIC, cap=1 << 20):
+    def record(self, policy=HEURISTIC, cap=1 << 20, with_hints=False):
+        """Runs the list on one stream, timing every command: (features [n, 12],
+        latency us [n]) and, with_hints, the uds' complexity hints [n]."""
         n = self.num_commands()
         cap = max(1, min(cap, n))
         feats = np.empty((cap, 12), np.float32)
         lat = np.empty(cap, np.float32)
+        hints = np.empty(cap, np.float64)
         got = C.c_int()
-        check(lib.bbx_rt_record(self.h, policy, feats.ctypes.data, lat.ctypes.data, cap, C.byref(got)))
+        check(lib.bbx_rt_record(self.h, policy, feats.ctypes.data, lat.ctypes.data, hints.ctypes.data, cap,
+                                C.byref(got)))
         k = min(cap, got.value)
+        if with_hints:
+            return feats[:k].copy(), lat[:k].copy(), hints[:k].copy()
         return feats[:k].copy(), lat[:k].copy()
+
+    def set_workers(self, n):
+        """Worker streams of the per-op path (1 = the plain single-stream path)."""
+        check(lib.bbx_rt_set_workers(self.h, int(n)))
+
+    def set_hint_predictor(self, a, b):
+        """Predicted latency exp(a ln(hint) + b) us from the uds' complexity hints."""
+        check(lib.bbx_rt_set_hint_predictor(self.h, float(a), float(b)))
+        self._predictor = None
 
     def set_predictor(self, mlp):
         """The runtime calls into `mlp` whenever it schedules, so it holds a

@@ -245,15 +245,21 @@ def run_dag_workload(args):
         else:
             # learned scheduling: train the MLP on timings the runtime records itself
             t0 = time.perf_counter()
-            feats, lats = [], []
+            feats, lats, hints = [], [], []
             for d in range(args.train_dags):
-                rt, _ = build("bf16" if d % 2 == 0 else "f32", 1000 + d, reuse=0.8)
-                f, l = rt.record()
+                # config-4-style training DAGs (2000 ops), sizes up to 4096 like the held-out DAG
+                rt = runtime.Runtime()
+                workloads.random_dag(rt, n_ops=2000, depth=8, seed=1000 + d, dtype="bf16" if d % 2 == 0 else "f32",
+                                     hi=4096, reuse=0.8)
+                torch.cuda.synchronize()
+                f, l, h = rt.record(with_hints=True)
                 feats.append(f)
                 lats.append(l)
+                hints.append(h)
                 rt.close()
             X = np.concatenate(feats)
             y = np.log(np.maximum(np.concatenate(lats), 1e-3))
+            H = np.log(np.maximum(np.concatenate(hints), 1.0))
             rec_s = time.perf_counter() - t0
             n_hold = len(y) // 10
             mlp = runtime.Mlp(seed=1)
@@ -266,44 +272,68 @@ def run_dag_workload(args):
             pred = mlp.predict(X[:n_hold])
             infer_s = time.perf_counter() - t2
             hold_mse = float(np.mean((pred - y[:n_hold]) ** 2))
-            # the complexity-hint baseline predictor: log(flops-like hint) fit by least squares
-            hint = X[:, 11] * np.log(2)
-            A = np.stack([hint[n_hold:], np.ones(len(y) - n_hold)], 1)
-            coef = np.linalg.lstsq(A, y[n_hold:], rcond=None)[0]
-            hint_mse = float(np.mean((coef[0] * hint[:n_hold] + coef[1] - y[:n_hold]) ** 2))
-            # held-out DAG: makespan learned vs heuristic on the same kernels
+            # the heuristic cost, calibrated: log latency ~ a ln(get_complexity_hint) + b by least squares
+            A = np.stack([H[n_hold:], np.ones(len(y) - n_hold)], 1)
+            ha, hb = np.linalg.lstsq(A, y[n_hold:], rcond=None)[0]
+            hint_mse = float(np.mean((ha * H[:n_hold] + hb - y[:n_hold]) ** 2))
+            # held-out DAG: makespans on the same kernels under each cost source
             rt, info = build("bf16", 4242, reuse=0.8)
-            make = {}
-            for pol, nm in ((runtime.HEURISTIC, "heuristic"), (runtime.LEARNED, "learned")):
-                if pol == runtime.LEARNED:
-                    rt.set_predictor(mlp)
+            preds = {"heuristic": None, "hint": ("hint", ha, hb), "learned": ("mlp", mlp)}
+
+            def install(p):
+                if p is None:
+                    rt.set_predictor(None)
+                elif p[0] == "hint":
+                    rt.set_hint_predictor(p[1], p[2])
+                else:
+                    rt.set_predictor(p[1])
+                return runtime.HEURISTIC if p is None else runtime.LEARNED
+
+            make, waves = {}, {}
+            for nm, p in preds.items():
+                pol = install(p)
                 dag = rt.build_dag(pol, tile_n=0)
                 for _ in range(args.warmup):
                     dag.launch()
                 make[nm] = _time_on(rt.stream.value, dag.launch, args.steps)
-                make[nm + "_waves"] = dag.stats()["waves"]
+                waves[nm] = dag.stats()["waves"]
                 dag.close()
-            # per-op reservation-station order: LIFO vs learned critical-path priority
-            rt.set_predictor(None)
+            # per-op path through the reservation station on 4 worker streams:
+            # LIFO + round-robin vs critical-path priority + earliest-finish stream
+            per_op = {}
+            rt.set_workers(4)
+            for nm, p in preds.items():
+                pol = install(p)
+                rt.run(pol)
+                per_op[nm] = float(np.median([_time_on(rt.stream.value, lambda: rt.run(pol), 1) for _ in range(3)]))
+            rt.set_workers(1)
+            install(None)
             rt.run(runtime.HEURISTIC)
-            lifo = _time_on(rt.stream.value, lambda: rt.run(runtime.HEURISTIC), 1)
-            rt.set_predictor(mlp)
-            rt.run(runtime.LEARNED)
-            cp = _time_on(rt.stream.value, lambda: rt.run(runtime.LEARNED), 1)
+            one_stream = float(np.median([_time_on(rt.stream.value, lambda: rt.run(runtime.HEURISTIC), 1)
+                                          for _ in range(3)]))
             flops = info["flops"]
             value = flops / make["learned"] / 1e9
+            r3 = lambda v: round(v, 3)
             line.update({"metric": "block-op DAG makespan, learned vs heuristic schedule", "value": round(value, 2),
-                         "unit": "TFLOP/s", "ms_per_step": round(make["learned"], 3), "dtype": "bf16",
+                         "unit": "TFLOP/s", "ms_per_step": r3(make["learned"]), "dtype": "bf16",
                          "config": {"workload": "held-out random DAG, %d ops, sizes 128..4096" % info["n_ops"],
                                     "flops_per_step": flops, "train_timings": int(len(y) - n_hold),
                                     "train_dags": args.train_dags},
-                         "makespan_ms": {"grouped_learned": round(make["learned"], 3),
-                                         "grouped_heuristic": round(make["heuristic"], 3),
-                                         "per_op_learned_priority": round(cp, 3), "per_op_lifo": round(lifo, 3)},
-                         "learned_gain": {"grouped": round(make["heuristic"] / make["learned"], 4),
-                                          "per_op": round(lifo / cp, 4)},
+                         "makespan_ms": {"grouped_heuristic": r3(make["heuristic"]),
+                                         "grouped_hint": r3(make["hint"]),
+                                         "grouped_learned": r3(make["learned"]),
+                                         "per_op_4_streams_lifo": r3(per_op["heuristic"]),
+                                         "per_op_4_streams_hint": r3(per_op["hint"]),
+                                         "per_op_4_streams_learned": r3(per_op["learned"]),
+                                         "per_op_1_stream_lifo": r3(one_stream)},
+                         "waves": waves,
+                         "learned_gain": {"grouped_vs_heuristic": round(make["heuristic"] / make["learned"], 4),
+                                          "grouped_vs_hint": round(make["hint"] / make["learned"], 4),
+                                          "per_op_vs_heuristic": round(per_op["heuristic"] / per_op["learned"], 4),
+                                          "per_op_vs_hint": round(per_op["hint"] / per_op["learned"], 4)},
                          "cost_model": {"holdout_mse_log_latency": round(hold_mse, 4),
                                         "complexity_hint_mse_log_latency": round(hint_mse, 4),
+                                        "hint_fit": [round(float(ha), 4), round(float(hb), 4)],
                                         "train_loss": round(loss, 4), "record_s": round(rec_s, 1),
                                         "train_s": round(train_s, 2), "infer_s_per_%d" % n_hold: round(infer_s, 4)},
                          "gpu_launches": None})

@@ -302,9 +302,16 @@ int bbx_rt_save_bbts(bbx_rt_t* rt, const char* path);
  * command, like command_runner_t::local_command_runner
  * (src/commands/command_runner.cc:18-259). Synchronous. */
 int bbx_rt_run(bbx_rt_t* rt, int policy);
-/* Same, recording each command's (12 features, latency in us) as training data
- * for the cost model; returns the number of records in *n_out. */
-int bbx_rt_record(bbx_rt_t* rt, int policy, float* features, float* latency_us, int cap, int* n_out);
+/* Worker streams of the per-op path (1..16; default 1 = the plain path, one
+ * stream). The reference runs ready commands on num_threads worker threads
+ * (src/server/node.cc:67-69); here each worker is a stream and a command waits
+ * only on the completion events of its inputs' producers. */
+int bbx_rt_set_workers(bbx_rt_t* rt, int workers);
+/* Same as bbx_rt_run on one stream, recording each command's (12 features,
+ * latency in us, the ud's get_complexity_hint) as training data for the cost
+ * model; any output pointer may be null; returns the record count in *n_out. */
+int bbx_rt_record(bbx_rt_t* rt, int policy, float* features, float* latency_us, double* hints, int cap,
+                  int* n_out);
 
 #define BBX_SCHED_HEURISTIC 0
 #define BBX_SCHED_LEARNED 1
@@ -348,6 +355,10 @@ int bbx_mlp_get_params(bbx_mlp_t* mlp, float* out);
 int bbx_mlp_set_params(bbx_mlp_t* mlp, const float* in);
 /* install the MLP as the runtime's latency predictor (policy BBX_SCHED_LEARNED) */
 int bbx_rt_set_predictor(bbx_rt_t* rt, bbx_mlp_t* mlp);
+/* install the calibrated complexity-hint model exp(a * ln(max(hint, 1)) + b) us
+ * as the predictor instead: the reference's get_complexity_hint, fit to
+ * recorded latencies, driving the same list scheduling as the MLP. */
+int bbx_rt_set_hint_predictor(bbx_rt_t* rt, double a, double b);
 
 #ifdef __cplusplus
 }

@@ -431,3 +431,36 @@ def test_random_bf16_dag_with_contractions_matches_per_op(R, policy):
             a = rt1.get_bytes(t)
             b = dag.read_bytes(t, a.nbytes)
             assert np.array_equal(a, b), t
+
+
+# ------------------------------------------------------------------ multi-stream per-op executor
+@pytest.mark.parametrize("dtype", ["bf16", "f32"])
+def test_worker_streams_match_one_stream(R, dtype):
+    """Ready commands spread over 4 worker streams (round-robin under the
+    heuristic, earliest predicted finish under the learned / hint policies)
+    give byte-identical blocks to the single-stream path, run after run."""
+    runtime, workloads = R
+    mk = lambda rt: workloads.random_dag(rt, n_ops=120, depth=6, seed=33, dtype=dtype, lo=128, hi=512, step=64,
+                                         contraction_dims=(16, 64), mix=(0.45, 0.2, 0.2, 0.15), max_inputs=12)
+    rt1 = runtime.Runtime()
+    info = mk(rt1)
+    rt1.run()
+    want = {t: rt1.get_bytes(t) for t in info["finals"]}
+    rt2 = runtime.Runtime()
+    mk(rt2)
+    rt2.set_workers(4)
+    feats, lat, hints = rt2.record(with_hints=True)  # record always runs on one stream
+    assert len(lat) == len(hints) and np.all(hints > 0) and np.all(lat > 0)
+    a, b = np.polyfit(np.log(hints), np.log(lat), 1)
+    runs = [(runtime.HEURISTIC, None), (runtime.LEARNED, "hint"), (runtime.LEARNED, "mlp"), (runtime.HEURISTIC, None)]
+    for policy, pred in runs:
+        if pred == "hint":
+            rt2.set_hint_predictor(a, b)
+        elif pred == "mlp":
+            rt2.set_predictor(runtime.Mlp(seed=2))
+        else:
+            rt2.set_predictor(None)
+        rt2.run(policy)
+        for t, v in want.items():
+            assert np.array_equal(rt2.get_bytes(t), v), (policy, pred, t)
+    assert rt2.count() == rt1.count()  # every deleted intermediate was freed
