@@ -65,6 +65,8 @@ class TcPlan:
     def __init__(self, problems, in_dtype=BF16, tile_n=0):
         arr = (TcProblem * len(problems))(*problems)
         self.h = C.c_void_p()
+        self.in_dtype = in_dtype
+        self.trans = (bool(problems[0].trans_a), bool(problems[0].trans_b))
         check(lib.bbx_tc_plan_create(in_dtype, arr, len(problems), tile_n, C.byref(self.h)))
 
     def launch(self, stream=None):
@@ -78,9 +80,11 @@ class TcPlan:
     @property
     def kernel_name(self):
         tn = self.tile_n
+        a = "MN-major A" if self.trans[0] else "K-major A"
+        b = "K-major B" if self.trans[1] else "MN-major B"
         if tn == 512:
-            return "tc_gemm2_kernel<K-major A,MN-major B> (2-SM 256x256 pair, cta_group::2)"
-        return "tc_gemm_kernel<%d,K-major A,MN-major B,bf16>" % tn
+            return "tc_gemm2_kernel<%s,%s> (2-SM 256x256 pair, cta_group::2)" % (a, b)
+        return "tc_gemm_kernel<%d,%s,%s,%s>" % (tn, a, b, "e4m3" if self.in_dtype == E4M3 else "bf16")
 
     def close(self):
         if self.h:

@@ -124,18 +124,40 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
-def cpu_sample_tflops(threads):
+def cpu_sample_tflops(threads, a=None, b=None, want_result=False):
     """One 4096x4096 output block with K=4096 (137 GFLOP) through the oracle's
-    blocked FP32 SGEMM, the CPU restatement of dense_matrix_mult (one block op)."""
+    blocked FP32 SGEMM, the CPU restatement of dense_matrix_mult (one block op).
+    a / b: the block inputs as FP32 arrays (seeded U(-1,1) when not given)."""
     import numpy as np
     import oracle
-    rng = np.random.default_rng(0)
-    a = rng.uniform(-1, 1, (BS, BS)).astype(np.float32)
-    b = rng.uniform(-1, 1, (BS, BS)).astype(np.float32)
+    if a is None:
+        rng = np.random.default_rng(0)
+        a = rng.uniform(-1, 1, (BS, BS)).astype(np.float32)
+        b = rng.uniform(-1, 1, (BS, BS)).astype(np.float32)
     t0 = time.perf_counter()
-    oracle.sgemm(a, b, threads=threads)
+    c = oracle.sgemm(a, b, threads=threads)
     dt = time.perf_counter() - t0
+    if want_result:
+        return 2.0 * BS ** 3 / dt / 1e12, dt, c
     return 2.0 * BS ** 3 / dt / 1e12, dt
+
+
+def max_over_ranks(ms, world, device):
+    """A device-timed duration of this rank -> the job's duration (max over
+    ranks). Every rank must call it at the same point."""
+    if world == 1:
+        return float(ms)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_tflops(flop_per_rank_step, world, ms):
+    """Whole-job throughput: the FLOPs all ranks processed in one step over the
+    slowest rank's step time."""
+    return world * flop_per_rank_step / (ms * 1e-3) / 1e12
 
 
 def dist_setup(args):
@@ -185,6 +207,141 @@ def _time_on(stream_ptr, fn, reps):
     return e0.elapsed_time(e1) / reps
 
 
+# ------------------------------------------------------------------ FP64 checks of whole DAGs
+# FP64 runs on the GPU only here, in the accuracy check: blocks are widened
+# device to device (the library's cast kernel) and the DAG is re-evaluated
+# with torch in FP64 from the same stored inputs.
+def dev_block_f64(rt, tid, dag=None):
+    """A dense (f32 / bf16) or cutensor block as an FP64 tensor: dense ->
+    (rows, cols); cutensor -> its dims, indexed like the column-major modes."""
+    import struct
+    import numpy as np
+    import torch
+    from bbts_b200._lib import lib, check
+    if dag is not None:
+        ptr, meta = dag.tensor(tid)
+    else:
+        meta = rt.meta(tid)
+        ptr, _ = rt.payload(tid)
+    fmt_id = struct.unpack_from("<i", meta, 0)[0]
+    if fmt_id == rt.fmt("cutensor"):
+        rank = struct.unpack_from("<I", meta, 4)[0]
+        dims = list(struct.unpack_from("<%dq" % rank, meta, 12))
+        n, dt = int(np.prod(dims)), 0
+    else:
+        _, rows, cols = struct.unpack_from("<iII", meta, 0)
+        dims, n = [rows, cols], rows * cols
+        dt = 1 if fmt_id == rt.fmt("dense_bf16") else 0
+    out = torch.empty(n, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    check(lib.bbx_cast(dt, ptr, 0, out.data_ptr(), n, None))
+    torch.cuda.synchronize()
+    if fmt_id == rt.fmt("cutensor"):
+        return out.double().view(*reversed(dims)).permute(*reversed(range(len(dims))))
+    return out.double().view(rows, cols)
+
+
+def rel_err_f64(x, ref):
+    """(normwise max|x - ref| / max|ref|, elementwise max with a floor of 1e-6 max|ref|)."""
+    d = (x - ref).abs()
+    den = float(ref.abs().max())
+    den = den if den > 0 else 1.0
+    return float(d.max()) / den, float((d / ref.abs().clamp_min(1e-6 * den)).max())
+
+
+def dag_accuracy(rt, info, dag=None):
+    """Re-evaluates a random_dag / bmm command list in FP64 from the stored
+    inputs and returns the worst normwise and elementwise relative errors over
+    its result blocks (results read from the DAG when given, else the runtime)."""
+    import torch
+    vals = {}
+    ops = info.get("ops")
+    if ops is None:  # bmm: C(i, j) = sum_k A(i, k) B(k, j)
+        split = info["split"]
+        ops = [(2, None, (i, j)) for i in range(split) for j in range(split)]
+    finals = info.get("finals") or list(info["C"].values())
+    keep = set(finals)
+    last = {}
+    for idx, (_, ins, _) in enumerate(ops):
+        for t in ins or ():
+            last[t] = idx
+    worst, worst_el = 0.0, 0.0
+    get = lambda t: vals[t] if t in vals else vals.setdefault(t, dev_block_f64(rt, t))
+    for idx, (kind, ins, out) in enumerate(ops):
+        if ins is None:
+            i, j = out
+            r = sum(get(info["A"][(i, k)]) @ get(info["B"][(k, j)]) for k in range(info["split"]))
+            out = info["C"][(i, j)]
+        elif kind == 0:
+            r = get(ins[0]) @ get(ins[1])
+        elif kind in (1, 2):
+            r = sum(get(t) for t in ins)
+        else:
+            r = torch.einsum("ijk,kl->ijl", get(ins[0]), get(ins[1]))
+        vals[out] = r
+        for t in ins or ():
+            if last[t] == idx and t not in keep:
+                vals.pop(t, None)  # FP64 values live only until their last reader
+    for t in finals:
+        n, e = rel_err_f64(dev_block_f64(rt, t, dag), vals[t])
+        worst, worst_el = max(worst, n), max(worst_el, e)
+    return {"max_rel_err_vs_fp64": worst, "elementwise_max_rel_err": worst_el, "blocks_checked": len(finals),
+            "definition": "max over result blocks of max|x - x64| / max|x64|; x64 = FP64 re-evaluation of the "
+                          "command list from the same stored inputs (intermediates unrounded)"}
+
+
+def ffnn_accuracy(rt, info, dag=None):
+    """The FFN step in FP64 from the stored inputs, twice: all-FP64, and with
+    bf16 rounding at the points where the blocked step stores bf16
+    (activations, the softmax gradient, dA2 and each dA1 block product), which
+    separates kernel error from the error of bf16 storage itself."""
+    import numpy as np
+    import torch
+    batch, d_in, h1, h2, classes = info["dims"]
+    bs = info["bs"]
+    R, KI, K1, K2 = batch // bs, d_in // bs, h1 // bs, h2 // bs
+    blk = lambda t: dev_block_f64(rt, t)
+    X = torch.cat([torch.cat([blk(info["X"][(i, k)]) for k in range(KI)], 1) for i in range(R)], 0)
+    W1 = torch.cat([torch.cat([blk(info["W1"][(k, j)]) for j in range(K1)], 1) for k in range(KI)], 0)
+    W2 = torch.cat([torch.cat([blk(info["W2"][(k, j)]) for j in range(K2)], 1) for k in range(K1)], 0)
+    W3 = torch.cat([blk(info["W3"][k]) for k in range(K2)], 0)
+    y = torch.from_numpy(np.concatenate([rt.get_bytes(info["labels"][i]).view(np.int32) for i in range(R)])).long()
+    y = y.cuda()
+    rows = torch.arange(batch, device="cuda")
+
+    def net(emulate):
+        rb = (lambda x: x.to(torch.bfloat16).double()) if emulate else (lambda x: x)
+        A1 = rb(torch.relu(X @ W1))
+        A2 = rb(torch.relu(A1 @ W2))
+        Z3 = A2 @ W3
+        P = torch.softmax(Z3, 1)
+        loss = -torch.log(P[rows, y])
+        G3 = P.clone()
+        G3[rows, y] -= 1.0
+        G3 = rb(G3 / batch)
+        dW3 = A2.t() @ G3
+        dZ2 = rb(G3 @ W3.t()) * (A2 > 0)
+        dW2 = A1.t() @ dZ2
+        dA1 = sum(rb(dZ2[:, j * bs:(j + 1) * bs] @ W2[:, j * bs:(j + 1) * bs].t()) for j in range(K2))
+        dW1 = X.t() @ (rb(dA1) * (A1 > 0))
+        return {"loss": loss, "dW1": dW1, "dW2": dW2, "dW3": dW3}
+
+    get = lambda t: dev_block_f64(rt, t, dag)
+    got = {"loss": torch.cat([get(info["loss"][i]).reshape(-1) for i in range(R)]),
+           "dW1": torch.cat([torch.cat([get(info["dW1"][(k, j)]) for j in range(K1)], 1) for k in range(KI)], 0),
+           "dW2": torch.cat([torch.cat([get(info["dW2"][(k, j)]) for j in range(K2)], 1) for k in range(K1)], 0),
+           "dW3": torch.cat([get(info["dW3"][(k, 0)]) for k in range(K2)], 0)}
+    out = {}
+    for tag, emulate in (("vs_fp64", False), ("vs_fp64_bf16_storage_model", True)):
+        ref = net(emulate)
+        out[tag] = {k: float("%.4g" % rel_err_f64(got[k], ref[k])[0]) for k in got}
+        del ref
+    return {"max_rel_err_vs_fp64": max(out["vs_fp64"].values()),
+            "max_rel_err_vs_storage_model": max(out["vs_fp64_bf16_storage_model"].values()), **out,
+            "definition": "per tensor max|x - x64| / max|x64| over loss, dW1, dW2, dW3; x64 from the same stored "
+                          "inputs; the storage model rounds to bf16 where the blocked step stores bf16"}
+
+
 def run_dag_workload(args):
     """Whole-DAG configurations through the runtime: grouped graph path vs the
     plain FP32 per-op path, and learned vs heuristic scheduling."""
@@ -221,14 +378,25 @@ def run_dag_workload(args):
                 dag.launch()
             ms = _time_on(rt.stream.value, dag.launch, args.steps)
             flops = info["flops"]
-            result["grouped_bf16"] = {"ms": round(ms, 3), "tflops": round(flops / ms / 1e9, 2), "dag": st}
+            check = ffnn_accuracy if args.workload == "ffnn" else dag_accuracy
+            result["grouped_bf16"] = {"ms": round(ms, 3), "tflops": round(flops / ms / 1e9, 2), "dag": st,
+                                      "accuracy": check(rt, info, dag)}
             dag.close()
             rt.close()
-            # plain FP32 per-op path: same DAG in f32 blocks, reservation-station LIFO, one launch per op
+            # the FP32 variant of the same DAG: f32 blocks through the grouped graph path
             rt, info32 = build("f32", 7)
+            dag = rt.build_dag(runtime.HEURISTIC, tile_n=-1)
+            for _ in range(args.warmup):
+                dag.launch()
+            gms = _time_on(rt.stream.value, dag.launch, max(1, min(5, args.steps)))
+            result["grouped_fp32"] = {"ms": round(gms, 3), "tflops": round(info32["flops"] / gms / 1e9, 3),
+                                      "accuracy": check(rt, info32, dag)}
+            dag.close()
+            # plain FP32 per-op path: same DAG in f32 blocks, reservation-station LIFO, one launch per op
             rt.run()
             pms = _time_on(rt.stream.value, rt.run, max(1, min(3, args.steps)))
-            result["plain_fp32_per_op"] = {"ms": round(pms, 3), "tflops": round(info32["flops"] / pms / 1e9, 3)}
+            result["plain_fp32_per_op"] = {"ms": round(pms, 3), "tflops": round(info32["flops"] / pms / 1e9, 3),
+                                           "accuracy": check(rt, info32)}
             rt.close()
             value = flops / ms / 1e9
             name = {"bmm": "blocked matmul 4096^2 in 1024^2 blocks (64 matrix_mult + 16 4-input reduces)",
@@ -239,8 +407,12 @@ def run_dag_workload(args):
             line.update({"metric": "block-op DAG TFLOP/s and makespan vs plain FP32 path", "value": round(value, 2),
                          "unit": "TFLOP/s", "ms_per_step": round(ms, 3), "dtype": "bf16",
                          "config": {"workload": name, "flops_per_step": flops},
-                         "makespan_ms": {"grouped_bf16_graph": round(ms, 3), "plain_fp32_per_op": round(pms, 3)},
-                         "speedup_vs_plain_fp32": round(pms / ms, 2), "detail": result,
+                         "makespan_ms": {"grouped_bf16_graph": round(ms, 3), "grouped_fp32_graph": round(gms, 3),
+                                         "plain_fp32_per_op": round(pms, 3)},
+                         "speedup_vs_plain_fp32": round(pms / ms, 2),
+                         "max_rel_err_vs_fp64": {k: result[k]["accuracy"]["max_rel_err_vs_fp64"]
+                                                 for k in ("grouped_bf16", "grouped_fp32", "plain_fp32_per_op")},
+                         "detail": result,
                          "gpu_launches": st["tc_launches"] + st["stream_launches"] + st["other_launches"]})
         else:
             # learned scheduling: train the MLP on timings the runtime records itself
@@ -398,12 +570,9 @@ def main():
     rc = bbts_b200.lib.bbx_check_device_status(None, None)
     if rc != 0:
         raise RuntimeError(bbts_b200.last_error())
-    t = torch.tensor([total_ms], device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, world, dev)
     ms = total_ms / args.steps
-    value = world * FLOP_PER_STEP / (ms * 1e-3) / 1e12
+    value = job_tflops(FLOP_PER_STEP, world, ms)
 
     # ---------------- roofline of the dominant kernel (the grouped tcgen05 launch)
     hbm, bf16_peak, bf16_sust, src = load_peaks()
@@ -418,6 +587,62 @@ def main():
                 "traffic": TRAFFIC_BYTES_PER_LAUNCH.get(plan.tile_n) if GRID == 8 else None,
                 "peak_source": src + " bf16 sustained (of measured)", "frac_of_burst": round(achieved / bf16_peak, 4),
                 "kernel": plan.kernel_name, "launches_timed": args.steps}
+
+    # ---------------- accuracy: every output block against FP64 on the same (bf16) inputs
+    def block_errors(C):
+        errs = []
+        for i in range(GRID):
+            a64 = A[i].double()
+            for j in range(GRID):
+                r = a64 @ B[j].double()
+                errs.append(float((C[i * GRID + j].double() - r).abs().max() / r.abs().max()))
+        return errs
+
+    acc_bf16 = block_errors(Cblk)
+    accuracy = {"definition": "per output block max|x - x64| / max|x64|, x64 = FP64 product of the same inputs "
+                              "(FP64 only in this check)",
+                "bf16_max": max(acc_bf16), "bf16_per_block": [float("%.3g" % e) for e in acc_bf16]}
+
+    # ---------------- FP8-E4M3 variant: one absmax scale per 4096^2 block, same grouped launch shape
+    fp8 = None
+    if GRID == 8:
+        qA = [torch.empty(BS, BS, dtype=torch.float8_e4m3fn, device=dev) for _ in range(GRID)]
+        qB = [torch.empty(BS, BS, dtype=torch.float8_e4m3fn, device=dev) for _ in range(GRID)]
+        sA = torch.empty(GRID, device=dev)
+        sB = torch.empty(GRID, device=dev)
+
+        def quantize_all():
+            for i in range(GRID):
+                ops.quantize_e4m3(A[i], qA[i], sA[i:i + 1])
+                ops.quantize_e4m3(B[i], qB[i], sB[i:i + 1], transpose=True)  # K-major B for the fp8 MMA
+
+        quantize_all()
+        torch.cuda.synchronize()
+        hsA, hsB = sA.cpu().tolist(), sB.cpu().tolist()
+        plan8 = ops.TcPlan([ops.tc_problem(qA[i], qB[j], Cblk[i * GRID + j], trans_b=True, alpha=hsA[i] * hsB[j])
+                            for i in range(GRID) for j in range(GRID)], in_dtype=ops.E4M3)
+        for _ in range(args.warmup):
+            plan8.launch()
+        barrier()
+        q0, q1, q2 = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        q0.record(stream)
+        for _ in range(args.steps):
+            plan8.launch()
+        q1.record(stream)
+        for _ in range(args.steps):
+            quantize_all()
+        q2.record(stream)
+        barrier()
+        ms8 = q0.elapsed_time(q1) / args.steps
+        msq = q1.elapsed_time(q2) / args.steps
+        acc8 = block_errors(Cblk)
+        fp8 = {"value": round(FLOP_PER_STEP / (ms8 * 1e-3) / 1e12, 2), "unit": "TFLOP/s", "ms_per_step": round(ms8, 3),
+               "quantize_ms_per_step": round(msq, 3), "kernel": plan8.kernel_name,
+               "max_rel_err": max(acc8), "per_block": [float("%.3g" % e) for e in acc8],
+               "note": "e4m3 keeps 3 mantissa bits: outside the 1e-2 budget, reported per block"}
+        plan8.close()
+        del qA, qB
+        plan.launch()  # the bf16 result back in C for the e2e / CPU comparisons
 
     # ---------------- e2e through the C ABI with pinned host blocks
     hA = [torch.empty(BS, BS, dtype=torch.bfloat16, pin_memory=True) for _ in range(GRID)]
@@ -447,11 +672,10 @@ def main():
     e1.record(stream)
     barrier()
     e2e_ms = e0.elapsed_time(e1) / e2e_steps
-    t = torch.tensor([e2e_ms], device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_ms = float(t.item())
-    e2e_val = world * FLOP_PER_STEP / (e2e_ms * 1e-3) / 1e12
+    e2e_ms = max_over_ranks(e2e_ms, world, dev)
+    e2e_val = job_tflops(FLOP_PER_STEP, world, e2e_ms)
+
+    c_block0 = Cblk[0].cpu()  # the bf16 path's block (0, 0), before the comparator reuses C
 
     # ---------------- plain FP32 per-op path (the comparator): one SIMT launch per block op
     plain = None
@@ -483,9 +707,16 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        v, dt = cpu_sample_tflops(threads)
+        # block (0, 0) of this step, from the same bf16 inputs widened to FP32
+        a0 = A[0].float().cpu().numpy()
+        b0 = B[0].float().cpu().numpy()
+        v, dt, c0 = cpu_sample_tflops(threads, a0, b0, want_result=True)
+        r = torch.from_numpy(c0).double()
+        cpu_err = float((c_block0.double() - r).abs().max() / r.abs().max())
         cpu = {"value": round(v, 5), "unit": "TFLOP/s", "cores": threads, "kind": "port",
-               "sample": "one 4096^3 FP32 block matmul (1/64 of a step), oracle blocked SGEMM, %.1f s" % dt}
+               "sample": "output block (0,0) of the step: one 4096^3 FP32 block matmul (1/64 of a step) on the "
+                         "same inputs, oracle blocked SGEMM, %.1f s" % dt}
+        accuracy["vs_cpu_port_block0"] = cpu_err
 
     plan.close()
     if rank == 0:
@@ -501,6 +732,7 @@ def main():
                 "e2e": {"value": round(e2e_val, 2), "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_ms, 2)},
                 "roofline": roofline, "plain_fp32": plain, "cpu_baseline": cpu,
+                "accuracy": accuracy, "fp8_e4m3": fp8,
                 "gpu_launches": args.steps, "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -1,0 +1,54 @@
+"""Replica aggregation of bench.py on two gloo ranks (CPU): the job time is the
+slowest rank's device time and the job throughput counts every rank's work."""
+import os
+import socket
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _rank_main(rank, world, port, out):
+    import datetime
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    import bench
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        ms = bench.max_over_ranks(10.0 + 5.0 * rank, world, torch.device("cpu"))
+        out[rank] = (ms, bench.job_tflops(8.796e12, world, ms))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_max_over_ranks_and_job_throughput():
+    world = 2
+    port = _free_port()
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.spawn(_rank_main, args=(world, port, out), nprocs=world, join=True)
+        res = dict(out)
+    assert res[0] == res[1]                      # every rank sees the job's time
+    ms, tf = res[0]
+    assert ms == 15.0                            # the slowest rank
+    assert tf == pytest.approx(2 * 8.796e12 / 15e-3 / 1e12)
+
+
+def test_single_rank_needs_no_process_group():
+    sys.path.insert(0, ROOT)
+    import bench
+    assert bench.max_over_ranks(3.5, 1, None) == 3.5
+    assert bench.job_tflops(1e12, 1, 1000.0) == pytest.approx(1.0)
