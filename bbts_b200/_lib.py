@@ -41,6 +41,7 @@ SIGNATURES = {
     "bbx_tc_plan_launch": (i32, [vp, vp]),
     "bbx_tc_plan_destroy": (i32, [vp]),
     "bbx_tc_plan_tile_n": (i32, [vp]),
+    "bbx_dag_profile": (i32, [vp, vp, i32, vp, vp, vp, vp, vp, C.POINTER(i32)]),
     "bbx_add_f32": (i32, [pf, pf, pf, i64, vp]),
     "bbx_reduce_f32": (i32, [C.POINTER(vp), i32, pf, i64, i32, vp]),
     "bbx_unary_f32": (i32, [i32, pf, pf, i64, f32, vp]),

@@ -688,8 +688,9 @@ static int build_stream_table(const bbx_stream_op_t* ops, int count, std::vector
     }
     o.kind = q.kind; o.op = q.op; o.in_dtype = q.in_dtype; o.out_dtype = q.out_dtype;
     o.n_in = need; o.kahan = q.kahan; o.n = q.n; o.out = q.out; o.p0 = q.p0; o.p1 = q.p1;
+    // 2: every pointer 16-byte aligned (the wide path); 1: the 4-element path
     const uintptr_t need_align = (q.in_dtype == BBX_F32 || q.out_dtype == BBX_F32) ? 15 : 7;
-    o.vec = (align & need_align) == 0;
+    o.vec = (align & 15) == 0 ? 2 : (align & need_align) == 0 ? 1 : 0;
     o.chunk_start = chunks;
     chunks += (q.n + kStreamChunk - 1) / kStreamChunk;
   }

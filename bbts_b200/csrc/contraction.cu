@@ -66,6 +66,86 @@ __global__ void k_gather_sum(const float* __restrict__ in, void* out, int out_bf
 
 constexpr long long kGatherChunk = 4096;
 
+// Row path: the innermost output mode is unit-stride in both the source and
+// the destination and nothing is summed, so one warp copies a row with
+// coalesced accesses and the outer modes are decomposed once per row.
+static bool row_mode_ok(const GatherArgs& a) {
+  const int last = a.rank_o - 1;
+  return a.rank_s == 0 && last >= 0 && a.istride[last] == 1 && a.ostride[last] == 1 && a.odims[last] >= 16;
+}
+
+// Each warp carries kRowsPerWarp rows at once, so every lane has that many
+// independent loads in flight (rows are short: a row-at-a-time warp holds a
+// single 128-byte load and cannot fill HBM). The first row's outer index is
+// decomposed once; the following rows step it with a carry.
+constexpr int kRowsPerWarp = 4;
+
+__device__ __forceinline__ void gather_rows(const GatherRec& rec, long long row0, long long row1) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  // the record's fields in registers: stores to the destination could alias
+  // the record as far as the compiler knows, which would reload it every row
+  const int outer = rec.a.rank_o - 1;  // dims 0 .. outer-1 index rows, dim `outer` runs along a row
+  long long odims[3], istr[3], ostr[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    odims[d] = d < outer ? rec.a.odims[d] : 1;
+    istr[d] = d < outer ? rec.a.istride[d] : 0;
+    ostr[d] = d < outer ? rec.a.ostride[d] : 0;
+  }
+  const float* __restrict__ src = rec.src;
+  void* const dst = rec.dst;
+  const bool bf16 = rec.dst_bf16 != 0;
+  const int row_len = (int)rec.row_len;
+  for (long long row = row0 + (long long)warp * kRowsPerWarp; row < row1; row += (long long)nwarps * kRowsPerWarp) {
+    long long idx[3] = {0, 0, 0};
+    long long rem = row;
+#pragma unroll
+    for (int d = 2; d >= 0; --d) {
+      if (d < outer) {
+        idx[d] = rem % odims[d];
+        rem /= odims[d];
+      }
+    }
+    long long so[kRowsPerWarp], dso[kRowsPerWarp];
+    int nr = 0;
+#pragma unroll
+    for (int u = 0; u < kRowsPerWarp; ++u) {
+      so[u] = idx[0] * istr[0] + idx[1] * istr[1] + idx[2] * istr[2];
+      dso[u] = idx[0] * ostr[0] + idx[1] * ostr[1] + idx[2] * ostr[2];
+      if (row + u < row1) nr = u + 1;
+#pragma unroll
+      for (int d = 2; d >= 0; --d) {  // next row: the last outer dim is fastest
+        if (d < outer) {
+          if (++idx[d] < odims[d]) break;
+          idx[d] = 0;
+        }
+      }
+    }
+    for (int x = lane; x < row_len; x += 32) {
+      float v[kRowsPerWarp];
+#pragma unroll
+      for (int u = 0; u < kRowsPerWarp; ++u)
+        if (u < nr) v[u] = __ldg(src + so[u] + x);
+#pragma unroll
+      for (int u = 0; u < kRowsPerWarp; ++u) {
+        if (u < nr) {
+          if (bf16) ((__nv_bfloat16*)dst)[dso[u] + x] = __float2bfloat16_rn(v[u]);
+          else ((float*)dst)[dso[u] + x] = v[u];
+        }
+      }
+    }
+  }
+}
+
+// One gather record on the row path (the per-call contraction).
+__global__ void k_gather_rows1(const __grid_constant__ GatherRec r, long long chunks) {
+  const long long rows = r.n / r.row_len;
+  for (long long c = blockIdx.x; c < chunks; c += gridDim.x) {
+    const long long row0 = c * r.rows_per_chunk;
+    gather_rows(r, row0, min(row0 + r.rows_per_chunk, rows));
+  }
+}
+
 // Many gathers in one launch: chunk c belongs to the record whose
 // [chunk_start, next chunk_start) range holds it.
 __global__ void k_gather_group(const GatherRec* __restrict__ recs, int count, long long total_chunks) {
@@ -76,6 +156,11 @@ __global__ void k_gather_group(const GatherRec* __restrict__ recs, int count, lo
       if (recs[mid].chunk_start <= c) lo = mid; else hi = mid - 1;
     }
     const GatherRec& r = recs[lo];
+    if (r.row_mode) {
+      const long long row0 = (c - r.chunk_start) * r.rows_per_chunk;
+      gather_rows(r, row0, min(row0 + r.rows_per_chunk, r.n / r.row_len));
+      continue;
+    }
     const long long e0 = (c - r.chunk_start) * kGatherChunk;
     const long long e1 = min(e0 + kGatherChunk, r.n);
     for (long long e = e0 + threadIdx.x; e < e1; e += blockDim.x) gather_one(r.src, r.dst, r.dst_bf16, r.a, e);
@@ -84,6 +169,22 @@ __global__ void k_gather_group(const GatherRec* __restrict__ recs, int count, lo
 
 static int launch_gather(const float* in, void* out, bool bf16, const GatherArgs& a, long long n, cudaStream_t st) {
   if (n == 0) return BBX_OK;
+  if (row_mode_ok(a)) {
+    GatherRec r{};  // travels by value in the kernel parameters
+    r.a = a;
+    r.src = in;
+    r.dst = out;
+    r.dst_bf16 = bf16 ? 1 : 0;
+    r.n = n;
+    r.row_mode = 1;
+    r.row_len = a.odims[a.rank_o - 1];
+    r.rows_per_chunk = std::max<long long>(32, 2 * kGatherChunk / r.row_len);
+    const long long chunks = (n / r.row_len + r.rows_per_chunk - 1) / r.rows_per_chunk;
+    k_gather_rows1<<<(int)std::min<long long>(chunks, 148 * 8), 256, 0, st>>>(r, chunks);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_error(BBX_ERR_CUDA, "k_gather_rows1: %s", cudaGetErrorString(e));
+    return BBX_OK;
+  }
   long long blocks = (n + 255) / 256;
   if (blocks > 148 * 16) blocks = 148 * 16;
   k_gather_sum<<<(int)blocks, 256, 0, st>>>(in, out, bf16 ? 1 : 0, a, n);
@@ -153,6 +254,14 @@ int lower_contraction(int rank_l, const long long* dims_l, const int* modes_l, i
     return set_error(BBX_ERR_INVALID, "contraction group too large");
   L->kdim = nk > 0 ? nk : 1;  // no contracted mode: an outer product, k = 1
   L->pk = bf16 ? ((L->kdim + 7) / 8) * 8 : L->kdim;
+  L->pm = bf16 ? ((L->nm + 7) / 8) * 8 : L->nm;
+  L->pn = bf16 ? ((L->nn + 7) / 8) * 8 : L->nn;
+  // staging major-ness (tensor-core lowering only): MN-major when the source's
+  // fastest mode is one of the operand's M (lhs) / N (rhs) modes
+  L->lc_mn = bf16 && rank_l > 0 && cls(modes_l[0]) == CI;
+  L->rc_mn = bf16 && rank_r > 0 && cls(modes_r[0]) == CN;
+  L->lc_elems = L->nb * (L->lc_mn ? L->kdim * L->pm : L->nm * L->pk);
+  L->rc_elems = L->nb * (L->rc_mn ? L->kdim * L->pn : L->nn * L->pk);
 
   // Column-major group flattening: stride of each mode inside its group.
   auto group_strides = [&](const std::vector<int>& g, long long base, long long* st_of) {
@@ -185,8 +294,12 @@ int lower_contraction(int rank_l, const long long* dims_l, const int* modes_l, i
     }
     if (a->rank_o == 0) { a->rank_o = 1; a->odims[0] = 1; }  // empty groups behave as extent 1
   };
-  make_gather(gB, gI, gK, gL, strl, L->nm, L->pk, &L->ga);
-  make_gather(gB, gN, gK, gR, strr, L->nn, L->pk, &L->gb);
+  // K-major: [b][m][k] = outer B, mid M (pitch pk), inner K; MN-major:
+  // [b][k][m] = outer B, mid K (pitch pm), inner M
+  if (L->lc_mn) make_gather(gB, gK, gI, gL, strl, L->kdim, L->pm, &L->ga);
+  else make_gather(gB, gI, gK, gL, strl, L->nm, L->pk, &L->ga);
+  if (L->rc_mn) make_gather(gB, gK, gN, gR, strr, L->kdim, L->pn, &L->gb);
+  else make_gather(gB, gN, gK, gR, strr, L->nn, L->pk, &L->gb);
   L->nl = L->nb * L->nm * L->kdim;
   L->nr = L->nb * L->nn * L->kdim;
 
@@ -218,6 +331,36 @@ int lower_contraction(int rank_l, const long long* dims_l, const int* modes_l, i
   return BBX_OK;
 }
 
+ContractionGemm contraction_gemm(const ContractionLowering& L, const void* lc, const void* rc, void* ct, long long b) {
+  ContractionGemm g{};
+  const char* l = (const char*)lc;
+  const char* r = (const char*)rc;
+  if (L.rc_mn) {  // Rc[b][k][n]: A stored k x n, MN-major
+    g.a = r + 2 * b * L.kdim * L.pn;
+    g.trans_a = 1;
+    g.lda = L.pn;
+  } else {        // Rc[b][n][k]: A stored n x k, K-major
+    g.a = r + 2 * b * L.nn * L.pk;
+    g.trans_a = 0;
+    g.lda = L.pk;
+  }
+  if (L.lc_mn) {  // Lc[b][k][m]: op(B) = k x m stored as is
+    g.b = l + 2 * b * L.kdim * L.pm;
+    g.trans_b = 0;
+    g.ldb = L.pm;
+  } else {        // Lc[b][m][k]: B stored m x k, transposed
+    g.b = l + 2 * b * L.nm * L.pk;
+    g.trans_b = 1;
+    g.ldb = L.pk;
+  }
+  g.c = (char*)ct + 4 * b * L.nn * L.nm;
+  g.m = (int)L.nn;
+  g.n = (int)L.nm;
+  g.k = (int)L.kdim;
+  g.ldc = L.nm;
+  return g;
+}
+
 struct GatherPlan {
   GatherRec* d = nullptr;
   int count = 0;
@@ -229,8 +372,17 @@ int gather_plan_create(const GatherRec* recs, int count, GatherPlan** out) {
   std::vector<GatherRec> h(recs, recs + count);
   long long chunks = 0;
   for (auto& r : h) {
+    r.row_mode = row_mode_ok(r.a) ? 1 : 0;
     r.chunk_start = chunks;
-    chunks += (r.n + kGatherChunk - 1) / kGatherChunk;
+    if (r.row_mode) {
+      r.row_len = r.a.odims[r.a.rank_o - 1];
+      r.rows_per_chunk = std::max<long long>(32, 2 * kGatherChunk / r.row_len);
+      chunks += (r.n / r.row_len + r.rows_per_chunk - 1) / r.rows_per_chunk;
+    } else {
+      r.row_len = 0;
+      r.rows_per_chunk = 0;
+      chunks += (r.n + kGatherChunk - 1) / kGatherChunk;
+    }
   }
   auto* p = new GatherPlan();
   p->count = count;
@@ -282,9 +434,9 @@ extern "C" int bbx_contraction(const float* lhs, int rank_l, const long long* di
   void *Lc = nullptr, *Rc = nullptr;
   float* Ct = nullptr;
   cudaError_t e;
-  e = cudaMallocAsync(&Lc, (size_t)(L.nb * L.nm * L.pk * esz + 16), st);
+  e = cudaMallocAsync(&Lc, (size_t)(L.lc_elems * esz + 16), st);
   if (e != cudaSuccess) return set_error(BBX_ERR_CUDA, "cudaMallocAsync: %s", cudaGetErrorString(e));
-  e = cudaMallocAsync(&Rc, (size_t)(L.nb * L.nn * L.pk * esz + 16), st);
+  e = cudaMallocAsync(&Rc, (size_t)(L.rc_elems * esz + 16), st);
   if (e != cudaSuccess) { cudaFreeAsync(Lc, st); return set_error(BBX_ERR_CUDA, "cudaMallocAsync: %s", cudaGetErrorString(e)); }
   if (!L.direct) {
     e = cudaMallocAsync((void**)&Ct, (size_t)(L.nb * L.nn * L.nm * 4), st);
@@ -304,12 +456,11 @@ extern "C" int bbx_contraction(const float* lhs, int rank_l, const long long* di
       for (long long b = 0; b < L.nb; ++b) {
         bbx_tc_problem_t& q = probs[(size_t)b];
         memset(&q, 0, sizeof(q));
-        q.a = (const __nv_bfloat16*)Rc + b * L.nn * pitch;
-        q.b = (const __nv_bfloat16*)Lc + b * L.nm * pitch;
-        q.c = C + b * L.nn * L.nm;
-        q.m = (int)L.nn; q.n = (int)L.nm; q.k = (int)L.kdim;
-        q.trans_a = 0; q.trans_b = 1;
-        q.lda = pitch; q.ldb = pitch; q.ldc = L.nm;
+        const ContractionGemm g = contraction_gemm(L, Lc, Rc, C, b);
+        q.a = g.a; q.b = g.b; q.c = g.c;
+        q.m = g.m; q.n = g.n; q.k = g.k;
+        q.trans_a = g.trans_a; q.trans_b = g.trans_b;
+        q.lda = g.lda; q.ldb = g.ldb; q.ldc = g.ldc;
         q.alpha = alpha; q.beta = 0.f;
       }
       rc = bbx_matmul_tc(BBX_BF16, probs.data(), (int)L.nb, 0, stream);

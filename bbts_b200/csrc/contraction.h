@@ -16,16 +16,33 @@ struct GatherArgs {
   long long sdims[4], sstride[4];
 };
 
-// Lc[b][m][k] (pitch pk) <- lhs, Rc[b][n][k] <- rhs; Ct[b][n][m] = alpha Rc Lc^T;
-// if !direct, out <- Ct through `go`.
+// Lc <- lhs and Rc <- rhs, then Ct[b][n][m] = alpha Rc Lc^T; if !direct,
+// out <- Ct through `go`. Staging layouts (bf16 lowering): each operand is
+// K-major (Lc[b][m][k], Rc[b][n][k], pitch pk) or MN-major (Lc[b][k][m] pitch
+// pm, Rc[b][k][n] pitch pn), whichever keeps its source's fastest mode
+// fastest, so the gather streams; the tensor cores read either layout. The
+// FP32 lowering is always K-major.
 struct ContractionLowering {
   bool empty;          // an output extent is 0: nothing to do
   bool direct;         // Ct is the output itself
-  long long nb, nm, nn, kdim, pk;
+  bool lc_mn, rc_mn;   // Lc / Rc staged MN-major
+  long long nb, nm, nn, kdim, pk, pm, pn;
+  long long lc_elems, rc_elems;  // staging sizes in elements, padding included
   long long nl, nr;    // elements gathered into Lc / Rc (unpadded)
   long long no;        // output elements (for the final gather)
   GatherArgs ga, gb, go;
 };
+
+// The batched GEMM of a bf16 lowering as tensor-core problem fields for batch
+// b: A = Rc (rows n), B = Lc (columns m), C = Ct[b] (f32, ldc = nm).
+struct ContractionGemm {
+  const void* a;
+  const void* b;
+  void* c;
+  int m, n, k, trans_a, trans_b;
+  long long lda, ldb, ldc;
+};
+ContractionGemm contraction_gemm(const ContractionLowering& L, const void* lc, const void* rc, void* ct, long long b);
 
 // Returns 0 or a BBX_ERR_* code (message via set_error).
 int lower_contraction(int rank_l, const long long* dims_l, const int* modes_l, int rank_r,
@@ -38,9 +55,11 @@ struct GatherRec {
   const float* src;
   void* dst;
   int dst_bf16;
-  int pad_;
+  int row_mode;            // set by gather_plan_create: innermost mode contiguous on both sides
   long long n;
-  long long chunk_start;
+  long long chunk_start;   // set by gather_plan_create
+  long long row_len;       // row mode: elements per row (the innermost extent)
+  long long rows_per_chunk;
 };
 
 struct GatherPlan;

@@ -91,7 +91,35 @@ struct group_t {
   bbx::GatherPlan* gather_plan = nullptr;
   std::vector<opaque_t> opaque;
   std::vector<int> deps;  // indices of earlier groups this one waits for
+  double flops = 0.0;     // algorithmic work of the launch: 2mnk for tensor groups,
+  double bytes = 0.0;     // bytes read + written once for streaming / gather groups
 };
+
+double tc_group_flops(const std::vector<bbx_tc_problem_t>& ps) {
+  double f = 0;
+  for (auto& q : ps) f += 2.0 * q.m * (double)q.n * q.k;
+  return f;
+}
+
+double tc_group_bytes(const std::vector<bbx_tc_problem_t>& ps, int in_esz) {
+  double b = 0;
+  for (auto& q : ps)
+    b += ((double)q.m * q.k + (double)q.k * q.n) * in_esz + (double)q.m * q.n * ((q.flags & BBX_EPI_OUT_BF16) ? 2 : 4);
+  return b;
+}
+
+double stream_group_bytes(const std::vector<bbx_stream_op_t>& ops) {
+  double b = 0;
+  for (auto& s : ops)
+    b += (double)s.n * (s.n_in * (s.in_dtype == BBX_BF16 ? 2 : 4) + (s.out_dtype == BBX_BF16 ? 2 : 4));
+  return b;
+}
+
+double gather_group_bytes(const std::vector<bbx::GatherRec>& rs) {
+  double b = 0;
+  for (auto& r : rs) b += (double)r.n * (4 + (r.dst_bf16 ? 2 : 4));
+  return b;
+}
 
 }  // namespace
 
@@ -405,8 +433,8 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
       d->tensors[t] = tp;
       return t;
     };
-    cs.lc = stage((size_t)(cs.L.nb * cs.L.nm * cs.L.pk * 2 + 16));
-    cs.rc = stage((size_t)(cs.L.nb * cs.L.nn * cs.L.pk * 2 + 16));
+    cs.lc = stage((size_t)(cs.L.lc_elems * 2 + 16));
+    cs.rc = stage((size_t)(cs.L.rc_elems * 2 + 16));
     cs.ct = cs.L.direct ? TID_NONE : stage((size_t)(cs.L.nb * cs.L.nn * cs.L.nm * 4));
     cstage[i] = cs;
   }
@@ -521,15 +549,16 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
           gpre.writes.push_back(cs.lc);
           gpre.writes.push_back(cs.rc);
           void* C = L.direct ? d->tensors.at(n.outs[0]).payload : d->tensors.at(cs.ct).payload;
-          const int key = ELEM_BF16 * 4 + 0 + 1;  // A = Rc (K-major), B = Lc stored n x k (trans_b)
+          // A = Rc, B = Lc in their staging layouts: the problems join the
+          // group of matmuls with the same operand layouts
+          const int key = ELEM_BF16 * 4 + (L.rc_mn ? 2 : 0) + (L.lc_mn ? 0 : 1);
           for (long long b = 0; b < L.nb; ++b) {
+            const bbx::ContractionGemm g = bbx::contraction_gemm(L, tl.payload, tr.payload, C, b);
             bbx_tc_problem_t q{};
-            q.a = (const char*)tr.payload + 2 * b * L.nn * L.pk;
-            q.b = (const char*)tl.payload + 2 * b * L.nm * L.pk;
-            q.c = (char*)C + 4 * b * L.nn * L.nm;
-            q.m = (int)L.nn; q.n = (int)L.nm; q.k = (int)L.kdim;
-            q.trans_a = 0; q.trans_b = 1;
-            q.lda = L.pk; q.ldb = L.pk; q.ldc = L.nm;
+            q.a = g.a; q.b = g.b; q.c = g.c;
+            q.m = g.m; q.n = g.n; q.k = g.k;
+            q.trans_a = g.trans_a; q.trans_b = g.trans_b;
+            q.lda = g.lda; q.ldb = g.ldb; q.ldc = g.ldc;
             q.alpha = cs.p.alpha;
             tc_groups[key].push_back(q);
           }
@@ -606,6 +635,7 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
     // group order inside a wave: PRE, STREAM phases, OTHER (memory stream); TC (tensor stream); POST
     if (!pre.empty()) {
       dag_bbx(bbx::gather_plan_create(pre.data(), (int)pre.size(), &gpre.gather_plan));
+      gpre.bytes = gather_group_bytes(pre);
       d->groups.push_back(std::move(gpre));
       d->stats.stream_launches++;
     }
@@ -613,6 +643,7 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
       if (phases[ph].empty()) continue;
       group_t g{G_STREAM, w};
       dag_bbx(bbx_stream_plan_create(phases[ph].data(), (int)phases[ph].size(), &g.stream_plan));
+      g.bytes = stream_group_bytes(phases[ph]);
       g.reads = phase_rw[ph].first;
       g.writes = phase_rw[ph].second;
       d->groups.push_back(std::move(g));
@@ -629,6 +660,8 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
       const int tn = tile_n < 0 ? autotune_tile_n(dt, (kv.first & 2) != 0, (kv.first & 1) != 0, kv.second) : tile_n;
       dag_bbx(bbx_tc_plan_create(dt == ELEM_E4M3 ? BBX_E4M3 : BBX_BF16, kv.second.data(), (int)kv.second.size(), tn,
                                  &g.tc_plan));
+      g.flops = tc_group_flops(kv.second);
+      g.bytes = tc_group_bytes(kv.second, dt == ELEM_E4M3 ? 1 : 2);
       g.reads = tc_rw[kv.first].first;
       g.writes = tc_rw[kv.first].second;
       d->groups.push_back(std::move(g));
@@ -636,6 +669,7 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
     }
     if (!post.empty()) {
       dag_bbx(bbx::gather_plan_create(post.data(), (int)post.size(), &gpost.gather_plan));
+      gpost.bytes = gather_group_bytes(post);
       d->groups.push_back(std::move(gpost));
       d->stats.stream_launches++;
     }
@@ -720,6 +754,33 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
 }
 
 void dag_launch(dag_t* d, cudaStream_t st) { dag_cuda(cudaGraphLaunch(d->exec, st), "cudaGraphLaunch"); }
+
+// Replays every group on its own, one after another on `st`, bracketed by
+// timing events: each launch's duration without the graph's overlap, for
+// per-group roofline fractions. Group order is topological, so one stream
+// honours every dependency; the results equal a graph replay's.
+std::vector<dag_group_profile_t> dag_profile(dag_t* d, cudaStream_t st) {
+  const size_t G = d->groups.size();
+  std::vector<cudaEvent_t> ev(G + 1);
+  for (auto& e : ev) dag_cuda(cudaEventCreate(&e), "cudaEventCreate");
+  dag_cuda(cudaEventRecord(ev[0], st), "profile event");
+  for (size_t gi = 0; gi < G; ++gi) {
+    launch_group(d, d->groups[gi], st);
+    dag_cuda(cudaEventRecord(ev[gi + 1], st), "profile event");
+  }
+  dag_cuda(cudaEventSynchronize(ev[G]), "profile sync");
+  std::vector<dag_group_profile_t> out(G);
+  for (size_t gi = 0; gi < G; ++gi) {
+    const group_t& g = d->groups[gi];
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev[gi], ev[gi + 1]);
+    out[gi] = {(int)g.kind, g.wave, ms, g.flops, g.bytes};
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  return out;
+}
+
+int dag_num_groups(const dag_t* d) { return (int)d->groups.size(); }
 
 void dag_destroy(dag_t* d) {
   if (!d) return;

@@ -352,6 +352,27 @@ int bbx_dag_stats(bbx_dag_t* dag, double* flops, double* bytes, int* waves, int*
   return BBX_OK;
 }
 
+int bbx_dag_profile(bbx_dag_t* dag, void* stream, int cap, int* kinds, int* waves, float* ms, double* flops,
+                    double* bytes, int* n_out) {
+  if (!dag) return bbx::set_error(BBX_ERR_INVALID, "null dag");
+  if (cap <= 0) {  // count only, nothing runs
+    if (n_out) *n_out = dag_num_groups(dag->d);
+    return BBX_OK;
+  }
+  RT_TRY({
+    auto prof = dag_profile(dag->d, (cudaStream_t)stream);
+    const int n = std::min<int>(cap, (int)prof.size());
+    for (int i = 0; i < n; ++i) {
+      if (kinds) kinds[i] = prof[i].kind;
+      if (waves) waves[i] = prof[i].wave;
+      if (ms) ms[i] = prof[i].ms;
+      if (flops) flops[i] = prof[i].flops;
+      if (bytes) bytes[i] = prof[i].bytes;
+    }
+    if (n_out) *n_out = (int)prof.size();
+  });
+}
+
 int bbx_dag_tensor(bbx_dag_t* dag, int tid, void** ptr, void* meta_out) {
   if (!dag) return bbx::set_error(BBX_ERR_INVALID, "null dag");
   tensor_meta_t m;

@@ -120,5 +120,14 @@ struct dag_stats_t {
   size_t arena_bytes;
 };
 dag_stats_t dag_stats(const dag_t* d);
+// kind: 0 contraction input gathers, 1 grouped streaming ops, 2 ops called
+// through their impls, 3 grouped tcgen05 GEMM, 4 contraction output gathers
+struct dag_group_profile_t {
+  int kind, wave;
+  float ms;
+  double flops, bytes;
+};
+std::vector<dag_group_profile_t> dag_profile(dag_t* d, cudaStream_t st);
+int dag_num_groups(const dag_t* d);
 
 }  // namespace bbts

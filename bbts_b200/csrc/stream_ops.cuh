@@ -341,7 +341,7 @@ struct StreamOp {
   void* out;
   float p0, p1;
   long long chunk_start;
-  int vec;  // all pointers 16-byte aligned (f32) / 8-byte aligned (bf16)
+  int vec;  // 2: all pointers 16-byte aligned; 1: 16-byte (f32) / 8-byte (bf16) aligned; 0: scalar
   int pad_;
 };
 
@@ -389,6 +389,135 @@ struct StreamInline {
   StreamOp ops[kStreamInline];
 };
 
+// ---- wide path: every pointer of the op 16-byte aligned, one 16-byte access
+// per input per step (8 bf16 or 4 f32 elements)
+template <int DT, int VW>
+__device__ __forceinline__ void ldv(const void* p, long long i, float (&v)[VW]) {
+  if constexpr (DT == 0) {
+    const float4 x = *(const float4*)((const float*)p + i);
+    v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+  } else {
+    const uint4 x = *(const uint4*)((const __nv_bfloat16*)p + i);
+    const uint32_t w[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float2 f = __bfloat1622float2(*(const __nv_bfloat162*)&w[q]);
+      v[2 * q] = f.x;
+      v[2 * q + 1] = f.y;
+    }
+  }
+}
+
+template <int DT, int VW>
+__device__ __forceinline__ void stv(void* p, long long i, const float (&v)[VW]) {
+  if constexpr (DT == 0) {
+#pragma unroll
+    for (int q = 0; q < VW; q += 4) *(float4*)((float*)p + i + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
+  } else {
+    uint32_t w[VW / 2];
+#pragma unroll
+    for (int q = 0; q < VW / 2; ++q) {
+      const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+      w[q] = *(const uint32_t*)&h;
+    }
+    if constexpr (VW == 8) *(uint4*)((__nv_bfloat16*)p + i) = make_uint4(w[0], w[1], w[2], w[3]);
+    else *(uint2*)((__nv_bfloat16*)p + i) = make_uint2(w[0], w[1]);
+  }
+}
+
+// a += b in order (Kahan-compensated when asked), elementwise over VW lanes
+template <int VW>
+__device__ __forceinline__ void fold_in(float (&a)[VW], float (&comp)[VW], const float (&b)[VW], bool kahan) {
+#pragma unroll
+  for (int u = 0; u < VW; ++u) {
+    if (kahan) {
+      const float y = __fsub_rn(b[u], comp[u]);
+      const float t = __fadd_rn(a[u], y);
+      comp[u] = __fsub_rn(__fsub_rn(t, a[u]), y);
+      a[u] = t;
+    } else {
+      a[u] = __fadd_rn(a[u], b[u]);
+    }
+  }
+}
+
+// Elements [e0, e1) of one op. Sums fold the inputs left to right exactly as
+// the narrow path does; loads of up to four inputs are issued before they are
+// folded, so each thread keeps several 16-byte loads in flight.
+template <int IDT, int ODT, typename OpT>
+__device__ __forceinline__ void stream_wide(const OpT& o, long long e0, long long e1) {
+  constexpr int VW = IDT == 1 ? 8 : 4;
+  const int kind = o.kind, nin = o.n_in, op = o.op;
+  const bool kahan = o.kahan != 0;
+  const float p0 = o.p0, p1 = o.p1;
+  const void* const* in = o.in;  // read per use: a local copy indexed at run time would live in local memory
+  void* const out = o.out;
+  for (long long i = e0 + (long long)VW * threadIdx.x; i < e1; i += (long long)VW * blockDim.x) {
+    if (i + VW <= e1) {
+      float a[VW], r[VW];
+      ldv<IDT, VW>(in[0], i, a);
+      if (kind == S_SUM) {
+        float comp[VW];
+#pragma unroll
+        for (int u = 0; u < VW; ++u) comp[u] = 0.f;
+        int j = 1;
+        for (; j + 3 < nin; j += 4) {
+          float b0[VW], b1[VW], b2[VW], b3[VW];
+          ldv<IDT, VW>(in[j], i, b0);
+          ldv<IDT, VW>(in[j + 1], i, b1);
+          ldv<IDT, VW>(in[j + 2], i, b2);
+          ldv<IDT, VW>(in[j + 3], i, b3);
+          fold_in(a, comp, b0, kahan);
+          fold_in(a, comp, b1, kahan);
+          fold_in(a, comp, b2, kahan);
+          fold_in(a, comp, b3, kahan);
+        }
+        for (; j < nin; ++j) {
+          float b0[VW];
+          ldv<IDT, VW>(in[j], i, b0);
+          fold_in(a, comp, b0, kahan);
+        }
+#pragma unroll
+        for (int u = 0; u < VW; ++u) r[u] = a[u];
+      } else if (kind == S_BINARY) {
+        float b[VW];
+        ldv<IDT, VW>(in[1], i, b);
+#pragma unroll
+        for (int u = 0; u < VW; ++u) r[u] = apply_binary(op, a[u], b[u], p0, p1);
+      } else if (kind == S_UNARY) {
+#pragma unroll
+        for (int u = 0; u < VW; ++u) r[u] = apply_unary(op, a[u], p0);
+      } else {
+#pragma unroll
+        for (int u = 0; u < VW; ++u) r[u] = a[u];
+      }
+      stv<ODT, VW>(out, i, r);
+    } else {
+      for (long long q = i; q < e1; ++q) {
+        float x = ld1(in[0], IDT, q);
+        if (kind == S_SUM) {
+          float comp = 0.f;
+          for (int j = 1; j < nin; ++j) {
+            const float v = ld1(in[j], IDT, q);
+            if (kahan) {
+              const float y = __fsub_rn(v, comp), t = __fadd_rn(x, y);
+              comp = __fsub_rn(__fsub_rn(t, x), y);
+              x = t;
+            } else {
+              x = __fadd_rn(x, v);
+            }
+          }
+        } else if (kind == S_BINARY) {
+          x = apply_binary(op, x, ld1(in[1], IDT, q), p0, p1);
+        } else if (kind == S_UNARY) {
+          x = apply_unary(op, x, p0);
+        }
+        st1(out, ODT, q, x);
+      }
+    }
+  }
+}
+
 template <typename TableT>
 __device__ __forceinline__ void stream_group_body(const TableT* __restrict__ table, int count,
                                                   long long total_chunks);
@@ -418,6 +547,15 @@ __device__ __forceinline__ void stream_group_body(const TableT* __restrict__ tab
     const long long e0 = (c - o.chunk_start) * kStreamChunk;
     const long long e1 = min(e0 + kStreamChunk, o.n);
     const int kind = o.kind, idt = o.in_dtype, odt = o.out_dtype, nin = o.n_in;
+    if (o.vec == 2) {
+      switch (idt * 2 + odt) {
+        case 0: stream_wide<0, 0>(o, e0, e1); break;
+        case 1: stream_wide<0, 1>(o, e0, e1); break;
+        case 2: stream_wide<1, 0>(o, e0, e1); break;
+        default: stream_wide<1, 1>(o, e0, e1); break;
+      }
+      continue;
+    }
     if (o.vec) {
       for (long long i = e0 + 4 * threadIdx.x; i < e1; i += 4 * blockDim.x) {
         if (i + 4 <= e1) {

@@ -247,6 +247,25 @@ class Dag:
         return {"flops": fl.value, "bytes": by.value, "waves": w.value, "tc_launches": t.value,
                 "stream_launches": s.value, "other_launches": o.value, "arena_bytes": ar.value}
 
+    GROUP_KINDS = ("gather_in", "stream", "impl", "tc_gemm", "gather_out")
+
+    def profile(self, stream=None):
+        """Each launch group replayed on its own: a list of dicts with kind,
+        wave, ms, flops and bytes (the algorithmic work of the launch)."""
+        st = stream if stream is not None else self.rt.stream
+        n = C.c_int()
+        check(lib.bbx_dag_profile(self.h, st, 0, None, None, None, None, None, C.byref(n)))
+        cap = n.value
+        kinds = np.empty(cap, np.int32)
+        waves = np.empty(cap, np.int32)
+        ms = np.empty(cap, np.float32)
+        fl = np.empty(cap, np.float64)
+        by = np.empty(cap, np.float64)
+        check(lib.bbx_dag_profile(self.h, st, cap, kinds.ctypes.data, waves.ctypes.data, ms.ctypes.data,
+                                  fl.ctypes.data, by.ctypes.data, C.byref(n)))
+        return [{"kind": self.GROUP_KINDS[k], "wave": int(w), "ms": float(m), "flops": float(f), "bytes": float(b)}
+                for k, w, m, f, b in zip(kinds, waves, ms, fl, by)]
+
     def tensor(self, tid):
         p = C.c_void_p()
         m = C.create_string_buffer(META_BYTES)

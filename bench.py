@@ -346,6 +346,32 @@ def ffnn_accuracy(rt, info, dag=None):
                           "inputs; the storage model rounds to bf16 where the blocked step stores bf16"}
 
 
+def group_rooflines(prof, hbm_gbs, bf16_tflops):
+    """Per launch-group class of a DAG replayed group by group: time, and the
+    tensor fraction of the GEMM groups (FLOPs / time vs the burst bf16 peak: each
+    launch is timed alone) or the HBM fraction of the streaming / gather groups
+    (algorithmic bytes / time vs the measured copy bandwidth)."""
+    out = {}
+    for g in prof:
+        a = out.setdefault(g["kind"], {"launches": 0, "ms": 0.0, "flops": 0.0, "bytes": 0.0})
+        a["launches"] += 1
+        a["ms"] += g["ms"]
+        a["flops"] += g["flops"]
+        a["bytes"] += g["bytes"]
+    for k, a in out.items():
+        s = a["ms"] * 1e-3
+        if k == "tc_gemm":
+            a["tflops"] = round(a["flops"] / s / 1e12, 1) if s > 0 else None
+            a["frac_of_bf16_burst"] = round(a["flops"] / s / 1e12 / bf16_tflops, 3) if s > 0 else None
+        elif a["bytes"] > 0:
+            a["gbs"] = round(a["bytes"] / s / 1e9, 1) if s > 0 else None
+            a["frac_of_hbm"] = round(a["bytes"] / s / 1e9 / hbm_gbs, 3) if s > 0 else None
+        a["ms"] = round(a["ms"], 3)
+    out["serial_sum_ms"] = round(sum(g["ms"] for g in prof), 3)
+    out["per_group"] = [[g["kind"], g["wave"], round(g["ms"], 4), g["flops"], g["bytes"]] for g in prof]
+    return out
+
+
 def run_dag_workload(args):
     """Whole-DAG configurations through the runtime: grouped graph path vs the
     plain FP32 per-op path, and learned vs heuristic scheduling."""
@@ -384,10 +410,19 @@ def run_dag_workload(args):
             flops = info["flops"]
             check = ffnn_accuracy if args.workload == "ffnn" else dag_accuracy
             result["grouped_bf16"] = {"ms": round(ms, 3), "tflops": round(flops / ms / 1e9, 2), "dag": st,
+                                      "groups": group_rooflines(dag.profile(), hbm, bf16_peak),
                                       "accuracy": check(rt, info, dag)}
             dag.close()
             rt.close()
-            # the FP32 variant of the same DAG: f32 blocks through the grouped graph path
+            # plain FP32 per-op path: same DAG in f32 blocks on a fresh runtime,
+            # reservation-station LIFO, one launch per op; median of 3 runs after a warm-up
+            rt, info32 = build("f32", 7)
+            rt.run()
+            pms = float(np.median([_time_on(rt.stream.value, rt.run, 1) for _ in range(3)]))
+            result["plain_fp32_per_op"] = {"ms": round(pms, 3), "tflops": round(info32["flops"] / pms / 1e9, 3),
+                                           "accuracy": check(rt, info32)}
+            rt.close()
+            # the FP32 variant through the grouped graph path
             rt, info32 = build("f32", 7)
             dag = rt.build_dag(runtime.HEURISTIC, tile_n=-1)
             for _ in range(args.warmup):
@@ -396,11 +431,6 @@ def run_dag_workload(args):
             result["grouped_fp32"] = {"ms": round(gms, 3), "tflops": round(info32["flops"] / gms / 1e9, 3),
                                       "accuracy": check(rt, info32, dag)}
             dag.close()
-            # plain FP32 per-op path: same DAG in f32 blocks, reservation-station LIFO, one launch per op
-            rt.run()
-            pms = _time_on(rt.stream.value, rt.run, max(1, min(3, args.steps)))
-            result["plain_fp32_per_op"] = {"ms": round(pms, 3), "tflops": round(info32["flops"] / pms / 1e9, 3),
-                                           "accuracy": check(rt, info32)}
             rt.close()
             value = flops / ms / 1e9
             name = {"bmm": "blocked matmul 4096^2 in 1024^2 blocks (64 matrix_mult + 16 4-input reduces)",

@@ -327,6 +327,15 @@ int bbx_dag_launch(bbx_dag_t* dag, void* stream);
 int bbx_dag_destroy(bbx_dag_t* dag);
 int bbx_dag_stats(bbx_dag_t* dag, double* flops, double* bytes, int* waves, int* tc_launches,
                   int* stream_launches, int* other_launches, size_t* arena_bytes);
+/* Replays each launch group of the DAG on its own, one after another on
+ * `stream`, and reports per group (up to cap): kind (0 contraction input
+ * gathers, 1 grouped streaming ops, 2 ops called through their impls, 3
+ * grouped tcgen05 GEMM, 4 contraction output gathers), wave, duration in ms and
+ * the algorithmic FLOPs / bytes of the launch; *n_out = the group count.
+ * Synchronous; results equal a graph replay's. cap <= 0 only counts the
+ * groups and runs nothing. */
+int bbx_dag_profile(bbx_dag_t* dag, void* stream, int cap, int* kinds, int* waves, float* ms, double* flops,
+                    double* bytes, int* n_out);
 /* device address and meta of a tensor the DAG reads or produces */
 int bbx_dag_tensor(bbx_dag_t* dag, int tid, void** ptr, void* meta_out);
 /* copies up to `cap` payload bytes of a DAG tensor to host memory (synchronous) */

@@ -362,6 +362,8 @@ def test_contraction_golden(T, precision):
     ([50, 40], [0, 1], [40, 30], [1, 2], [2, 0]),                 # transposed output
     ([20, 30, 6], [0, 1, 2], [30, 25], [1, 3], [3, 0]),           # lhs-only mode summed
     ([8, 9], [0, 1], [10, 11], [2, 3], [0, 2, 1, 3]),             # outer product
+    ([37, 64], [0, 2], [129, 64], [3, 2], [0, 3]),               # both operands staged MN-major
+    ([24, 40, 5], [0, 2, 1], [33, 40, 5], [3, 2, 1], [0, 3, 1]),  # batched, both MN-major
 ])
 @pytest.mark.parametrize("precision", [0, 1])
 def test_contraction_random_vs_f64(T, spec, precision):
@@ -379,6 +381,13 @@ def test_contraction_random_vs_f64(T, spec, precision):
     else:
         ref = oracle.contraction_f64(lhs, dl, ml, rhs, dr, mr, mo, 0.5)
         assert rel_err(host(out), ref) <= 1e-2
+        # with no mode summed inside a gather (every lhs / rhs mode is shared or
+        # kept), the bf16 staging rounds the inputs themselves: against FP64 of
+        # the rounded inputs only the f32 accumulation differs, so a
+        # staging-layout slip cannot hide inside the bf16 budget
+        if set(ml) <= set(mr) | set(mo) and set(mr) <= set(ml) | set(mo):
+            ref_q = oracle.contraction_f64(bf16_round(lhs), dl, ml, bf16_round(rhs), dr, mr, mo, 0.5)
+            assert rel_err(host(out), ref_q) <= 1e-5
 
 
 # ----------------------------------------------------------------- 2-SM (cta_group::2) tile

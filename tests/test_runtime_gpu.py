@@ -464,3 +464,24 @@ def test_worker_streams_match_one_stream(R, dtype):
         for t, v in want.items():
             assert np.array_equal(rt2.get_bytes(t), v), (policy, pred, t)
     assert rt2.count() == rt1.count()  # every deleted intermediate was freed
+
+
+def test_dag_profile_accounts_for_the_work(R):
+    """Group-by-group replay: the tensor groups carry all 2mnk of the matmuls,
+    the streaming group the (n_in + 1) block reads / writes of the 4-input
+    reduces, and a profiled replay leaves the same results as the graph."""
+    runtime, workloads = R
+    rt = runtime.Runtime()
+    info = workloads.bmm(rt, n=1024, split=4, dtype="bf16", seed=6, host=False)
+    dag = rt.build_dag(runtime.HEURISTIC)
+    dag.launch()
+    first = {t: dag.read_bytes(t, 256 * 256 * 4) for t in info["C"].values()}
+    prof = dag.profile()
+    assert len(prof) == dag.stats()["tc_launches"] + dag.stats()["stream_launches"]
+    tc = [g for g in prof if g["kind"] == "tc_gemm"]
+    st = [g for g in prof if g["kind"] == "stream"]
+    assert sum(g["flops"] for g in tc) == info["flops"]
+    assert sum(g["bytes"] for g in st) == 16 * 5 * 256 * 256 * 4  # f32 partials and sums
+    assert all(g["ms"] > 0 for g in prof)
+    for t, v in first.items():
+        assert np.array_equal(dag.read_bytes(t, v.nbytes), v)
