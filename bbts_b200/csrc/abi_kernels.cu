@@ -379,9 +379,16 @@ int bbx_tc_plan_create(int in_dtype, const bbx_tc_problem_t* problems, int count
   rc = group_layout(problems, count, &p->amn, &p->bmn);
   if (rc) { delete p; return rc; }
   p->host.resize(count);
+  // The persistent grid strides over the concatenated tile list, so CTA c runs
+  // tiles c, c + grid, ... Problems go in descending-K order (stable): each
+  // round of `grid` consecutive tiles then holds tiles of similar cost, which
+  // evens out the work per CTA when a group mixes short and long K loops.
+  std::vector<int> order(count);
+  for (int i = 0; i < count; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return problems[x].k > problems[y].k; });
   int tiles = 0;
   for (int i = 0; i < count; ++i) {
-    rc = build_problem(in_dtype, problems[i], tile_n, &p->host[i]);
+    rc = build_problem(in_dtype, problems[order[i]], tile_n, &p->host[i]);
     if (rc) { delete p; return rc; }
     p->host[i].tile_start = tiles;
     tiles += p->host[i].tiles_m * p->host[i].tiles_n;

@@ -60,6 +60,16 @@ struct TcArgs {
   TcProblem inline_probs[kTcMaxInline];
 };
 
+// Per-problem tile metadata (tile_start, tiles_m, tiles_n, k) is staged in
+// shared memory for groups of up to kTcMetaMax problems, so locating a tile
+// is an on-chip binary search instead of a chain of dependent global loads.
+constexpr int kTcMetaMax = 512;
+constexpr int kTcMetaBytes = kTcMetaMax * 16;
+// Epilogue staging: each of the 4 epilogue warps turns its 32 rows x 32
+// columns into contiguous row segments through a 32 x 33 float buffer.
+constexpr int kTcEpiPitch = 33;
+constexpr int kTcEpiBytes = 4 * 32 * kTcEpiPitch * 4;
+
 template <int BN, bool A_MN, bool B_MN, bool FP8>
 struct TcCfg {
   static constexpr int BM = 128;
@@ -72,7 +82,8 @@ struct TcCfg {
   static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
   static constexpr int STAGES = (BN == 256) ? 4 : 6;
   static constexpr int TMEM_COLS = 2 * BN;            // double-buffered accumulator
-  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align slack*/ + 256 /*bars*/;
+  static constexpr int SMEM_BYTES =
+      STAGES * STAGE_BYTES + 1024 /*align slack*/ + 256 /*bars*/ + kTcMetaBytes + kTcEpiBytes;
   static constexpr int THREADS = 192;
   static constexpr int MN_BOX = 128 / ELEM;           // MN-major TMA box width (elements)
 };
@@ -81,26 +92,163 @@ __device__ __forceinline__ const TcProblem* tc_problem(const TcArgs& args, int p
   return args.table ? (args.table + p) : (args.inline_probs + p);
 }
 
-// Map a global tile index to (problem, tile_m, tile_n). Tiles inside a problem
-// are visited in groups of 8 tile-rows so concurrently running CTAs share
-// operand tiles in L2.
-__device__ __forceinline__ void tc_locate(const TcArgs& args, int t, int& p, int& tm, int& tn) {
+// All threads of the CTA; visible after the prologue's __syncthreads.
+__device__ __forceinline__ void tc_stage_meta(const TcArgs& args, int4* meta) {
+  if (args.num_problems > kTcMetaMax) return;
+  for (int i = threadIdx.x; i < args.num_problems; i += blockDim.x) {
+    const TcProblem* pr = tc_problem(args, i);
+    meta[i] = make_int4(pr->tile_start, pr->tiles_m, pr->tiles_n, pr->k);
+  }
+}
+
+// Map a global tile index to (problem, tile_m, tile_n) and the problem's k.
+// Tiles inside a problem are visited in groups of 8 tile-rows so concurrently
+// running CTAs share operand tiles in L2.
+__device__ __forceinline__ void tc_locate(const TcArgs& args, const int4* meta, int t, int& p, int& tm, int& tn,
+                                          int& k) {
   int lo = 0, hi = args.num_problems - 1;
-  while (lo < hi) {  // last problem with tile_start <= t
-    int mid = (lo + hi + 1) >> 1;
-    if (tc_problem(args, mid)->tile_start <= t) lo = mid; else hi = mid - 1;
+  int4 e;
+  if (args.num_problems <= kTcMetaMax) {
+    while (lo < hi) {  // last problem with tile_start <= t
+      const int mid = (lo + hi + 1) >> 1;
+      if (meta[mid].x <= t) lo = mid; else hi = mid - 1;
+    }
+    e = meta[lo];
+  } else {
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (tc_problem(args, mid)->tile_start <= t) lo = mid; else hi = mid - 1;
+    }
+    const TcProblem* pr = tc_problem(args, lo);
+    e = make_int4(pr->tile_start, pr->tiles_m, pr->tiles_n, pr->k);
   }
   p = lo;
-  const TcProblem* pr = tc_problem(args, p);
-  int lt = t - pr->tile_start;
+  k = e.w;
+  const int lt = t - e.x;
   constexpr int G = 8;
-  int per_group = G * pr->tiles_n;
-  int group = lt / per_group;
-  int first_m = group * G;
-  int gsize = min(pr->tiles_m - first_m, G);
-  int r = lt - group * per_group;
+  const int per_group = G * e.z;
+  const int group = lt / per_group;
+  const int first_m = group * G;
+  const int gsize = min(e.y - first_m, G);
+  const int r = lt - group * per_group;
   tm = first_m + r % gsize;
   tn = r / gsize;
+}
+
+// Accumulator drain of one epilogue warp: its 32 rows (row0 .. row0+31, one
+// TMEM lane each) x the tile's BN columns, 32 columns at a time.
+//   1. each lane loads its row's 32 values (two tcgen05.ld, one wait), applies
+//      alpha and the column bias and writes them to the warp's 32 x 33 buffer;
+//   2. the warp writes the 32 rows back as contiguous segments -- f32: 8 lanes
+//      x 16 B per 128-byte row segment, 4 rows per store; bf16: 4 lanes x 16 B,
+//      8 rows per store -- adding beta * C, then ReLU, then converting.
+// Row-per-lane stores would put every lane of a store in a different row (32
+// half-sector writes per instruction); these write whole sectors. Warp-
+// collective: every lane runs it; rows at or past m and columns at or past n
+// are not written.
+template <int BN>
+__device__ __forceinline__ void tc_epi_rows(const TcProblem* pr, uint32_t t_row, int row0, int lane, float* stage,
+                                            int col_base) {
+  const int flags = pr->flags;
+  const float alpha = pr->alpha, beta = pr->beta;
+  const long long ldc = pr->ldc;
+  const int n = pr->n, m = pr->m;
+  const bool has_bias = (flags & EPI_BIAS) != 0;
+  const bool has_beta = (flags & EPI_BETA) != 0;
+  const bool relu = (flags & EPI_RELU) != 0;
+  float* srow = stage + lane * kTcEpiPitch;
+#pragma unroll 1
+  for (int c = 0; c < BN / 16; c += 2) {
+    const int col0 = col_base + c * 16;
+    if (col0 >= n) break;  // warp-uniform
+    uint32_t r0[16], r1[16];
+    tmem_ld16_nowait(t_row + c * 16, r0);
+    tmem_ld16_nowait(t_row + (c + 1) * 16, r1);
+    tmem_ld_wait();
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      float x0 = __uint_as_float(r0[i]) * alpha, x1 = __uint_as_float(r1[i]) * alpha;
+      if (has_bias) {
+        if (col0 + i < n) x0 += pr->bias[col0 + i];
+        if (col0 + 16 + i < n) x1 += pr->bias[col0 + 16 + i];
+      }
+      srow[i] = x0;
+      srow[16 + i] = x1;
+    }
+    __syncwarp();
+    if (flags & EPI_OUT_BF16) {
+      const int rr = lane >> 2, cc = (lane & 3) * 8;
+#pragma unroll 1
+      for (int sidx = 0; sidx < 4; ++sidx) {
+        const int r = sidx * 8 + rr, row = row0 + r, col = col0 + cc;
+        if (row >= m || col >= n) continue;
+        const float* sv = stage + r * kTcEpiPitch + cc;
+        __nv_bfloat16* cp = (__nv_bfloat16*)pr->c + (long long)row * ldc + col;
+        float v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = sv[q];
+        if (col + 8 <= n && ((((uintptr_t)cp) & 15) == 0)) {
+          if (has_beta) {
+            const uint4 o = *(const uint4*)cp;
+            const __nv_bfloat162* h = (const __nv_bfloat162*)&o;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const float2 f = __bfloat1622float2(h[q]);
+              v[2 * q] += beta * f.x;
+              v[2 * q + 1] += beta * f.y;
+            }
+          }
+          if (relu) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) v[q] = fmaxf(v[q], 0.f);
+          }
+          uint4 pk;
+          __nv_bfloat162* h = (__nv_bfloat162*)&pk;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) h[q] = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+          *(uint4*)cp = pk;
+        } else {
+          for (int q = 0; q < 8 && col + q < n; ++q) {
+            float x = v[q];
+            if (has_beta) x += beta * __bfloat162float(cp[q]);
+            if (relu) x = fmaxf(x, 0.f);
+            cp[q] = __float2bfloat16_rn(x);
+          }
+        }
+      }
+    } else {
+      const int rr = lane >> 3, cc = (lane & 7) * 4;
+#pragma unroll 1
+      for (int sidx = 0; sidx < 8; ++sidx) {
+        const int r = sidx * 4 + rr, row = row0 + r, col = col0 + cc;
+        if (row >= m || col >= n) continue;
+        const float* sv = stage + r * kTcEpiPitch + cc;
+        float* cp = (float*)pr->c + (long long)row * ldc + col;
+        float v[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) v[q] = sv[q];
+        if (col + 4 <= n && ((((uintptr_t)cp) & 15) == 0)) {
+          if (has_beta) {
+            const float4 o = *(const float4*)cp;
+            v[0] += beta * o.x; v[1] += beta * o.y; v[2] += beta * o.z; v[3] += beta * o.w;
+          }
+          if (relu) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) v[q] = fmaxf(v[q], 0.f);
+          }
+          *(float4*)cp = make_float4(v[0], v[1], v[2], v[3]);
+        } else {
+          for (int q = 0; q < 4 && col + q < n; ++q) {
+            float x = v[q];
+            if (has_beta) x += beta * cp[q];
+            if (relu) x = fmaxf(x, 0.f);
+            cp[q] = x;
+          }
+        }
+      }
+    }
+    __syncwarp();  // the buffer is rewritten by the next 32 columns
+  }
 }
 
 template <int BN, bool A_MN, bool B_MN, bool FP8>
@@ -116,10 +264,13 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
   uint64_t* tfull_bar = bars + 2 * C::STAGES;      // [2]
   uint64_t* tempty_bar = bars + 2 * C::STAGES + 2; // [2]
   uint32_t* tmem_slot = (uint32_t*)(bars + 2 * C::STAGES + 4);
+  int4* meta = (int4*)(smem + C::STAGES * C::STAGE_BYTES + 256);  // [kTcMetaMax]
   volatile uint32_t* status = args.status;
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
+  // epilogue warps 2..5: a 32 x kTcEpiPitch float buffer each, after the metadata
+  float* epi_stage = (float*)(meta + kTcMetaMax) + (warp >= 2 ? (warp - 2) * 32 * kTcEpiPitch : 0);
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < C::STAGES; ++s) {
@@ -132,6 +283,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     }
     fence_mbar_init();
   }
+  tc_stage_meta(args, meta);
   if (warp == 1) tmem_alloc(tmem_slot, C::TMEM_COLS);
   tc_fence_before();
   __syncthreads();
@@ -145,10 +297,19 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       uint32_t ph = 0;
       bool ok = true;
       for (int t = blockIdx.x; t < args.total_tiles && ok; t += gridDim.x) {
-        int p, tm, tn;
-        tc_locate(args, t, p, tm, tn);
+        int p, tm, tn, kdim;
+        tc_locate(args, meta, t, p, tm, tn, kdim);
         const TcProblem* pr = tc_problem(args, p);
-        const int kb_n = (pr->k + C::BK - 1) / C::BK;
+        if (args.table && t + (int)gridDim.x < args.total_tiles) {
+          // the next tile's tensor maps, if it starts a new problem
+          int p2, tm2, tn2, k2;
+          tc_locate(args, meta, t + gridDim.x, p2, tm2, tn2, k2);
+          if (p2 != p) {
+            prefetch_tensormap(&args.table[p2].tmap_a);
+            prefetch_tensormap(&args.table[p2].tmap_b);
+          }
+        }
+        const int kb_n = (kdim + C::BK - 1) / C::BK;
         for (int kb = 0; kb < kb_n; ++kb) {
           if (!mbar_wait(&empty_bar[s], ph ^ 1, status, DEV_TIMEOUT_EMPTY)) { ok = false; break; }
           uint8_t* sa = stage_base + s * C::STAGE_BYTES;
@@ -197,10 +358,9 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       uint32_t acc_ph = 0;
       bool ok = true;
       for (int t = blockIdx.x; t < args.total_tiles && ok; t += gridDim.x) {
-        int p, tm, tn;
-        tc_locate(args, t, p, tm, tn);
-        const TcProblem* pr = tc_problem(args, p);
-        const int kb_n = (pr->k + C::BK - 1) / C::BK;
+        int p, tm, tn, kdim;
+        tc_locate(args, meta, t, p, tm, tn, kdim);
+        const int kb_n = (kdim + C::BK - 1) / C::BK;
         if (!mbar_wait(&tempty_bar[acc], acc_ph ^ 1, status, DEV_TIMEOUT_TMEM_EMPTY)) break;
         tc_fence_after();
         const uint32_t d_tmem = tmem_base + acc * BN;
@@ -234,85 +394,15 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     int acc = 0;
     uint32_t acc_ph = 0;
     for (int t = blockIdx.x; t < args.total_tiles; t += gridDim.x) {
-      int p, tm, tn;
-      tc_locate(args, t, p, tm, tn);
+      int p, tm, tn, kdim;
+      tc_locate(args, meta, t, p, tm, tn, kdim);
       const TcProblem* pr = tc_problem(args, p);
       // Warp-uniform outcome: tcgen05.ld below is warp-collective.
       const bool got = mbar_wait(&tfull_bar[acc], acc_ph, status, DEV_TIMEOUT_TMEM_FULL);
       if (!__all_sync(0xffffffffu, got)) break;
       tc_fence_after();
-      const int row = tm * C::BM + lane_base + lane;
-      const bool row_ok = row < pr->m;
-      const int flags = pr->flags;
-      const float alpha = pr->alpha, beta = pr->beta;
-      const long long ldc = pr->ldc;
-      const int n = pr->n;
       const uint32_t t_row = tmem_base + acc * BN + ((uint32_t)lane_base << 16);
-      for (int c = 0; c < BN / 16; ++c) {
-        const int col0 = tn * BN + c * 16;
-        if (col0 >= n) break;  // warp-uniform
-        float v[16];
-        tmem_ld16(t_row + c * 16, v);
-        if (!row_ok) continue;
-        const bool full = (col0 + 16 <= n);
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          float x = v[i] * alpha;
-          if ((flags & EPI_BIAS) && (full || col0 + i < n)) x += pr->bias[col0 + i];
-          v[i] = x;
-        }
-        if (flags & EPI_OUT_BF16) {
-          __nv_bfloat16* cp = (__nv_bfloat16*)pr->c + (long long)row * ldc + col0;
-          if (flags & EPI_BETA) {
-#pragma unroll
-            for (int i = 0; i < 16; ++i)
-              if (full || col0 + i < n) v[i] += beta * __bfloat162float(cp[i]);
-          }
-          if (flags & EPI_RELU) {
-#pragma unroll
-            for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i], 0.f);
-          }
-          if (full && ((((uintptr_t)cp) & 15) == 0)) {
-            uint4 pk[2];
-            __nv_bfloat162* h = (__nv_bfloat162*)pk;
-#pragma unroll
-            for (int i = 0; i < 8; ++i) h[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
-            ((uint4*)cp)[0] = pk[0];
-            ((uint4*)cp)[1] = pk[1];
-          } else {
-            for (int i = 0; i < 16; ++i)
-              if (col0 + i < n) cp[i] = __float2bfloat16_rn(v[i]);
-          }
-        } else {
-          float* cp = (float*)pr->c + (long long)row * ldc + col0;
-          const bool vec = full && ((((uintptr_t)cp) & 15) == 0);
-          if (flags & EPI_BETA) {
-            if (vec) {
-#pragma unroll
-              for (int q = 0; q < 4; ++q) {
-                float4 o = ((const float4*)cp)[q];
-                v[4 * q + 0] += beta * o.x; v[4 * q + 1] += beta * o.y;
-                v[4 * q + 2] += beta * o.z; v[4 * q + 3] += beta * o.w;
-              }
-            } else {
-              for (int i = 0; i < 16; ++i)
-                if (col0 + i < n) v[i] += beta * cp[i];
-            }
-          }
-          if (flags & EPI_RELU) {
-#pragma unroll
-            for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i], 0.f);
-          }
-          if (vec) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-              ((float4*)cp)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-          } else {
-            for (int i = 0; i < 16; ++i)
-              if (col0 + i < n) cp[i] = v[i];
-          }
-        }
-      }
+      tc_epi_rows<BN>(pr, t_row, tm * C::BM + lane_base, lane, epi_stage, tn * BN);
       tc_fence_before();
       mbar_arrive(&tempty_bar[acc]);
       if (++acc == 2) { acc = 0; acc_ph ^= 1; }
@@ -351,7 +441,7 @@ struct Tc2Cfg {
   static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
   static constexpr int STAGES = 6;
   static constexpr int TMEM_COLS = 512;
-  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256 + kTcMetaBytes + kTcEpiBytes;
   static constexpr int THREADS = 192;
 };
 
@@ -368,10 +458,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
   uint64_t* tfull_bar = bars + 2 * C::STAGES;
   uint64_t* tempty_bar = bars + 2 * C::STAGES + 2;
   uint32_t* tmem_slot = (uint32_t*)(bars + 2 * C::STAGES + 4);
+  int4* meta = (int4*)(smem + C::STAGES * C::STAGE_BYTES + 256);  // [kTcMetaMax]
   volatile uint32_t* status = args.status;
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
+  // epilogue warps 2..5: a 32 x kTcEpiPitch float buffer each, after the metadata
+  float* epi_stage = (float*)(meta + kTcMetaMax) + (warp >= 2 ? (warp - 2) * 32 * kTcEpiPitch : 0);
   const uint32_t rank = cluster_ctarank();
   const bool leader = rank == 0;
   const int pair = blockIdx.x >> 1, num_pairs = gridDim.x >> 1;
@@ -387,6 +480,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
     }
     fence_mbar_init();
   }
+  tc_stage_meta(args, meta);
   if (warp == 1) tmem_alloc_2sm(tmem_slot, C::TMEM_COLS);
   tc_fence_before();
   __syncthreads();
@@ -402,10 +496,19 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
       uint32_t ph = 0;
       bool ok = true;
       for (int t = pair; t < args.total_tiles && ok; t += num_pairs) {
-        int p, tm, tn;
-        tc_locate(args, t, p, tm, tn);
+        int p, tm, tn, kdim;
+        tc_locate(args, meta, t, p, tm, tn, kdim);
         const TcProblem* pr = tc_problem(args, p);
-        const int kb_n = (pr->k + C::BK - 1) / C::BK;
+        if (args.table && t + num_pairs < args.total_tiles) {
+          // the next tile's tensor maps, if it starts a new problem
+          int p2, tm2, tn2, k2;
+          tc_locate(args, meta, t + num_pairs, p2, tm2, tn2, k2);
+          if (p2 != p) {
+            prefetch_tensormap(&args.table[p2].tmap_a);
+            prefetch_tensormap(&args.table[p2].tmap_b);
+          }
+        }
+        const int kb_n = (kdim + C::BK - 1) / C::BK;
         for (int kb = 0; kb < kb_n; ++kb) {
           if (!mbar_wait(&empty_bar[s], ph ^ 1, status, DEV_TIMEOUT_EMPTY)) { ok = false; break; }
           uint8_t* sa = stage_base + s * C::STAGE_BYTES;
@@ -449,10 +552,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
       uint32_t acc_ph = 0;
       bool ok = true;
       for (int t = pair; t < args.total_tiles && ok; t += num_pairs) {
-        int p, tm, tn;
-        tc_locate(args, t, p, tm, tn);
-        const TcProblem* pr = tc_problem(args, p);
-        const int kb_n = (pr->k + C::BK - 1) / C::BK;
+        int p, tm, tn, kdim;
+        tc_locate(args, meta, t, p, tm, tn, kdim);
+        const int kb_n = (kdim + C::BK - 1) / C::BK;
         if (!mbar_wait(&tempty_bar[acc], acc_ph ^ 1, status, DEV_TIMEOUT_TMEM_EMPTY)) break;
         tc_fence_after();
         const uint32_t d_tmem = tmem_base + acc * C::BN;
@@ -486,84 +588,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
     int acc = 0;
     uint32_t acc_ph = 0;
     for (int t = pair; t < args.total_tiles; t += num_pairs) {
-      int p, tm, tn;
-      tc_locate(args, t, p, tm, tn);
+      int p, tm, tn, kdim;
+      tc_locate(args, meta, t, p, tm, tn, kdim);
       const TcProblem* pr = tc_problem(args, p);
       const bool got = mbar_wait(&tfull_bar[acc], acc_ph, status, DEV_TIMEOUT_TMEM_FULL);
       if (!__all_sync(0xffffffffu, got)) break;
       tc_fence_after();
-      const int row = tm * C::BM + (int)rank * 128 + lane_base + lane;
-      const bool row_ok = row < pr->m;
-      const int flags = pr->flags;
-      const float alpha = pr->alpha, beta = pr->beta;
-      const long long ldc = pr->ldc;
-      const int n = pr->n;
       const uint32_t t_row = tmem_base + acc * C::BN + ((uint32_t)lane_base << 16);
-      for (int c = 0; c < C::BN / 16; ++c) {
-        const int col0 = tn * C::BN + c * 16;
-        if (col0 >= n) break;  // warp-uniform
-        float v[16];
-        tmem_ld16(t_row + c * 16, v);
-        if (!row_ok) continue;
-        const bool full = (col0 + 16 <= n);
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          float x = v[i] * alpha;
-          if ((flags & EPI_BIAS) && (full || col0 + i < n)) x += pr->bias[col0 + i];
-          v[i] = x;
-        }
-        if (flags & EPI_OUT_BF16) {
-          __nv_bfloat16* cp = (__nv_bfloat16*)pr->c + (long long)row * ldc + col0;
-          if (flags & EPI_BETA) {
-#pragma unroll
-            for (int i = 0; i < 16; ++i)
-              if (full || col0 + i < n) v[i] += beta * __bfloat162float(cp[i]);
-          }
-          if (flags & EPI_RELU) {
-#pragma unroll
-            for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i], 0.f);
-          }
-          if (full && ((((uintptr_t)cp) & 15) == 0)) {
-            uint4 pk[2];
-            __nv_bfloat162* h = (__nv_bfloat162*)pk;
-#pragma unroll
-            for (int i = 0; i < 8; ++i) h[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
-            ((uint4*)cp)[0] = pk[0];
-            ((uint4*)cp)[1] = pk[1];
-          } else {
-            for (int i = 0; i < 16; ++i)
-              if (col0 + i < n) cp[i] = __float2bfloat16_rn(v[i]);
-          }
-        } else {
-          float* cp = (float*)pr->c + (long long)row * ldc + col0;
-          const bool vec = full && ((((uintptr_t)cp) & 15) == 0);
-          if (flags & EPI_BETA) {
-            if (vec) {
-#pragma unroll
-              for (int q = 0; q < 4; ++q) {
-                float4 o = ((const float4*)cp)[q];
-                v[4 * q + 0] += beta * o.x; v[4 * q + 1] += beta * o.y;
-                v[4 * q + 2] += beta * o.z; v[4 * q + 3] += beta * o.w;
-              }
-            } else {
-              for (int i = 0; i < 16; ++i)
-                if (col0 + i < n) v[i] += beta * cp[i];
-            }
-          }
-          if (flags & EPI_RELU) {
-#pragma unroll
-            for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i], 0.f);
-          }
-          if (vec) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-              ((float4*)cp)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-          } else {
-            for (int i = 0; i < 16; ++i)
-              if (col0 + i < n) cp[i] = v[i];
-          }
-        }
-      }
+      tc_epi_rows<C::BN>(pr, t_row, tm * C::BM + (int)rank * 128 + lane_base, lane, epi_stage, tn * C::BN);
       tc_fence_before();
       mbar_arrive_cluster(acc == 0 ? tempty_leader0 : tempty_leader1);
       if (++acc == 2) { acc = 0; acc_ph ^= 1; }

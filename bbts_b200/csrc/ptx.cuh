@@ -68,13 +68,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 // Bounded wait for the phase with the given parity to complete. Returns false
 // (and records `code` in *status) if the clock budget runs out or another
 // thread has already flagged an error.
+// The shared status word lives in global memory and every waiting thread of
+// every CTA would poll the same address: it is read only every 256 failed
+// tries (a delay of microseconds before another thread's error is seen), so
+// the spin stays on chip; the clock budget is checked every try.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
                                           volatile uint32_t* status, uint32_t code) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
-  while (true) {
+  for (uint32_t it = 1;; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
-    if (*status != DEV_OK) return false;
+    if ((it & 255u) == 0 && *status != DEV_OK) return false;
     if (clock64() - t0 > kWaitBudgetCycles) {
       atomicCAS((unsigned int*)status, DEV_OK, code);
       return false;
@@ -151,6 +155,26 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
 }
 
 // Load 16 consecutive f32 columns of this thread's TMEM lane.
+// 16 columns of this warp's 32 TMEM lanes without waiting: issue several, then
+// one tmem_ld_wait() before the registers are read.
+__device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Brings a tensor map (in global memory) into the TMA unit's descriptor cache
+// ahead of its first use.
+__device__ __forceinline__ void prefetch_tensormap(const void* tmap) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(tmap) : "memory");
+}
+
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   uint32_t r[16];
   asm volatile(
