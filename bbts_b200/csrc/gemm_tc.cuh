@@ -66,8 +66,9 @@ struct TcArgs {
 constexpr int kTcMetaMax = 512;
 constexpr int kTcMetaBytes = kTcMetaMax * 16;
 // Epilogue staging: each of the 4 epilogue warps turns its 32 rows x 32
-// columns into contiguous row segments through a 32 x 33 float buffer.
-constexpr int kTcEpiPitch = 33;
+// columns into contiguous row segments through a 32 x 36 float buffer (the
+// 144-byte pitch keeps 16-byte accesses conflict-free in both directions).
+constexpr int kTcEpiPitch = 36;
 constexpr int kTcEpiBytes = 4 * 32 * kTcEpiPitch * 4;
 
 template <int BN, bool A_MN, bool B_MN, bool FP8>
@@ -138,7 +139,7 @@ __device__ __forceinline__ void tc_locate(const TcArgs& args, const int4* meta, 
 // Accumulator drain of one epilogue warp: its 32 rows (row0 .. row0+31, one
 // TMEM lane each) x the tile's BN columns, 32 columns at a time.
 //   1. each lane loads its row's 32 values (two tcgen05.ld, one wait), applies
-//      alpha and the column bias and writes them to the warp's 32 x 33 buffer;
+//      alpha and the column bias and writes them to the warp's 32 x 36 buffer;
 //   2. the warp writes the 32 rows back as contiguous segments -- f32: 8 lanes
 //      x 16 B per 128-byte row segment, 4 rows per store; bf16: 4 lanes x 16 B,
 //      8 rows per store -- adding beta * C, then ReLU, then converting.
@@ -165,28 +166,30 @@ __device__ __forceinline__ void tc_epi_rows(const TcProblem* pr, uint32_t t_row,
     tmem_ld16_nowait(t_row + c * 16, r0);
     tmem_ld16_nowait(t_row + (c + 1) * 16, r1);
     tmem_ld_wait();
+    float x[32];
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
-      float x0 = __uint_as_float(r0[i]) * alpha, x1 = __uint_as_float(r1[i]) * alpha;
-      if (has_bias) {
-        if (col0 + i < n) x0 += pr->bias[col0 + i];
-        if (col0 + 16 + i < n) x1 += pr->bias[col0 + 16 + i];
-      }
-      srow[i] = x0;
-      srow[16 + i] = x1;
+      x[i] = __uint_as_float(r0[i]) * alpha;
+      x[16 + i] = __uint_as_float(r1[i]) * alpha;
     }
+    if (has_bias) {
+#pragma unroll
+      for (int i = 0; i < 32; ++i)
+        if (col0 + i < n) x[i] += pr->bias[col0 + i];
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) *(float4*)(srow + 4 * j) = make_float4(x[4 * j], x[4 * j + 1], x[4 * j + 2], x[4 * j + 3]);
     __syncwarp();
     if (flags & EPI_OUT_BF16) {
       const int rr = lane >> 2, cc = (lane & 3) * 8;
-#pragma unroll 1
+#pragma unroll
       for (int sidx = 0; sidx < 4; ++sidx) {
         const int r = sidx * 8 + rr, row = row0 + r, col = col0 + cc;
         if (row >= m || col >= n) continue;
         const float* sv = stage + r * kTcEpiPitch + cc;
         __nv_bfloat16* cp = (__nv_bfloat16*)pr->c + (long long)row * ldc + col;
-        float v[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) v[q] = sv[q];
+        const float4 s0 = *(const float4*)sv, s1 = *(const float4*)(sv + 4);
+        float v[8] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
         if (col + 8 <= n && ((((uintptr_t)cp) & 15) == 0)) {
           if (has_beta) {
             const uint4 o = *(const uint4*)cp;
@@ -218,15 +221,14 @@ __device__ __forceinline__ void tc_epi_rows(const TcProblem* pr, uint32_t t_row,
       }
     } else {
       const int rr = lane >> 3, cc = (lane & 7) * 4;
-#pragma unroll 1
+#pragma unroll
       for (int sidx = 0; sidx < 8; ++sidx) {
         const int r = sidx * 4 + rr, row = row0 + r, col = col0 + cc;
         if (row >= m || col >= n) continue;
         const float* sv = stage + r * kTcEpiPitch + cc;
         float* cp = (float*)pr->c + (long long)row * ldc + col;
-        float v[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) v[q] = sv[q];
+        const float4 s0 = *(const float4*)sv;
+        float v[4] = {s0.x, s0.y, s0.z, s0.w};
         if (col + 4 <= n && ((((uintptr_t)cp) & 15) == 0)) {
           if (has_beta) {
             const float4 o = *(const float4*)cp;

@@ -549,9 +549,10 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
           gpre.writes.push_back(cs.lc);
           gpre.writes.push_back(cs.rc);
           void* C = L.direct ? d->tensors.at(n.outs[0]).payload : d->tensors.at(cs.ct).payload;
-          // A = Rc, B = Lc in their staging layouts: the problems join the
-          // group of matmuls with the same operand layouts
-          const int key = ELEM_BF16 * 4 + (L.rc_mn ? 2 : 0) + (L.lc_mn ? 0 : 1);
+          // A = Rc, B = Lc in their staging layouts. Contraction problems get
+          // groups of their own (key bit 8): they wait for the wave's gathers,
+          // while the matmul groups can start as soon as their inputs exist
+          const int key = 256 + ELEM_BF16 * 4 + (L.rc_mn ? 2 : 0) + (L.lc_mn ? 0 : 1);
           for (long long b = 0; b < L.nb; ++b) {
             const bbx::ContractionGemm g = bbx::contraction_gemm(L, tl.payload, tr.payload, C, b);
             bbx_tc_problem_t q{};
@@ -655,7 +656,7 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
     }
     for (auto& kv : tc_groups) {
       group_t g{G_TC, w};
-      const int dt = kv.first / 4;
+      const int dt = (kv.first & 0xff) / 4;
       // tile_n < 0: autotune per group; 0: size heuristic; 128 / 256: forced
       const int tn = tile_n < 0 ? autotune_tile_n(dt, (kv.first & 2) != 0, (kv.first & 1) != 0, kv.second) : tile_n;
       dag_bbx(bbx_tc_plan_create(dt == ELEM_E4M3 ? BBX_E4M3 : BBX_BF16, kv.second.data(), (int)kv.second.size(), tn,
