@@ -675,10 +675,22 @@ static int build_stream_table(const bbx_stream_op_t* ops, int count, std::vector
                               long long* total) {
   static_assert(kStreamMaxIn == BBX_STREAM_MAX_IN, "stream op fan-in mismatch");
   out->resize(count);
+  // Blocks stride over the chunk list (block b takes chunks b, b + grid, ...),
+  // and a chunk costs about (inputs + 1) x its bytes: ops go in descending
+  // fan-in, then size, so each round of `grid` chunks has similar cost. The ops
+  // of one launch are independent, so the order changes no result.
+  std::vector<int> order(count);
+  for (int i = 0; i < count; ++i) order[i] = i;
+  auto fan_in = [&](int i) { return ops[i].kind == S_SUM ? ops[i].n_in : (ops[i].kind == S_BINARY ? 2 : 1); };
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    if (fan_in(x) != fan_in(y)) return fan_in(x) > fan_in(y);
+    return ops[x].n > ops[y].n;
+  });
   long long chunks = 0;
-  for (int i = 0; i < count; ++i) {
+  for (int k = 0; k < count; ++k) {
+    const int i = order[k];
     const bbx_stream_op_t& q = ops[i];
-    StreamOp& o = (*out)[i];
+    StreamOp& o = (*out)[k];
     memset(&o, 0, sizeof(o));
     if (q.kind < S_SUM || q.kind > S_CAST) return set_error(BBX_ERR_INVALID, "stream op %d: kind %d", i, q.kind);
     const int need = q.kind == S_SUM ? q.n_in : (q.kind == S_BINARY ? 2 : 1);

@@ -332,7 +332,7 @@ namespace bbx {
 // [chunk_start, chunk_start + chunks) range contains it.
 enum StreamKind : int { S_SUM = 0, S_UNARY = 1, S_BINARY = 2, S_CAST = 3 };
 constexpr int kStreamMaxIn = 16;
-constexpr long long kStreamChunk = 8192;
+constexpr long long kStreamChunk = 16384;  // elements (measured: 4.3 TB/s on a DAG level vs 4.2 at 8192)
 
 struct StreamOp {
   int kind, op, in_dtype, out_dtype, n_in, kahan;
