@@ -66,24 +66,62 @@ __global__ void k_gather_sum(const float* __restrict__ in, void* out, int out_bf
 
 constexpr long long kGatherChunk = 4096;
 
-// Row path: the innermost output mode is unit-stride in both the source and
-// the destination and nothing is summed, so one warp copies a row with
-// coalesced accesses and the outer modes are decomposed once per row.
+// Row path: after merging, the innermost output mode is unit-stride in both the
+// source and the destination and nothing is summed. Work items are (row,
+// segment) pairs, a segment being up to kGatherSeg elements of one row, so
+// short rows and rows as long as a whole tensor both spread over warps. Each
+// warp carries kRowsPerWarp items at once, so every lane keeps that many
+// independent loads in flight.
+constexpr long long kGatherSeg = 1024;
+constexpr int kRowsPerWarp = 4;
+
 static bool row_mode_ok(const GatherArgs& a) {
   const int last = a.rank_o - 1;
   return a.rank_s == 0 && last >= 0 && a.istride[last] == 1 && a.ostride[last] == 1 && a.odims[last] >= 16;
 }
 
-// Each warp carries kRowsPerWarp rows at once, so every lane has that many
-// independent loads in flight (rows are short: a row-at-a-time warp holds a
-// single 128-byte load and cannot fill HBM). The first row's outer index is
-// decomposed once; the following rows step it with a carry.
-constexpr int kRowsPerWarp = 4;
+void simplify_gather(GatherArgs* a) {
+  if (a->rank_o <= 1) return;
+  long long od[4], is[4], os[4];  // fastest first
+  int r = 1;
+  od[0] = a->odims[a->rank_o - 1];
+  is[0] = a->istride[a->rank_o - 1];
+  os[0] = a->ostride[a->rank_o - 1];
+  for (int d = a->rank_o - 2; d >= 0; --d) {
+    if (a->istride[d] == is[r - 1] * od[r - 1] && a->ostride[d] == os[r - 1] * od[r - 1]) {
+      od[r - 1] *= a->odims[d];  // (i_d, i_f) -> i_d * n_f + i_f on both sides
+    } else {
+      od[r] = a->odims[d];
+      is[r] = a->istride[d];
+      os[r] = a->ostride[d];
+      ++r;
+    }
+  }
+  a->rank_o = r;
+  for (int q = 0; q < r; ++q) {
+    a->odims[q] = od[r - 1 - q];
+    a->istride[q] = is[r - 1 - q];
+    a->ostride[q] = os[r - 1 - q];
+  }
+}
 
-__device__ __forceinline__ void gather_rows(const GatherRec& rec, long long row0, long long row1) {
+static void set_row_mode(GatherRec* r) {
+  r->row_mode = row_mode_ok(r->a) ? 1 : 0;
+  if (!r->row_mode) {
+    r->row_len = r->segs = r->items_per_chunk = 0;
+    return;
+  }
+  r->row_len = r->a.odims[r->a.rank_o - 1];
+  r->segs = (r->row_len + kGatherSeg - 1) / kGatherSeg;
+  r->items_per_chunk = std::max<long long>(32, 4 * kGatherChunk / std::min(r->row_len, kGatherSeg));
+}
+
+static long long row_items(const GatherRec& r) { return (r.n / r.row_len) * r.segs; }
+
+__device__ __forceinline__ void gather_rows(const GatherRec& rec, long long item0, long long item1) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   // the record's fields in registers: stores to the destination could alias
-  // the record as far as the compiler knows, which would reload it every row
+  // the record as far as the compiler knows, which would reload it every item
   const int outer = rec.a.rank_o - 1;  // dims 0 .. outer-1 index rows, dim `outer` runs along a row
   long long odims[3], istr[3], ostr[3];
 #pragma unroll
@@ -95,42 +133,51 @@ __device__ __forceinline__ void gather_rows(const GatherRec& rec, long long row0
   const float* __restrict__ src = rec.src;
   void* const dst = rec.dst;
   const bool bf16 = rec.dst_bf16 != 0;
-  const int row_len = (int)rec.row_len;
-  for (long long row = row0 + (long long)warp * kRowsPerWarp; row < row1; row += (long long)nwarps * kRowsPerWarp) {
-    long long idx[3] = {0, 0, 0};
-    long long rem = row;
-#pragma unroll
-    for (int d = 2; d >= 0; --d) {
-      if (d < outer) {
-        idx[d] = rem % odims[d];
-        rem /= odims[d];
-      }
-    }
+  const long long row_len = rec.row_len, segs = rec.segs;
+  for (long long it = item0 + (long long)warp * kRowsPerWarp; it < item1; it += (long long)nwarps * kRowsPerWarp) {
     long long so[kRowsPerWarp], dso[kRowsPerWarp];
-    int nr = 0;
+    int len[kRowsPerWarp];
+    int maxlen = 0;
 #pragma unroll
     for (int u = 0; u < kRowsPerWarp; ++u) {
-      so[u] = idx[0] * istr[0] + idx[1] * istr[1] + idx[2] * istr[2];
-      dso[u] = idx[0] * ostr[0] + idx[1] * ostr[1] + idx[2] * ostr[2];
-      if (row + u < row1) nr = u + 1;
+      so[u] = dso[u] = 0;
+      len[u] = 0;
+      const long long item = it + u;
+      if (item < item1) {
+        const long long row = item / segs, start = (item - row * segs) * kGatherSeg;
+        long long rem = row, s = start, t = start;
 #pragma unroll
-      for (int d = 2; d >= 0; --d) {  // next row: the last outer dim is fastest
-        if (d < outer) {
-          if (++idx[d] < odims[d]) break;
-          idx[d] = 0;
+        for (int d = 2; d >= 0; --d) {
+          if (d < outer) {
+            const long long idx = rem % odims[d];
+            rem /= odims[d];
+            s += idx * istr[d];
+            t += idx * ostr[d];
+          }
         }
+        so[u] = s;
+        dso[u] = t;
+        len[u] = (int)min(kGatherSeg, row_len - start);
+        maxlen = max(maxlen, len[u]);
       }
     }
-    for (int x = lane; x < row_len; x += 32) {
-      float v[kRowsPerWarp];
+    // four 32-element steps per pass: 16 independent loads per lane in flight
+    for (int x0 = lane; x0 < maxlen; x0 += 128) {
+      float v[kRowsPerWarp][4];
 #pragma unroll
       for (int u = 0; u < kRowsPerWarp; ++u)
-        if (u < nr) v[u] = __ldg(src + so[u] + x);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (x0 + 32 * q < len[u]) v[u][q] = __ldg(src + so[u] + x0 + 32 * q);
 #pragma unroll
       for (int u = 0; u < kRowsPerWarp; ++u) {
-        if (u < nr) {
-          if (bf16) ((__nv_bfloat16*)dst)[dso[u] + x] = __float2bfloat16_rn(v[u]);
-          else ((float*)dst)[dso[u] + x] = v[u];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int x = x0 + 32 * q;
+          if (x < len[u]) {
+            if (bf16) ((__nv_bfloat16*)dst)[dso[u] + x] = __float2bfloat16_rn(v[u][q]);
+            else ((float*)dst)[dso[u] + x] = v[u][q];
+          }
         }
       }
     }
@@ -139,10 +186,10 @@ __device__ __forceinline__ void gather_rows(const GatherRec& rec, long long row0
 
 // One gather record on the row path (the per-call contraction).
 __global__ void k_gather_rows1(const __grid_constant__ GatherRec r, long long chunks) {
-  const long long rows = r.n / r.row_len;
+  const long long items = (r.n / r.row_len) * r.segs;
   for (long long c = blockIdx.x; c < chunks; c += gridDim.x) {
-    const long long row0 = c * r.rows_per_chunk;
-    gather_rows(r, row0, min(row0 + r.rows_per_chunk, rows));
+    const long long i0 = c * r.items_per_chunk;
+    gather_rows(r, i0, min(i0 + r.items_per_chunk, items));
   }
 }
 
@@ -157,8 +204,8 @@ __global__ void k_gather_group(const GatherRec* __restrict__ recs, int count, lo
     }
     const GatherRec& r = recs[lo];
     if (r.row_mode) {
-      const long long row0 = (c - r.chunk_start) * r.rows_per_chunk;
-      gather_rows(r, row0, min(row0 + r.rows_per_chunk, r.n / r.row_len));
+      const long long i0 = (c - r.chunk_start) * r.items_per_chunk;
+      gather_rows(r, i0, min(i0 + r.items_per_chunk, (r.n / r.row_len) * r.segs));
       continue;
     }
     const long long e0 = (c - r.chunk_start) * kGatherChunk;
@@ -167,8 +214,11 @@ __global__ void k_gather_group(const GatherRec* __restrict__ recs, int count, lo
   }
 }
 
-static int launch_gather(const float* in, void* out, bool bf16, const GatherArgs& a, long long n, cudaStream_t st) {
+static int launch_gather(const float* in, void* out, bool bf16, const GatherArgs& args, long long n,
+                         cudaStream_t st) {
   if (n == 0) return BBX_OK;
+  GatherArgs a = args;
+  simplify_gather(&a);
   if (row_mode_ok(a)) {
     GatherRec r{};  // travels by value in the kernel parameters
     r.a = a;
@@ -176,10 +226,8 @@ static int launch_gather(const float* in, void* out, bool bf16, const GatherArgs
     r.dst = out;
     r.dst_bf16 = bf16 ? 1 : 0;
     r.n = n;
-    r.row_mode = 1;
-    r.row_len = a.odims[a.rank_o - 1];
-    r.rows_per_chunk = std::max<long long>(32, 2 * kGatherChunk / r.row_len);
-    const long long chunks = (n / r.row_len + r.rows_per_chunk - 1) / r.rows_per_chunk;
+    set_row_mode(&r);
+    const long long chunks = (row_items(r) + r.items_per_chunk - 1) / r.items_per_chunk;
     k_gather_rows1<<<(int)std::min<long long>(chunks, 148 * 8), 256, 0, st>>>(r, chunks);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_error(BBX_ERR_CUDA, "k_gather_rows1: %s", cudaGetErrorString(e));
@@ -372,17 +420,11 @@ int gather_plan_create(const GatherRec* recs, int count, GatherPlan** out) {
   std::vector<GatherRec> h(recs, recs + count);
   long long chunks = 0;
   for (auto& r : h) {
-    r.row_mode = row_mode_ok(r.a) ? 1 : 0;
+    simplify_gather(&r.a);
+    set_row_mode(&r);
     r.chunk_start = chunks;
-    if (r.row_mode) {
-      r.row_len = r.a.odims[r.a.rank_o - 1];
-      r.rows_per_chunk = std::max<long long>(32, 2 * kGatherChunk / r.row_len);
-      chunks += (r.n / r.row_len + r.rows_per_chunk - 1) / r.rows_per_chunk;
-    } else {
-      r.row_len = 0;
-      r.rows_per_chunk = 0;
-      chunks += (r.n + kGatherChunk - 1) / kGatherChunk;
-    }
+    if (r.row_mode) chunks += (row_items(r) + r.items_per_chunk - 1) / r.items_per_chunk;
+    else chunks += (r.n + kGatherChunk - 1) / kGatherChunk;
   }
   auto* p = new GatherPlan();
   p->count = count;

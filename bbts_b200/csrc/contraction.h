@@ -58,9 +58,14 @@ struct GatherRec {
   int row_mode;            // set by gather_plan_create: innermost mode contiguous on both sides
   long long n;
   long long chunk_start;   // set by gather_plan_create
-  long long row_len;       // row mode: elements per row (the innermost extent)
-  long long rows_per_chunk;
+  long long row_len;       // row mode: elements per row (the innermost extent, after merging)
+  long long segs;          // row mode: segments of kGatherSeg elements per row
+  long long items_per_chunk;  // row mode: (row, segment) items per chunk
 };
+
+// Merges adjacent output modes that are contiguous in both the source and the
+// destination (a padded or permuted copy then runs as long rows).
+void simplify_gather(GatherArgs* a);
 
 struct GatherPlan;
 int gather_plan_create(const GatherRec* recs, int count, GatherPlan** out);
