@@ -157,9 +157,10 @@ static int make_map(CUtensorMap* map, const void* base, int dtype, long long row
   EncodeTiledFn enc;
   int rc = get_encode_fn(&enc);
   if (rc) return rc;
-  const int esz = dtype == BBX_E4M3 ? 1 : 2;
-  CUtensorMapDataType dt =
-      dtype == BBX_E4M3 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+  const int esz = dtype == BBX_E4M3 ? 1 : dtype == BBX_F32 ? 4 : 2;
+  CUtensorMapDataType dt = dtype == BBX_E4M3  ? CU_TENSOR_MAP_DATA_TYPE_UINT8
+                           : dtype == BBX_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                              : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
   cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
   cuuint64_t strides[1] = {(cuuint64_t)(ld * esz)};
   cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
@@ -257,6 +258,15 @@ static int build_problem(int in_dtype, const bbx_tc_problem_t& q, int bn_code, T
   out->alpha = q.alpha;
   out->beta = q.beta;
   out->flags = q.flags & (EPI_RELU | EPI_OUT_BF16 | EPI_BIAS | EPI_BETA);
+  // C through TMA stores when its base and pitch meet the 16-byte rules and the
+  // epilogue does not read C: 32-row boxes of 128 bytes (32 f32 / 64 bf16)
+  const bool c_bf16 = (out->flags & EPI_OUT_BF16) != 0;
+  const int c_esz = c_bf16 ? 2 : 4;
+  if (!(out->flags & EPI_BETA) && (((uintptr_t)q.c) & 15) == 0 && ((q.ldc * c_esz) & 15) == 0) {
+    rc = make_map(&out->tmap_c, q.c, c_bf16 ? BBX_BF16 : BBX_F32, q.m, q.n, q.ldc, 128 / c_esz, 32);
+    if (rc) return rc;
+    out->flags |= EPI_TMA_STORE;
+  }
   return BBX_OK;
 }
 

@@ -33,12 +33,14 @@ enum : int {
   EPI_OUT_BF16 = 2,  // store bf16 instead of f32
   EPI_BIAS = 4,      // add bias[col]
   EPI_BETA = 8,      // read C and add beta * C
+  EPI_TMA_STORE = 16,  // set by the host: C is written by TMA stores through tmap_c
 };
 
 // One block product. 64-byte alignment is required by the tensor maps.
 struct alignas(64) TcProblem {
   CUtensorMap tmap_a;  // 128 B
   CUtensorMap tmap_b;  // 128 B
+  CUtensorMap tmap_c;  // 128 B, valid with EPI_TMA_STORE: 32-row x 128-byte boxes, 128-byte swizzle
   void* c;
   const float* bias;
   long long ldc;       // elements
@@ -65,11 +67,14 @@ struct TcArgs {
 // is an on-chip binary search instead of a chain of dependent global loads.
 constexpr int kTcMetaMax = 512;
 constexpr int kTcMetaBytes = kTcMetaMax * 16;
-// Epilogue staging: each of the 4 epilogue warps turns its 32 rows x 32
-// columns into contiguous row segments through a 32 x 36 float buffer (the
-// 144-byte pitch keeps 16-byte accesses conflict-free in both directions).
+// Epilogue slots, one per epilogue warp, 1024-byte aligned: either a 32 x 36
+// float staging buffer (the 144-byte pitch keeps 16-byte accesses conflict-free
+// in both directions) or a 32-row x 128-byte box for a TMA store, laid out with
+// the 128-byte swizzle.
 constexpr int kTcEpiPitch = 36;
-constexpr int kTcEpiBytes = 4 * 32 * kTcEpiPitch * 4;
+constexpr int kTcEpiSlot = 5120;
+constexpr int kTcEpiBytes = 4 * kTcEpiSlot;
+static_assert(32 * kTcEpiPitch * 4 <= kTcEpiSlot && 32 * 128 <= kTcEpiSlot && kTcEpiSlot % 1024 == 0, "epilogue slot");
 
 template <int BN, bool A_MN, bool B_MN, bool FP8>
 struct TcCfg {
@@ -84,7 +89,7 @@ struct TcCfg {
   static constexpr int STAGES = (BN == 256) ? 4 : 6;
   static constexpr int TMEM_COLS = 2 * BN;            // double-buffered accumulator
   static constexpr int SMEM_BYTES =
-      STAGES * STAGE_BYTES + 1024 /*align slack*/ + 256 /*bars*/ + kTcMetaBytes + kTcEpiBytes;
+      STAGES * STAGE_BYTES + 1024 /*align slack*/ + kTcEpiBytes + 256 /*bars*/ + kTcMetaBytes;
   static constexpr int THREADS = 192;
   static constexpr int MN_BOX = 128 / ELEM;           // MN-major TMA box width (elements)
 };
@@ -158,6 +163,10 @@ __device__ __forceinline__ void tc_epi_rows(const TcProblem* pr, uint32_t t_row,
   const bool has_beta = (flags & EPI_BETA) != 0;
   const bool relu = (flags & EPI_RELU) != 0;
   float* srow = stage + lane * kTcEpiPitch;
+  // the buffer shares its slot with the TMA-store box of earlier tiles (a group
+  // can mix problems with and without TMA stores): let those stores read it first
+  if (lane == 0) bulk_wait_read_all();
+  __syncwarp();
 #pragma unroll 1
   for (int c = 0; c < BN / 16; c += 2) {
     const int col0 = col_base + c * 16;
@@ -253,6 +262,98 @@ __device__ __forceinline__ void tc_epi_rows(const TcProblem* pr, uint32_t t_row,
   }
 }
 
+// Accumulator drain through TMA stores (problems with EPI_TMA_STORE: C's base
+// and pitch meet the 16-byte rules, no beta * C). Per 128 bytes of each of the
+// warp's 32 rows (32 f32 or 64 bf16 columns): the lane of row r loads its
+// values from TMEM, applies alpha, bias and ReLU, converts, and writes its 128
+// bytes into the warp's box with the 128-byte swizzle (16-byte chunk j of row r
+// at chunk j ^ (r & 7): conflict-free); one lane then issues the TMA store of
+// the 32 x 128-byte box, which clips rows >= m and columns >= n. The box is
+// rewritten only after the previous store has read it.
+template <int BN>
+__device__ __forceinline__ void tc_epi_rows_tma(const TcProblem* pr, uint32_t t_row, int row0, int lane,
+                                                uint8_t* box, int col_base) {
+  const int flags = pr->flags;
+  const float alpha = pr->alpha;
+  const int n = pr->n;
+  const bool has_bias = (flags & EPI_BIAS) != 0;
+  const bool relu = (flags & EPI_RELU) != 0;
+  const bool bf16 = (flags & EPI_OUT_BF16) != 0;
+  const int step = bf16 ? 64 : 32;  // columns per 128-byte row of the box
+  uint8_t* myrow = box + lane * 128;
+  if (row0 >= pr->m) return;  // warp-uniform: this warp's rows are all past the matrix, no box to store
+#pragma unroll 1
+  for (int c0 = 0; c0 < BN; c0 += step) {
+    const int col = col_base + c0;
+    if (col >= n) break;  // warp-uniform
+    uint32_t r0[16], r1[16], r2[16], r3[16];
+    tmem_ld16_nowait(t_row + c0, r0);
+    tmem_ld16_nowait(t_row + c0 + 16, r1);
+    if (bf16) {
+      tmem_ld16_nowait(t_row + c0 + 32, r2);
+      tmem_ld16_nowait(t_row + c0 + 48, r3);
+    }
+    tmem_ld_wait();
+    uint4 q[8];
+    if (bf16) {
+      float v[64];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        v[i] = __uint_as_float(r0[i]) * alpha;
+        v[16 + i] = __uint_as_float(r1[i]) * alpha;
+        v[32 + i] = __uint_as_float(r2[i]) * alpha;
+        v[48 + i] = __uint_as_float(r3[i]) * alpha;
+      }
+      if (has_bias) {
+#pragma unroll
+        for (int i = 0; i < 64; ++i)
+          if (col + i < n) v[i] += pr->bias[col + i];
+      }
+      if (relu) {
+#pragma unroll
+        for (int i = 0; i < 64; ++i) v[i] = fmaxf(v[i], 0.f);
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        __nv_bfloat162 h[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) h[t] = __floats2bfloat162_rn(v[8 * j + 2 * t], v[8 * j + 2 * t + 1]);
+        q[j] = make_uint4(*(uint32_t*)&h[0], *(uint32_t*)&h[1], *(uint32_t*)&h[2], *(uint32_t*)&h[3]);
+      }
+    } else {
+      float v[32];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        v[i] = __uint_as_float(r0[i]) * alpha;
+        v[16 + i] = __uint_as_float(r1[i]) * alpha;
+      }
+      if (has_bias) {
+#pragma unroll
+        for (int i = 0; i < 32; ++i)
+          if (col + i < n) v[i] += pr->bias[col + i];
+      }
+      if (relu) {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) v[i] = fmaxf(v[i], 0.f);
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        q[j] = make_uint4(__float_as_uint(v[4 * j]), __float_as_uint(v[4 * j + 1]), __float_as_uint(v[4 * j + 2]),
+                          __float_as_uint(v[4 * j + 3]));
+    }
+    if (lane == 0) bulk_wait_read_all();  // the previous store has read the box
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 8; ++j) *(uint4*)(myrow + ((j ^ (lane & 7)) << 4)) = q[j];
+    fence_proxy_async_smem();
+    __syncwarp();
+    if (lane == 0) {
+      tma_store_2d(&pr->tmap_c, box, col, row0);
+      bulk_commit();
+    }
+  }
+}
+
 template <int BN, bool A_MN, bool B_MN, bool FP8>
 __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__ TcArgs args) {
   using C = TcCfg<BN, A_MN, B_MN, FP8>;
@@ -260,19 +361,21 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
   // 1024-byte alignment for the 128B-swizzle atoms.
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t* stage_base = smem;
-  uint64_t* bars = (uint64_t*)(smem + C::STAGES * C::STAGE_BYTES);
+  uint8_t* epi_base = smem + C::STAGES * C::STAGE_BYTES;  // 4 epilogue slots, 1024-byte aligned
+  uint64_t* bars = (uint64_t*)(epi_base + kTcEpiBytes);
   uint64_t* full_bar = bars;                       // [STAGES]
   uint64_t* empty_bar = bars + C::STAGES;          // [STAGES]
   uint64_t* tfull_bar = bars + 2 * C::STAGES;      // [2]
   uint64_t* tempty_bar = bars + 2 * C::STAGES + 2; // [2]
   uint32_t* tmem_slot = (uint32_t*)(bars + 2 * C::STAGES + 4);
-  int4* meta = (int4*)(smem + C::STAGES * C::STAGE_BYTES + 256);  // [kTcMetaMax]
+  int4* meta = (int4*)((uint8_t*)bars + 256);  // [kTcMetaMax]
   volatile uint32_t* status = args.status;
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  // epilogue warps 2..5: a 32 x kTcEpiPitch float buffer each, after the metadata
-  float* epi_stage = (float*)(meta + kTcMetaMax) + (warp >= 2 ? (warp - 2) * 32 * kTcEpiPitch : 0);
+  // epilogue warps 2..5: one slot each (staging buffer or TMA-store box)
+  uint8_t* epi_buf = epi_base + (warp >= 2 ? (warp - 2) * kTcEpiSlot : 0);
+  float* epi_stage = (float*)epi_buf;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < C::STAGES; ++s) {
@@ -404,11 +507,13 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       if (!__all_sync(0xffffffffu, got)) break;
       tc_fence_after();
       const uint32_t t_row = tmem_base + acc * BN + ((uint32_t)lane_base << 16);
-      tc_epi_rows<BN>(pr, t_row, tm * C::BM + lane_base, lane, epi_stage, tn * BN);
+      if (pr->flags & EPI_TMA_STORE) tc_epi_rows_tma<BN>(pr, t_row, tm * C::BM + lane_base, lane, epi_buf, tn * BN);
+      else tc_epi_rows<BN>(pr, t_row, tm * C::BM + lane_base, lane, epi_stage, tn * BN);
       tc_fence_before();
       mbar_arrive(&tempty_bar[acc]);
       if (++acc == 2) { acc = 0; acc_ph ^= 1; }
     }
+    if (lane == 0) bulk_wait_all();  // this warp's TMA stores have landed before the CTA ends
   }
 
   tc_fence_before();
@@ -454,19 +559,21 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t* stage_base = smem;
-  uint64_t* bars = (uint64_t*)(smem + C::STAGES * C::STAGE_BYTES);
+  uint8_t* epi_base = smem + C::STAGES * C::STAGE_BYTES;  // 4 epilogue slots, 1024-byte aligned
+  uint64_t* bars = (uint64_t*)(epi_base + kTcEpiBytes);
   uint64_t* full_bar = bars;
   uint64_t* empty_bar = bars + C::STAGES;
   uint64_t* tfull_bar = bars + 2 * C::STAGES;
   uint64_t* tempty_bar = bars + 2 * C::STAGES + 2;
   uint32_t* tmem_slot = (uint32_t*)(bars + 2 * C::STAGES + 4);
-  int4* meta = (int4*)(smem + C::STAGES * C::STAGE_BYTES + 256);  // [kTcMetaMax]
+  int4* meta = (int4*)((uint8_t*)bars + 256);  // [kTcMetaMax]
   volatile uint32_t* status = args.status;
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  // epilogue warps 2..5: a 32 x kTcEpiPitch float buffer each, after the metadata
-  float* epi_stage = (float*)(meta + kTcMetaMax) + (warp >= 2 ? (warp - 2) * 32 * kTcEpiPitch : 0);
+  // epilogue warps 2..5: one slot each (staging buffer or TMA-store box)
+  uint8_t* epi_buf = epi_base + (warp >= 2 ? (warp - 2) * kTcEpiSlot : 0);
+  float* epi_stage = (float*)epi_buf;
   const uint32_t rank = cluster_ctarank();
   const bool leader = rank == 0;
   const int pair = blockIdx.x >> 1, num_pairs = gridDim.x >> 1;
@@ -597,11 +704,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
       if (!__all_sync(0xffffffffu, got)) break;
       tc_fence_after();
       const uint32_t t_row = tmem_base + acc * C::BN + ((uint32_t)lane_base << 16);
-      tc_epi_rows<C::BN>(pr, t_row, tm * C::BM + (int)rank * 128 + lane_base, lane, epi_stage, tn * C::BN);
+      const int row0 = tm * C::BM + (int)rank * 128 + lane_base;
+      if (pr->flags & EPI_TMA_STORE) tc_epi_rows_tma<C::BN>(pr, t_row, row0, lane, epi_buf, tn * C::BN);
+      else tc_epi_rows<C::BN>(pr, t_row, row0, lane, epi_stage, tn * C::BN);
       tc_fence_before();
       mbar_arrive_cluster(acc == 0 ? tempty_leader0 : tempty_leader1);
       if (++acc == 2) { acc = 0; acc_ph ^= 1; }
     }
+    if (lane == 0) bulk_wait_all();  // this warp's TMA stores have landed before the CTA ends
   }
 
   // the leader's MMAs read the peer's shared memory: neither CTA may release

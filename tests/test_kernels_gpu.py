@@ -449,3 +449,33 @@ def test_matmul_tc_2sm_grouped_epilogues(T):
     for o, r in zip(outs, refs):
         assert rel_err(host(o), r) <= 1e-5
     plan.close()
+
+
+@pytest.mark.parametrize("tile_n", [256, 512])
+def test_matmul_tc_mixed_store_paths(T, tile_n):
+    """One group alternating outputs that are written by TMA stores (f32, pitch
+    512 x 4 B) and outputs that are not (pitch 510 x 4 B is not a multiple of 16
+    bytes): every CTA runs tiles of both kinds back to back through the same
+    shared-memory slot, over three launches."""
+    torch, ops = T
+    rng = np.random.default_rng(31)
+    probs, keep, refs = [], [], []
+    for i in range(48):
+        m, k = 256 + 64 * (i % 3), 128 + 64 * (i % 4)
+        n = 512 if i % 2 == 0 else 510
+        a = bf16_round(rng.standard_normal((m, k)))
+        b = bf16_round(rng.standard_normal((k, n)))
+        A = dev(torch, a, torch.bfloat16)
+        B = torch.zeros(k, 512, dtype=torch.bfloat16, device="cuda")  # operand pitch stays 16-byte aligned
+        B[:, :n] = dev(torch, b, torch.bfloat16)
+        B = B[:, :n]
+        c = torch.full((m, n), float("nan"), device="cuda")  # C pitch n: 2048 B or 2040 B
+        keep += [A, B, c]
+        probs.append(ops.tc_problem(A, B, c))
+        refs.append(oracle.matmul_f64(a, b))
+    plan = ops.TcPlan(probs, tile_n=tile_n)
+    for _ in range(3):
+        plan.launch()
+        for i, ref in enumerate(refs):
+            assert rel_err(host(keep[3 * i + 2]), ref) <= 1e-5, i
+    plan.close()
