@@ -65,6 +65,7 @@ SIGNATURES = {
     "bbx_stream_plan_create": (i32, [vp, i32, C.POINTER(vp)]),
     "bbx_stream_plan_launch": (i32, [vp, vp]),
     "bbx_stream_plan_destroy": (i32, [vp]),
+    "bbx_stream_plan_bulk": (i32, [vp]),
     # runtime
     "bbx_rt_create": (i32, [C.POINTER(vp)]),
     "bbx_rt_destroy": (i32, [vp]),
@@ -90,6 +91,8 @@ SIGNATURES = {
     "bbx_rt_run": (i32, [vp, i32]),
     "bbx_rt_record": (i32, [vp, i32, vp, vp, vp, i32, C.POINTER(i32)]),
     "bbx_rt_set_workers": (i32, [vp, i32]),
+    "bbx_rt_set_storage_budget": (i32, [vp, C.c_ulonglong, C.c_ulonglong, C.c_char_p]),
+    "bbx_rt_spill_stats": (i32, [vp, C.POINTER(C.c_ulonglong), i32]),
     "bbx_rt_set_hint_predictor": (i32, [vp, C.c_double, C.c_double]),
     "bbx_dag_build": (i32, [vp, i32, i32, C.POINTER(vp)]),
     "bbx_dag_launch": (i32, [vp, vp]),

@@ -96,6 +96,9 @@ static int init_tc_attributes() {
   rc |= set_tc_attr<128, true, false, true>();   rc |= set_tc_attr<128, true, true, true>();
   rc |= set_tc2_attr<false, false>(); rc |= set_tc2_attr<false, true>();
   rc |= set_tc2_attr<true, false>();  rc |= set_tc2_attr<true, true>();
+  for (auto f : {(const void*)k_stream_bulk<false>, (const void*)k_stream_bulk<true>,
+                 (const void*)k_stream_bulk_inline<false>, (const void*)k_stream_bulk_inline<true>})
+    rc |= cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kBulkSmem) != cudaSuccess;
   return rc ? BBX_ERR_CUDA : BBX_OK;
 }
 
@@ -677,12 +680,16 @@ int bbx_permute(const float* in, int rank, const long long* in_dims, const int* 
 struct bbx_stream_plan {
   StreamOp* d_table = nullptr;
   int count = 0;
-  long long total_chunks = 0;
+  long long total_chunks = 0;  // items when bulk
+  bool bulk = false;
 };
 
 namespace bbx {
+// *bulk: every op qualifies for the bulk-staged kernel (all pointers 16-byte
+// aligned); the table then counts items of bulk_tile elements instead of
+// kStreamChunk chunks.
 static int build_stream_table(const bbx_stream_op_t* ops, int count, std::vector<StreamOp>* out,
-                              long long* total) {
+                              long long* total, bool* bulk) {
   static_assert(kStreamMaxIn == BBX_STREAM_MAX_IN, "stream op fan-in mismatch");
   out->resize(count);
   // Blocks stride over the chunk list (block b takes chunks b, b + grid, ...),
@@ -724,6 +731,18 @@ static int build_stream_table(const bbx_stream_op_t* ops, int count, std::vector
     chunks += (q.n + kStreamChunk - 1) / kStreamChunk;
   }
   *total = chunks;
+  bool all16 = true;
+  for (const StreamOp& o : *out) all16 = all16 && (o.n == 0 || o.vec == 2);
+  *bulk = all16;
+  if (all16) {
+    long long items = 0;
+    for (StreamOp& o : *out) {
+      o.tile = bulk_tile(o.n_in, o.in_dtype == BBX_BF16 ? 2 : 4, o.out_dtype == BBX_BF16 ? 2 : 4);
+      o.chunk_start = items;
+      items += (o.n + o.tile - 1) / o.tile;
+    }
+    *total = items;
+  }
   return BBX_OK;
 }
 }  // namespace bbx
@@ -734,11 +753,13 @@ int bbx_stream_plan_create(const bbx_stream_op_t* ops, int count, bbx_stream_pla
   if (!ops || count <= 0 || !out) return set_error(BBX_ERR_INVALID, "bad stream plan arguments");
   std::vector<StreamOp> table;
   long long total = 0;
-  int rc = build_stream_table(ops, count, &table, &total);
+  bool bulk = false;
+  int rc = build_stream_table(ops, count, &table, &total, &bulk);
   if (rc) return rc;
   auto* p = new bbx_stream_plan();
   p->count = count;
   p->total_chunks = total;
+  p->bulk = bulk;
   cudaError_t e = cudaMalloc(&p->d_table, sizeof(StreamOp) * count);
   if (e == cudaSuccess) e = cudaMemcpy(p->d_table, table.data(), sizeof(StreamOp) * count, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
@@ -756,10 +777,22 @@ int bbx_stream_plan_launch(bbx_stream_plan_t* p, void* stream) {
   DeviceState* d;
   int rc = device_state(&d);
   if (rc) return rc;
+  if (p->bulk) {
+    const long long grid = std::min<long long>(p->total_chunks, (long long)d->sms);
+    k_stream_bulk<kBulkStoreTS><<<(int)grid, kBulkThreads, kBulkSmem, (cudaStream_t)stream>>>(
+        p->d_table, p->count, p->total_chunks, d->status, kBulkPiece);
+    BBX_CHECK_LAUNCH("k_stream_bulk");
+    return BBX_OK;
+  }
   long long grid = std::min<long long>(p->total_chunks, (long long)d->sms * 8);
   k_stream_group<<<(int)grid, 256, 0, (cudaStream_t)stream>>>(p->d_table, p->count, p->total_chunks);
   BBX_CHECK_LAUNCH("k_stream_group");
   return BBX_OK;
+}
+
+int bbx_stream_plan_bulk(const bbx_stream_plan_t* p) {
+  if (!p) return set_error(BBX_ERR_INVALID, "null stream plan");
+  return p->bulk ? 1 : 0;
 }
 
 int bbx_stream_plan_destroy(bbx_stream_plan_t* p) {
@@ -779,12 +812,20 @@ int bbx_stream_group(const bbx_stream_op_t* ops, int count, void* stream) {
     const int c = std::min(kStreamInline, count - i);
     std::vector<StreamOp> table;
     long long total = 0;
-    rc = build_stream_table(ops + i, c, &table, &total);
+    bool bulk = false;
+    rc = build_stream_table(ops + i, c, &table, &total, &bulk);
     if (rc) return rc;
     if (total == 0) continue;
     StreamInline args;
     memset(&args, 0, sizeof(args));
     for (int j = 0; j < c; ++j) args.ops[j] = table[j];
+    if (bulk) {
+      const long long grid = std::min<long long>(total, (long long)d->sms);
+      k_stream_bulk_inline<kBulkStoreTS><<<(int)grid, kBulkThreads, kBulkSmem, (cudaStream_t)stream>>>(
+          args, c, total, d->status, kBulkPiece);
+      BBX_CHECK_LAUNCH("k_stream_bulk_inline");
+      continue;
+    }
     long long grid = std::min<long long>(total, (long long)d->sms * 8);
     k_stream_group_inline<<<(int)grid, 256, 0, (cudaStream_t)stream>>>(args, c, total);
     BBX_CHECK_LAUNCH("k_stream_group_inline");

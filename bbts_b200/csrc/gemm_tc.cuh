@@ -401,10 +401,16 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       int s = 0;
       uint32_t ph = 0;
       bool ok = true;
+      int last_p = -1;
       for (int t = blockIdx.x; t < args.total_tiles && ok; t += gridDim.x) {
         int p, tm, tn, kdim;
         tc_locate(args, meta, t, p, tm, tn, kdim);
         const TcProblem* pr = tc_problem(args, p);
+        if (args.table && p != last_p) {
+          tensormap_acquire(&pr->tmap_a);
+          tensormap_acquire(&pr->tmap_b);
+          last_p = p;
+        }
         if (args.table && t + (int)gridDim.x < args.total_tiles) {
           // the next tile's tensor maps, if it starts a new problem
           int p2, tm2, tn2, k2;
@@ -498,10 +504,15 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     const int lane_base = 32 * (warp & 3);
     int acc = 0;
     uint32_t acc_ph = 0;
+    int last_p = -1;
     for (int t = blockIdx.x; t < args.total_tiles; t += gridDim.x) {
       int p, tm, tn, kdim;
       tc_locate(args, meta, t, p, tm, tn, kdim);
       const TcProblem* pr = tc_problem(args, p);
+      if (args.table && p != last_p) {
+        if (lane == 0 && (pr->flags & EPI_TMA_STORE)) tensormap_acquire(&pr->tmap_c);
+        last_p = p;
+      }
       // Warp-uniform outcome: tcgen05.ld below is warp-collective.
       const bool got = mbar_wait(&tfull_bar[acc], acc_ph, status, DEV_TIMEOUT_TMEM_FULL);
       if (!__all_sync(0xffffffffu, got)) break;
@@ -604,10 +615,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
       int s = 0;
       uint32_t ph = 0;
       bool ok = true;
+      int last_p = -1;
       for (int t = pair; t < args.total_tiles && ok; t += num_pairs) {
         int p, tm, tn, kdim;
         tc_locate(args, meta, t, p, tm, tn, kdim);
         const TcProblem* pr = tc_problem(args, p);
+        if (args.table && p != last_p) {
+          tensormap_acquire(&pr->tmap_a);
+          tensormap_acquire(&pr->tmap_b);
+          last_p = p;
+        }
         if (args.table && t + num_pairs < args.total_tiles) {
           // the next tile's tensor maps, if it starts a new problem
           int p2, tm2, tn2, k2;
@@ -696,10 +713,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
     const uint32_t tempty_leader1 = mapa_shared(smem_u32(&tempty_bar[1]), 0);
     int acc = 0;
     uint32_t acc_ph = 0;
+    int last_p = -1;
     for (int t = pair; t < args.total_tiles; t += num_pairs) {
       int p, tm, tn, kdim;
       tc_locate(args, meta, t, p, tm, tn, kdim);
       const TcProblem* pr = tc_problem(args, p);
+      if (args.table && p != last_p) {
+        if (lane == 0 && (pr->flags & EPI_TMA_STORE)) tensormap_acquire(&pr->tmap_c);
+        last_p = p;
+      }
       const bool got = mbar_wait(&tfull_bar[acc], acc_ph, status, DEV_TIMEOUT_TMEM_FULL);
       if (!__all_sync(0xffffffffu, got)) break;
       tc_fence_after();

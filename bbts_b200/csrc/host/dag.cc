@@ -134,6 +134,11 @@ struct dag_t {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   dag_stats_t stats{};
+  // blocks the graph reads in place: held resident (never spilled) while it lives
+  std::vector<tid_t> held;
+  ~dag_t() {
+    if (rt && !held.empty()) rt->storage->release(held);
+  }
 };
 
 namespace {
@@ -223,23 +228,38 @@ int autotune_tile_n(int dtype, bool ta, bool tb, const std::vector<bbx_tc_proble
   cudaEventCreate(&e1);
   int best = 256;
   float best_ms = 1e30f;
+  // every candidate's plan is built before any runs and freed after all ran,
+  // so no plan's table lands where another candidate's tensor maps were used
+  std::vector<std::pair<int, bbx_tc_plan_t*>> cand;
   for (int tn : {512, 256, 128}) {
     if (tn == 512 && dtype == ELEM_E4M3) continue;  // the 2-SM pair tile is bf16 only
     bbx_tc_plan_t* p = nullptr;
-    if (bbx_tc_plan_create(dtype == ELEM_E4M3 ? BBX_E4M3 : BBX_BF16, ps.data(), (int)ps.size(), tn, &p) != 0) continue;
-    dag_bbx(bbx_tc_plan_launch(p, st));  // warm-up
-    cudaEventRecord(e0, st);
-    for (int r = 0; r < 3; ++r) dag_bbx(bbx_tc_plan_launch(p, st));
-    cudaEventRecord(e1, st);
-    dag_cuda(cudaEventSynchronize(e1), "tune sync");
-    float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    bbx_tc_plan_destroy(p);
-    if (ms < best_ms) { best_ms = ms; best = tn; }
+    if (bbx_tc_plan_create(dtype == ELEM_E4M3 ? BBX_E4M3 : BBX_BF16, ps.data(), (int)ps.size(), tn, &p) == 0)
+      cand.push_back({tn, p});
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  cudaStreamDestroy(st);
+  auto release = [&]() {
+    cudaStreamSynchronize(st);
+    for (auto& c : cand) bbx_tc_plan_destroy(c.second);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(st);
+  };
+  try {
+    for (auto& c : cand) {
+      dag_bbx(bbx_tc_plan_launch(c.second, st));  // warm-up
+      cudaEventRecord(e0, st);
+      for (int r = 0; r < 3; ++r) dag_bbx(bbx_tc_plan_launch(c.second, st));
+      cudaEventRecord(e1, st);
+      dag_cuda(cudaEventSynchronize(e1), "tune sync");
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best_ms) { best_ms = ms; best = c.first; }
+    }
+  } catch (...) {
+    release();
+    throw;
+  }
+  release();
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune[key] = best;
   if (path) {
@@ -276,7 +296,8 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
   d->rt = rt;
   const tensor_factory_t& tf = *rt->tf;
 
-  // ---- tensors that already exist (registered inputs)
+  // ---- tensors that already exist (registered inputs), resident for the graph's lifetime
+  d->held = rt->storage->hold_all();
   for (tid_t t : rt->storage->tids()) {
     tplan_t tp;
     tp.meta = rt->storage->get(t)->_meta;

@@ -141,7 +141,8 @@ int bbx_rt_tensor_get(bbx_rt_t* rt, int tid, void* meta_out, void* dst, size_t c
     size_t have = rt->rt.tf->get_payload_size(t->_meta);
     size_t n = std::min(have, cap);
     if (dst && n) {
-      cudaError_t e = cudaMemcpyAsync(dst, t->_meta.payload(), n,
+      void* src = rt->rt.storage->caller_payload(tid, nullptr, false);  // reloaded if spilled
+      cudaError_t e = cudaMemcpyAsync(dst, src, n,
                                       dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                                       rt->rt.stream);
       if (e == cudaSuccess) e = cudaStreamSynchronize(rt->rt.stream);
@@ -152,10 +153,28 @@ int bbx_rt_tensor_get(bbx_rt_t* rt, int tid, void* meta_out, void* dst, size_t c
 
 int bbx_rt_tensor_payload(bbx_rt_t* rt, int tid, void** ptr, size_t* bytes) {
   if (!rt) return bbx::set_error(BBX_ERR_INVALID, "null runtime");
-  block_t* b = rt->rt.storage->block(tid);
-  if (!b) return bbx::set_error(BBX_ERR_NOT_FOUND, "no tensor %d", tid);
-  if (ptr) *ptr = b->payload;
-  if (bytes) *bytes = b->bytes;
+  if (!rt->rt.storage->get(tid)) return bbx::set_error(BBX_ERR_NOT_FOUND, "no tensor %d", tid);
+  RT_TRY({
+    size_t n = 0;
+    void* p = rt->rt.storage->caller_payload(tid, &n, true);  // reloaded if spilled; the caller may write
+    if (ptr) *ptr = p;
+    if (bytes) *bytes = n;
+  });
+}
+
+int bbx_rt_set_storage_budget(bbx_rt_t* rt, unsigned long long device_bytes, unsigned long long host_bytes,
+                              const char* spill_file) {
+  if (!rt) return bbx::set_error(BBX_ERR_INVALID, "null runtime");
+  RT_TRY(rt->rt.storage->set_budget((size_t)device_bytes, (size_t)host_bytes, spill_file ? spill_file : ""));
+}
+
+int bbx_rt_spill_stats(bbx_rt_t* rt, unsigned long long* out, int n) {
+  if (!rt || !out) return bbx::set_error(BBX_ERR_INVALID, "null argument");
+  spill_stats_t s = rt->rt.storage->stats();
+  const unsigned long long v[10] = {s.evictions,        s.reloads,         s.d2h_bytes,      s.h2d_bytes,
+                                    s.file_write_bytes, s.file_read_bytes, s.clean_evictions, s.resident_bytes,
+                                    s.peak_resident_bytes, s.host_bytes};
+  for (int i = 0; i < n && i < 10; ++i) out[i] = v[i];
   return BBX_OK;
 }
 

@@ -1,7 +1,12 @@
 // Runtime: block storage, per-op runner and the grouped DAG executor.
 #include "runtime.h"
 
+#include <fcntl.h>
+#include <unistd.h>
+
 #include <algorithm>
+#include <cerrno>
+#include <cstring>
 #include <cmath>
 #include <numeric>
 #include <set>
@@ -24,6 +29,14 @@ bool starts_with(const std::string& s, const char* p) { return s.rfind(p, 0) == 
 }  // namespace
 
 // ------------------------------------------------------------------ storage
+namespace {
+constexpr size_t kStageBytes = 64ull << 20;  // file-tier staging buffer
+constexpr size_t kFileAlign = 4096;
+void wait_on(cudaStream_t st, const event_ptr& e) {
+  if (e) cuda_ok(cudaStreamWaitEvent(st, e.get(), 0), "cudaStreamWaitEvent(storage)");
+}
+}  // namespace
+
 block_storage_t::block_storage_t(tensor_factory_ptr_t tf, cudaStream_t st) : _tf(std::move(tf)), _st(st) {
   int dev = 0;
   cuda_ok(cudaGetDevice(&dev), "cudaGetDevice");
@@ -38,77 +51,304 @@ block_storage_t::block_storage_t(tensor_factory_ptr_t tf, cudaStream_t st) : _tf
 
 block_storage_t::~block_storage_t() {
   for (auto& kv : _blocks)
-    if (kv.second.owned && kv.second.payload) cudaFreeAsync(kv.second.payload, _st);
+    if (kv.second.owned && kv.second.resident && kv.second.payload) cudaFreeAsync(kv.second.payload, _st);
   cudaStreamSynchronize(_st);
+  if (_out_st) {
+    cudaStreamSynchronize(_out_st);
+    cudaStreamDestroy(_out_st);
+  }
   _blocks.clear();
+  _host_cache.clear();
+  _freed.reset();
+  for (void* h : _host_all) cudaFreeHost(h);
+  if (_stage) cudaFreeHost(_stage);
+  if (_fd >= 0) {
+    close(_fd);
+    unlink(_file.c_str());  // the spill file is scratch
+  }
   if (_pool) cudaMemPoolDestroy(_pool);
+}
+
+event_ptr block_storage_t::_record(cudaStream_t st) {
+  cudaEvent_t e;
+  cuda_ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate(storage)");
+  cudaError_t r = cudaEventRecord(e, st);
+  if (r != cudaSuccess) {
+    cudaEventDestroy(e);
+    cuda_ok(r, "cudaEventRecord(storage)");
+  }
+  return event_ptr(e, [](cudaEvent_t x) { cudaEventDestroy(x); });
+}
+
+void block_storage_t::_lru_remove(block_t& b) {
+  if (b.in_lru) {
+    _lru[b.lru_list].erase(b.lru_it);
+    b.in_lru = false;
+  }
+}
+
+// Most recently used position of the list the block belongs in.
+void block_storage_t::_lru_touch(tid_t tid, block_t& b) {
+  _lru_remove(b);
+  if (!_budget || b.pins || !b.resident || !b.owned) return;
+  b.lru_list = b.readers_left == 0 ? 1 : 0;
+  _lru[b.lru_list].push_front(tid);
+  b.lru_it = _lru[b.lru_list].begin();
+  b.in_lru = true;
+}
+
+void block_storage_t::_pin(tid_t, block_t& b) {
+  _lru_remove(b);
+  ++b.pins;
+}
+
+void block_storage_t::_unpin(tid_t tid, block_t& b) {
+  if (b.pins > 0) --b.pins;
+  if (b.pins == 0) _lru_touch(tid, b);
+}
+
+void block_storage_t::set_readers_left(tid_t tid, int n) {
+  std::lock_guard<std::recursive_mutex> lk(_m);
+  auto it = _blocks.find(tid);
+  if (it == _blocks.end()) return;
+  block_t& b = it->second;
+  const bool moved = b.in_lru && (b.lru_list == 1) != (n == 0);
+  b.readers_left = n;
+  if (moved) _lru_touch(tid, b);
+}
+
+// The host copy goes back to the pinned cache; the D2H that reuses it waits
+// for the last H2D that read it.
+void block_storage_t::_drop_copies(block_t& b) {
+  if (b.host) {
+    _host_cache.insert({b.bytes, {b.host, b.host_read}});
+    _stats.host_bytes -= b.bytes;
+    b.host = nullptr;
+  }
+  b.host_valid = false;
+  b.file_valid = false;
+  b.copied.reset();
+  b.host_read.reset();
+}
+
+void block_storage_t::_free_payload(block_t& b, cudaStream_t st) {
+  _lru_remove(b);
+  if (b.owned && b.resident && b.payload) {
+    cudaFreeAsync(b.payload, st);  // stream-ordered
+    _stats.resident_bytes -= b.bytes;
+  }
+  b.payload = nullptr;
+  _drop_copies(b);
+}
+
+void* block_storage_t::_host_alloc(size_t bytes, event_ptr* last_read) {
+  auto it = _host_cache.find(bytes);
+  if (it != _host_cache.end()) {
+    void* p = it->second.first;
+    *last_read = it->second.second;
+    _host_cache.erase(it);
+    return p;
+  }
+  void* p = nullptr;
+  cuda_ok(cudaHostAlloc(&p, bytes, cudaHostAllocDefault), "cudaHostAlloc(spill)");
+  _host_all.push_back(p);
+  last_read->reset();
+  return p;
+}
+
+// File tier: chunks through a pinned staging buffer, synchronous like the
+// reference's pwrite / pread (nvme_storage.cc:167,577).
+void block_storage_t::_file_io(block_t& b, bool write, cudaStream_t st) {
+  if (!_stage) cuda_ok(cudaHostAlloc(&_stage, kStageBytes, cudaHostAllocDefault), "cudaHostAlloc(stage)");
+  if (write && b.file_off < 0) {
+    b.file_off = _file_end;
+    _file_end += (long long)((b.bytes + kFileAlign - 1) / kFileAlign * kFileAlign);
+  }
+  for (size_t o = 0; o < b.bytes; o += kStageBytes) {
+    const size_t n = std::min(kStageBytes, b.bytes - o);
+    char* dev = (char*)b.payload + o;
+    if (write) {
+      cuda_ok(cudaMemcpyAsync(_stage, dev, n, cudaMemcpyDeviceToHost, st), "spill D2H (file)");
+      cuda_ok(cudaStreamSynchronize(st), "spill D2H sync");
+      for (size_t w = 0; w < n;) {
+        ssize_t r = pwrite(_fd, (char*)_stage + w, n - w, b.file_off + (long long)(o + w));
+        if (r <= 0) throw std::runtime_error("block storage: pwrite to the spill file failed: " + std::string(strerror(errno)));
+        w += (size_t)r;
+      }
+      _stats.file_write_bytes += n;
+    } else {
+      for (size_t w = 0; w < n;) {
+        ssize_t r = pread(_fd, (char*)_stage + w, n - w, b.file_off + (long long)(o + w));
+        if (r <= 0) throw std::runtime_error("block storage: pread from the spill file failed");
+        w += (size_t)r;
+      }
+      cuda_ok(cudaMemcpyAsync(dev, _stage, n, cudaMemcpyHostToDevice, st), "reload H2D (file)");
+      cuda_ok(cudaStreamSynchronize(st), "reload H2D sync");
+      _stats.file_read_bytes += n;
+    }
+  }
+}
+
+// Evicts one resident, unpinned, owned block: its bytes are copied out (unless
+// a copy from an earlier eviction is still valid) after its last uses, then
+// the payload is freed on the copy stream.
+void block_storage_t::_evict(tid_t, block_t& b) {
+  for (auto& u : b.uses) wait_on(_out_st, u.second);
+  if (b.caller_may_write) wait_on(_out_st, _record(_st));
+  if (b.host_valid || b.file_valid) {
+    ++_stats.clean_evictions;
+  } else if (_stats.host_bytes + b.bytes <= _host_budget) {
+    event_ptr last_read;
+    b.host = _host_alloc(b.bytes, &last_read);
+    wait_on(_out_st, last_read);
+    cuda_ok(cudaMemcpyAsync(b.host, b.payload, b.bytes, cudaMemcpyDeviceToHost, _out_st), "spill D2H");
+    b.copied = _record(_out_st);
+    b.host_valid = true;
+    _stats.host_bytes += b.bytes;
+    _stats.d2h_bytes += b.bytes;
+  } else if (_fd >= 0) {
+    _file_io(b, true, _out_st);
+    b.file_valid = true;
+    _stats.d2h_bytes += b.bytes;
+  } else {
+    throw std::runtime_error("block storage: the host spill budget is exhausted and no spill file is set");
+  }
+  cuda_ok(cudaFreeAsync(b.payload, _out_st), "cudaFreeAsync(spill)");
+  _lru_remove(b);
+  b.payload = nullptr;
+  b.tensor()->_meta.set_payload(nullptr);
+  b.resident = false;
+  b.uses.clear();
+  b.loaded.reset();
+  b.caller_may_write = false;
+  _stats.resident_bytes -= b.bytes;
+  ++_stats.evictions;
+}
+
+void block_storage_t::_make_room(size_t need, cudaStream_t st) {
+  if (!_budget) return;
+  if (need > _budget)
+    throw std::runtime_error("block storage: a request of " + std::to_string(need) +
+                             " bytes exceeds the device budget of " + std::to_string(_budget) + " bytes");
+  bool evicted = false;
+  while (_stats.resident_bytes + need > _budget) {
+    if (_lru[0].empty() && _lru[1].empty())
+      throw std::runtime_error("block storage: the device budget of " + std::to_string(_budget) +
+                               " bytes is held by blocks in use; " + std::to_string(need) + " more bytes needed");
+    tid_t v = _lru[1].empty() ? _lru[0].back() : _lru[1].back();
+    _evict(v, _blocks.at(v));
+    evicted = true;
+  }
+  if (evicted) {
+    _freed = _record(_out_st);
+    wait_on(st, _freed);  // the allocation below may reuse the freed memory
+  }
+}
+
+void block_storage_t::_reload(block_t& b, cudaStream_t st) {
+  _make_room(b.bytes, st);
+  void* p = nullptr;
+  cuda_ok(cudaMallocFromPoolAsync(&p, b.bytes, _pool, st), "cudaMallocFromPoolAsync(reload)");
+  b.payload = p;
+  if (b.host_valid) {
+    wait_on(st, b.copied);
+    cuda_ok(cudaMemcpyAsync(p, b.host, b.bytes, cudaMemcpyHostToDevice, st), "reload H2D");
+    b.host_read = _record(st);
+  } else if (b.file_valid) {
+    _file_io(b, false, st);
+  } else {
+    throw std::runtime_error("block storage: a spilled block has no copy to reload");
+  }
+  b.tensor()->_meta.set_payload(p);
+  b.resident = true;
+  b.loaded = _record(st);
+  b.loaded_st = st;
+  _stats.resident_bytes += b.bytes;
+  _stats.peak_resident_bytes = std::max(_stats.peak_resident_bytes, _stats.resident_bytes);
+  _stats.h2d_bytes += b.bytes;
+  ++_stats.reloads;
 }
 
 tensor_t* block_storage_t::create(tid_t tid, const tensor_meta_t& meta, cudaStream_t st) {
   if (!st) st = _st;
+  std::lock_guard<std::recursive_mutex> lk(_m);
+  auto it = _blocks.find(tid);
+  if (it != _blocks.end()) {
+    _free_payload(it->second, st);
+    _blocks.erase(it);
+  }
   size_t bytes = _tf->get_payload_size(meta);
+  _make_room(bytes, st);
   void* p = nullptr;
   if (bytes) cuda_ok(cudaMallocFromPoolAsync(&p, bytes, _pool, st), "cudaMallocFromPoolAsync(block)");
-  block_t b;
+  auto& b = _blocks[tid];
   b.header.reset(new char[sizeof(tensor_meta_t)]);
   std::memcpy(b.header.get(), &meta, sizeof(tensor_meta_t));
   b.tensor()->_meta.set_payload(p);
   b.payload = p;
   b.bytes = bytes;
   b.owned = true;
-  std::lock_guard<std::mutex> lk(_m);
-  auto it = _blocks.find(tid);
-  if (it != _blocks.end()) {
-    if (it->second.owned && it->second.payload) cudaFreeAsync(it->second.payload, st);
-    _blocks.erase(it);
+  _stats.resident_bytes += bytes;
+  _stats.peak_resident_bytes = std::max(_stats.peak_resident_bytes, _stats.resident_bytes);
+  if (_budget) {
+    if (_in_command) {
+      _pin(tid, b);
+      _scope.push_back(tid);
+    } else {
+      b.caller_may_write = true;  // filled by work the caller queues on the runtime stream
+      _unpin(tid, b);
+    }
   }
-  auto& slot = _blocks[tid];
-  slot = std::move(b);
-  return slot.tensor();
+  return b.tensor();
 }
 
 tensor_t* block_storage_t::create_view(tid_t tid, const tensor_meta_t& meta, void* payload, size_t bytes) {
-  block_t b;
+  std::lock_guard<std::recursive_mutex> lk(_m);
+  auto it = _blocks.find(tid);
+  if (it != _blocks.end()) {
+    _free_payload(it->second, _st);
+    _blocks.erase(it);
+  }
+  auto& b = _blocks[tid];
   b.header.reset(new char[sizeof(tensor_meta_t)]);
   std::memcpy(b.header.get(), &meta, sizeof(tensor_meta_t));
   b.tensor()->_meta.set_payload(payload);
   b.payload = payload;
   b.bytes = bytes;
-  b.owned = false;
-  std::lock_guard<std::mutex> lk(_m);
-  auto& slot = _blocks[tid];
-  if (slot.owned && slot.payload) cudaFreeAsync(slot.payload, _st);
-  slot = std::move(b);
-  return slot.tensor();
+  b.owned = false;  // never counted, never evicted
+  return b.tensor();
 }
 
 tensor_t* block_storage_t::get(tid_t tid) {
-  std::lock_guard<std::mutex> lk(_m);
+  std::lock_guard<std::recursive_mutex> lk(_m);
   auto it = _blocks.find(tid);
   return it == _blocks.end() ? nullptr : it->second.tensor();
 }
 
 block_t* block_storage_t::block(tid_t tid) {
-  std::lock_guard<std::mutex> lk(_m);
+  std::lock_guard<std::recursive_mutex> lk(_m);
   auto it = _blocks.find(tid);
   return it == _blocks.end() ? nullptr : &it->second;
 }
 
 bool block_storage_t::remove(tid_t tid, cudaStream_t st) {
-  std::lock_guard<std::mutex> lk(_m);
+  std::lock_guard<std::recursive_mutex> lk(_m);
   auto it = _blocks.find(tid);
   if (it == _blocks.end()) return false;
-  if (it->second.owned && it->second.payload) cudaFreeAsync(it->second.payload, st ? st : _st);  // stream-ordered
+  _free_payload(it->second, st ? st : _st);
   _blocks.erase(it);
   return true;
 }
 
 bool block_storage_t::assign_tid(tid_t from, tid_t to) {
-  std::lock_guard<std::mutex> lk(_m);
+  std::lock_guard<std::recursive_mutex> lk(_m);
   auto it = _blocks.find(from);
   if (it == _blocks.end() || _blocks.count(to)) return false;
   block_t b = std::move(it->second);
   _blocks.erase(it);
+  if (b.in_lru) *b.lru_it = to;  // the list node moves with the block
+  for (auto& t : _scope)
+    if (t == from) t = to;
   _blocks[to] = std::move(b);
   return true;
 }
@@ -118,6 +358,146 @@ std::vector<tid_t> block_storage_t::tids() const {
   for (auto& kv : _blocks) out.push_back(kv.first);
   return out;
 }
+
+void block_storage_t::set_budget(size_t device_bytes, size_t host_bytes, const std::string& file) {
+  std::lock_guard<std::recursive_mutex> lk(_m);
+  if (!_out_st) cuda_ok(cudaStreamCreateWithFlags(&_out_st, cudaStreamNonBlocking), "cudaStreamCreate(spill)");
+  // bring every spilled block back first (its copy may be in the file being replaced)
+  _budget = 0;
+  for (auto& kv : _blocks)
+    if (!kv.second.resident) _reload(kv.second, _st);
+  _lru[0].clear();
+  _lru[1].clear();
+  for (auto& kv : _blocks) kv.second.in_lru = false;
+  if (file != _file || !device_bytes) {
+    for (auto& kv : _blocks) kv.second.file_valid = false, kv.second.file_off = -1;
+    if (_fd >= 0) {
+      close(_fd);
+      unlink(_file.c_str());
+      _fd = -1;
+    }
+    _file = device_bytes ? file : std::string();
+    _file_end = 0;
+    if (!_file.empty()) {
+      _fd = open(_file.c_str(), O_CREAT | O_TRUNC | O_RDWR, 0600);
+      if (_fd < 0) throw std::runtime_error("block storage: cannot open the spill file " + _file);
+    }
+  }
+  _budget = device_bytes;
+  _host_budget = host_bytes;
+  _stats = spill_stats_t{};
+  for (auto& kv : _blocks)
+    if (kv.second.owned) _stats.resident_bytes += kv.second.bytes;
+  _stats.peak_resident_bytes = _stats.resident_bytes;
+  for (auto& kv : _blocks) _stats.host_bytes += kv.second.host ? kv.second.bytes : 0;
+  if (_budget) {
+    for (auto& kv : _blocks) {
+      block_t& b = kv.second;
+      if (b.owned && b.pins == 0) {
+        b.caller_may_write = true;  // writers unknown: wait for the runtime stream
+        _unpin(kv.first, b);
+      }
+    }
+    _make_room(0, _st);
+    _stats.peak_resident_bytes = _stats.resident_bytes;  // within the budget from here on
+  }
+  cuda_ok(cudaStreamSynchronize(_st), "set_budget sync");
+}
+
+void block_storage_t::begin_command() {
+  std::lock_guard<std::recursive_mutex> lk(_m);
+  _in_command = true;
+  _scope.clear();
+}
+
+tensor_t* block_storage_t::acquire(tid_t tid, cudaStream_t st) {
+  std::lock_guard<std::recursive_mutex> lk(_m);
+  auto it = _blocks.find(tid);
+  if (it == _blocks.end()) return nullptr;
+  block_t& b = it->second;
+  if (!_budget) return b.tensor();
+  if (!b.resident) _reload(b, st);
+  else if (b.loaded && b.loaded_st != st) wait_on(st, b.loaded);  // reloaded for a command on another stream
+  if (_in_command) {
+    _pin(tid, b);
+    _scope.push_back(tid);
+  } else if (b.in_lru) {
+    _lru_touch(tid, b);
+  }
+  return b.tensor();
+}
+
+void block_storage_t::end_command(cudaStream_t st) {
+  std::lock_guard<std::recursive_mutex> lk(_m);
+  _in_command = false;
+  if (!_budget || _scope.empty()) {
+    _scope.clear();
+    return;
+  }
+  event_ptr e = _record(st);
+  for (tid_t t : _scope) {
+    auto it = _blocks.find(t);
+    if (it == _blocks.end()) continue;  // removed inside the command (a reduce temporary)
+    block_t& b = it->second;
+    bool found = false;
+    for (auto& u : b.uses)
+      if (u.first == st) u.second = e, found = true;
+    if (!found) b.uses.push_back({st, e});
+    _unpin(t, b);
+  }
+  _scope.clear();
+}
+
+void* block_storage_t::caller_payload(tid_t tid, size_t* bytes, bool will_write) {
+  std::lock_guard<std::recursive_mutex> lk(_m);
+  auto it = _blocks.find(tid);
+  if (it == _blocks.end()) return nullptr;
+  block_t& b = it->second;
+  if (_budget) {
+    if (!b.resident) _reload(b, _st);
+    else if (b.loaded && b.loaded_st != _st) wait_on(_st, b.loaded);
+    if (will_write) {
+      b.caller_may_write = true;
+      _drop_copies(b);
+    }
+    if (b.in_lru) _lru_touch(tid, b);
+  }
+  if (bytes) *bytes = b.bytes;
+  return b.payload;
+}
+
+std::vector<tid_t> block_storage_t::hold_all() {
+  std::lock_guard<std::recursive_mutex> lk(_m);
+  std::vector<tid_t> held;
+  if (!_budget) return held;
+  try {
+    for (auto& kv : _blocks) {
+      block_t& b = kv.second;
+      if (!b.owned) continue;
+      if (!b.resident) _reload(b, _st);
+      else if (b.loaded && b.loaded_st != _st) wait_on(_st, b.loaded);
+      _pin(kv.first, b);
+      held.push_back(kv.first);
+    }
+  } catch (...) {
+    for (tid_t t : held) _unpin(t, _blocks.at(t));
+    throw;
+  }
+  cuda_ok(cudaStreamSynchronize(_st), "hold_all sync");
+  return held;
+}
+
+void block_storage_t::release(const std::vector<tid_t>& tids) {
+  std::lock_guard<std::recursive_mutex> lk(_m);
+  for (tid_t t : tids) {
+    auto it = _blocks.find(t);
+    if (it == _blocks.end()) continue;
+    it->second.caller_may_write = true;  // the DAG's launches ran on streams the storage does not know
+    _unpin(t, it->second);
+  }
+}
+
+spill_stats_t block_storage_t::stats() const { return _stats; }
 
 // ------------------------------------------------------------------ runtime
 runtime_t::runtime_t() {
@@ -228,7 +608,7 @@ void execute_command(runtime_t& rt, command_t& cmd, cudaStream_t st) {
     std::vector<tensor_meta_t> in_meta(ni), out_meta(no);
     ud_impl_t::tensor_args_t in_args(ni);
     for (size_t i = 0; i < ni; ++i) {
-      tensor_t* t = rt.storage->get(cmd.get_input(i).tid);
+      tensor_t* t = rt.storage->acquire(cmd.get_input(i).tid, st);
       if (!t) throw std::runtime_error("APPLY " + std::to_string(cmd.id) + ": input tensor missing");
       in_meta[i] = t->_meta;
       in_args.set(i, *t);
@@ -250,7 +630,7 @@ void execute_command(runtime_t& rt, command_t& cmd, cudaStream_t st) {
     const size_t ni = cmd.get_num_inputs();
     std::vector<tensor_t*> ins(ni);
     for (size_t i = 0; i < ni; ++i) {
-      ins[i] = rt.storage->get(cmd.get_input(i).tid);
+      ins[i] = rt.storage->acquire(cmd.get_input(i).tid, st);
       if (!ins[i]) throw std::runtime_error("REDUCE " + std::to_string(cmd.id) + ": input tensor missing");
     }
     tid_t out_tid = cmd.get_output(0).tid;
@@ -418,6 +798,18 @@ void runtime_t::run_per_op(int policy, std::vector<std::pair<op_features_t, floa
     reads.erase(t);
     ready.erase(t);
   };
+  // eviction hint under a storage budget: queued reads left per block
+  const bool hint_readers = storage->budget() > 0;
+  std::unordered_map<tid_t, int> readers_left;
+  if (hint_readers) {
+    for (auto& c : commands)
+      if (!c->is_delete())
+        for (size_t j = 0; j < c->get_num_inputs(); ++j) ++readers_left[c->get_input(j).tid];
+    for (tid_t t : storage->tids()) {
+      auto r = readers_left.find(t);
+      storage->set_readers_left(t, r == readers_left.end() ? 0 : r->second);
+    }
+  }
   std::vector<double> avail(K, 0.0);             // predicted time each stream frees up
   std::unordered_map<tid_t, double> t_ready;     // predicted time each block is written
   int rr = 0;
@@ -465,7 +857,25 @@ void runtime_t::run_per_op(int policy, std::vector<std::pair<op_features_t, floa
       cudaEventCreate(&e1);
       cudaEventRecord(e0, s);
     }
-    execute_command(*this, *cmd, s);
+    storage->begin_command();
+    try {
+      execute_command(*this, *cmd, s);
+    } catch (...) {
+      storage->end_command(s);
+      throw;
+    }
+    storage->end_command(s);
+    if (hint_readers) {
+      for (size_t j = 0; j < cmd->get_num_inputs(); ++j) {
+        const tid_t t = cmd->get_input(j).tid;
+        storage->set_readers_left(t, --readers_left[t]);
+      }
+      for (size_t o = 0; o < cmd->get_num_outputs(); ++o) {
+        const tid_t t = cmd->get_output(o).tid;
+        auto r = readers_left.find(t);
+        storage->set_readers_left(t, r == readers_left.end() ? 0 : r->second);
+      }
+    }
     if (record) {
       cudaEventRecord(e1, s);
       evs.push_back({e0, e1});

@@ -5,6 +5,7 @@
 // launch per wave, captured into a CUDA graph).
 #pragma once
 #include <cuda_runtime.h>
+#include <list>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -18,40 +19,133 @@
 
 namespace bbts {
 
+// Completion marker of stream work, shared by the blocks that wait on it.
+using event_ptr = std::shared_ptr<CUevent_st>;
+
 // One block: a host-side header in the reference layout whose payload slot
-// points at HBM.
+// points at HBM while the block is resident. A spilled block keeps its header;
+// its bytes live in pinned host memory (host tier) or in the spill file (file
+// tier) until a command needs it again.
 struct block_t {
   std::unique_ptr<char[]> header;  // sizeof(tensor_meta_t) bytes
-  void* payload = nullptr;
+  void* payload = nullptr;         // HBM; null while spilled
   size_t bytes = 0;
   bool owned = true;               // payload allocated by storage (freed by it)
+  bool resident = true;
+  // spill copies; blocks are written once by the command that creates them,
+  // so a copy stays valid across reloads until a caller is handed the
+  // payload pointer (it may write through it)
+  void* host = nullptr;
+  bool host_valid = false;
+  long long file_off = -1;
+  bool file_valid = false;
+  bool caller_may_write = false;   // last writer may be work the caller queued on the runtime stream
+  int pins = 0;                    // commands (or compiled DAGs) holding the payload
+  std::vector<std::pair<cudaStream_t, event_ptr>> uses;  // last use per stream while resident
+  event_ptr copied;                // the D2H that filled the host copy
+  event_ptr host_read;             // the last H2D that read the host copy
+  event_ptr loaded;                // the reload that made the payload resident again
+  cudaStream_t loaded_st = nullptr;
+  int readers_left = -1;           // commands still to read it in the running list (-1: unknown)
+  bool in_lru = false;
+  int lru_list = 0;                // 0: blocks still to be read, 1: blocks no queued command reads
+  std::list<tid_t>::iterator lru_it;
   tensor_t* tensor() const { return (tensor_t*)header.get(); }
 };
 
-// tid -> block. Payload allocations are stream-ordered on the runtime stream.
-// Payloads come from a memory pool the storage owns, stream-ordered on the
-// stream each call names (the runtime stream by default). The pool keeps freed
-// memory for reuse instead of returning it to the driver at every
-// synchronisation, so a block freed and re-created costs no new mapping.
+// Spill counters (bytes and counts since the budget was set).
+struct spill_stats_t {
+  unsigned long long evictions = 0, reloads = 0, d2h_bytes = 0, h2d_bytes = 0;
+  unsigned long long file_write_bytes = 0, file_read_bytes = 0, clean_evictions = 0;
+  unsigned long long resident_bytes = 0, peak_resident_bytes = 0, host_bytes = 0;
+};
+
+// tid -> block. Payloads come from a memory pool the storage owns,
+// stream-ordered on the stream each call names (the runtime stream by
+// default). The pool keeps freed memory for reuse instead of returning it to
+// the driver at every synchronisation, so a block freed and re-created costs
+// no new mapping.
+//
+// With a device budget (set_budget), resident payload bytes stay within it:
+// making room evicts the least recently used unpinned blocks, copying each
+// to pinned host memory while the host budget lasts and to the spill file
+// after that, and a spilled block is copied back when a command acquires it
+// (reference: nvme_storage_t, src/storage/nvme_storage.h:26-467 and
+// nvme_storage.cc:355-637 -- LRU of unreferenced tensors, eviction to a file
+// by pwrite, reload by pread, "Can not process this." when one request alone
+// exceeds the budget). Device-to-host spill copies run on a copy stream that
+// waits for the block's last uses; the streams that allocate next wait for
+// those frees.
 class block_storage_t {
  public:
   block_storage_t(tensor_factory_ptr_t tf, cudaStream_t st);
   ~block_storage_t();
   tensor_t* create(tid_t tid, const tensor_meta_t& meta, cudaStream_t st = nullptr);  // allocates the payload
   tensor_t* create_view(tid_t tid, const tensor_meta_t& meta, void* payload, size_t bytes);
-  tensor_t* get(tid_t tid);
+  tensor_t* get(tid_t tid);        // header only; the payload slot is null while spilled
   block_t* block(tid_t tid);
   bool remove(tid_t tid, cudaStream_t st = nullptr);
   bool assign_tid(tid_t from, tid_t to);
   size_t size() const { return _blocks.size(); }
   std::vector<tid_t> tids() const;
 
+  // ---- spill tier
+  // device_bytes 0 = no budget (nothing is ever spilled). host_bytes: pinned
+  // host memory the spill may hold; past it blocks go to `file` (none = error).
+  void set_budget(size_t device_bytes, size_t host_bytes, const std::string& file);
+  size_t budget() const { return _budget; }
+  // Commands: blocks acquired or created between begin_command and
+  // end_command stay resident until end_command records their use on `st`.
+  void begin_command();
+  tensor_t* acquire(tid_t tid, cudaStream_t st);  // resident + held for the current command
+  void end_command(cudaStream_t st);
+  // Resident payload for a caller outside a command (reads, and writes when
+  // will_write, queued on the runtime stream); valid until the next call that
+  // may evict.
+  void* caller_payload(tid_t tid, size_t* bytes, bool will_write);
+  // Eviction hint from the per-op runner: how many queued commands still read
+  // `tid` (0 = none: it is evicted before blocks that will be read again).
+  void set_readers_left(tid_t tid, int n);
+  // Compiled DAGs hold every existing block resident until released.
+  std::vector<tid_t> hold_all();
+  void release(const std::vector<tid_t>& tids);
+  spill_stats_t stats() const;
+
  private:
+  void _lru_remove(block_t& b);
+  void _lru_touch(tid_t tid, block_t& b);
+  void _make_room(size_t need, cudaStream_t st);
+  void _evict(tid_t tid, block_t& b);
+  void _reload(block_t& b, cudaStream_t st);
+  void _pin(tid_t tid, block_t& b);
+  void _unpin(tid_t tid, block_t& b);
+  void _drop_copies(block_t& b);
+  void _free_payload(block_t& b, cudaStream_t st);
+  void* _host_alloc(size_t bytes, event_ptr* last_read);
+  void _file_io(block_t& b, bool write, cudaStream_t st);
+  event_ptr _record(cudaStream_t st);
+
   tensor_factory_ptr_t _tf;
   cudaStream_t _st;
   cudaMemPool_t _pool = nullptr;
-  std::mutex _m;
+  std::recursive_mutex _m;
   std::unordered_map<tid_t, block_t> _blocks;
+  // spill state
+  size_t _budget = 0, _host_budget = 0;
+  std::string _file;
+  int _fd = -1;
+  long long _file_end = 0;
+  cudaStream_t _out_st = nullptr;  // device-to-host spill copies and the frees after them
+  event_ptr _freed;                // after the latest eviction's free
+  // resident unpinned owned blocks, front = most recently used; eviction takes
+  // the blocks no queued command reads (results, list 1) before the others
+  std::list<tid_t> _lru[2];
+  std::vector<tid_t> _scope;       // blocks held by the command being issued
+  bool _in_command = false;
+  std::multimap<size_t, std::pair<void*, event_ptr>> _host_cache;  // pinned buffers free for reuse
+  std::vector<void*> _host_all;
+  void* _stage = nullptr;          // pinned staging for the file tier
+  spill_stats_t _stats;
 };
 
 // Op features for the learned cost model: the 12 MLP inputs, plus the ud's

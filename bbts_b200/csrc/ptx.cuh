@@ -177,6 +177,15 @@ __device__ __forceinline__ void tma_store_2d(const void* tmap, const void* smem_
                "r"(smem_u32(smem_src)), "r"(x), "r"(y)
                : "memory");
 }
+// Untiled bulk copy of `bytes` from global memory into this CTA's shared
+// memory, completing on `bar` (complete_tx). Both addresses 16-byte aligned,
+// bytes a multiple of 16; the destination is this CTA's own window.
+__device__ __forceinline__ void bulk_load(void* smem_dst, const void* gsrc, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(smem_dst)),
+               "l"(gsrc), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 // every committed bulk store has finished reading its shared-memory source
 __device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
@@ -184,6 +193,16 @@ __device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bu
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 // this thread's shared-memory writes become visible to the async (TMA) proxy
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Orders this thread's later uses of the tensor map at `tmap` (in global
+// memory) after the generic-proxy writes that put it there. A plan's table of
+// maps is uploaded by a copy before its launches, possibly to an address
+// where an earlier plan's maps (other boxes, other tensors) were used and may
+// still sit in the TMA unit's descriptor cache: each thread that issues TMA
+// operations through a table map runs this before its first use of the map.
+__device__ __forceinline__ void tensormap_acquire(const void* tmap) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(tmap) : "memory");
+}
 
 // Brings a tensor map (in global memory) into the TMA unit's descriptor cache
 // ahead of its first use.

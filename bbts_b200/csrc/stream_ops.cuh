@@ -10,6 +10,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
 #include <cstdint>
+#include "ptx.cuh"
 #include "quant_ops.cuh"
 
 namespace bbx {
@@ -69,6 +70,39 @@ __device__ __forceinline__ float apply_binary(int op, float a, float b, float ca
     case B_DIV: return __fdiv_rn(a, b);
   }
   return a;
+}
+
+// The same element functions as apply_unary / apply_binary (bit-identical),
+// chosen once per call: `body` receives the function for `op`, so loops over
+// elements carry no per-element dispatch.
+template <typename Body>
+__device__ __forceinline__ void with_unary(int op, float p, Body&& body) {
+  switch (op) {
+    case U_RELU: body([](float v) { return v > 0.f ? v : 0.f; }); break;
+    case U_RELU_DIF: body([](float v) { return v > 0.f ? 1.f : 0.f; }); break;
+    case U_SIGMOID_REF: body([](float v) { return __fdiv_rn(1.f, __fadd_rn(1.f, expf(v))); }); break;
+    case U_SIGMOID: body([](float v) { return __fdiv_rn(1.f, __fadd_rn(1.f, expf(-v))); }); break;
+    case U_EXP: body([](float v) { return expf(v); }); break;
+    case U_SQUARE: body([](float v) { return __fmul_rn(v, v); }); break;
+    case U_SQRT: body([](float v) { return sqrtf(v); }); break;
+    case U_ADD_SCALAR: body([p](float v) { return __fadd_rn(v, p); }); break;
+    case U_SCALE: body([p](float v) { return __fmul_rn(v, p); }); break;
+    default: body([](float v) { return v; }); break;
+  }
+}
+
+template <typename Body>
+__device__ __forceinline__ void with_binary(int op, float ca, float cb, Body&& body) {
+  switch (op) {
+    case B_ADD: body([](float a, float b) { return __fadd_rn(a, b); }); break;
+    case B_WEIGHTED: body([ca, cb](float a, float b) { return __fadd_rn(__fmul_rn(ca, a), __fmul_rn(cb, b)); }); break;
+    case B_HADAMARD: body([](float a, float b) { return __fmul_rn(a, b); }); break;
+    case B_MAX: body([](float a, float b) { return a > b ? a : b; }); break;
+    case B_MIN: body([](float a, float b) { return a < b ? a : b; }); break;
+    case B_SUB: body([](float a, float b) { return __fsub_rn(a, b); }); break;
+    case B_DIV: body([](float a, float b) { return __fdiv_rn(a, b); }); break;
+    default: body([](float a, float) { return a; }); break;
+  }
 }
 
 // ------------------------------------------------------------------ kernels
@@ -342,7 +376,7 @@ struct StreamOp {
   float p0, p1;
   long long chunk_start;
   int vec;  // 2: all pointers 16-byte aligned; 1: 16-byte (f32) / 8-byte (bf16) aligned; 0: scalar
-  int pad_;
+  int tile; // bulk-staged plans: elements per item (chunk_start then counts items)
 };
 
 __device__ __forceinline__ void ld4(const void* p, int dt, long long i, float (&v)[4]) {
@@ -637,6 +671,270 @@ __device__ __forceinline__ void stream_group_body(const TableT* __restrict__ tab
       }
     }
   }
+}
+
+}  // namespace bbx
+
+namespace bbx {
+
+// ---- bulk-staged path: used when every pointer of every op is 16-byte
+// aligned. Work is dealt as items, one op's `tile` consecutive elements, with
+// `tile` sized per op so that every item moves about kBulkSlot bytes (inputs +
+// output) whatever its fan-in. One CTA per SM:
+//  - a producer thread copies each item's input tiles into a shared-memory
+//    stage with cp.async.bulk (kBulkStages stages, completion on the stage's
+//    `full` mbarrier);
+//  - kBulkConsumerWarps warps fold them in the same order as the register
+//    paths above (bit-identical results), with the element function chosen
+//    once per item (with_unary / with_binary), and store the output with
+//    16-byte stores, handing the stage back (`empty` mbarrier) right away.
+// Measured on the FFN and 2000-op DAG levels: 8 consumer warps beat 16, whole
+// input tiles per copy beat 2-8 KiB pieces, and consumer stores beat staging
+// the output tile for a bulk store (kBulkStoreTS, kept as an option). The
+// last (< 8-element) piece of an op, if any, is read and written with plain
+// accesses.
+constexpr int kBulkStages = 3;
+constexpr int kBulkSlot = 65536;     // bytes per stage: input tiles + output tile
+constexpr int kBulkConsumerWarps = 8;
+constexpr int kBulkConsumers = kBulkConsumerWarps * 32;
+constexpr int kBulkThreads = kBulkConsumers + 32;
+constexpr int kBulkSmem = kBulkStages * kBulkSlot + kBulkStages * 16 + kBulkStages * 4;
+constexpr bool kBulkStoreTS = false;   // output tiles by consumer stores (see stream_bulk_body)
+constexpr uint32_t kBulkPiece = 65536;  // bytes per bulk load (one copy per input tile: splitting measured slower)
+
+// Elements per item: a multiple of 64 whose input and output tiles fill at
+// most one stage.
+__host__ __device__ inline int bulk_tile(int n_in, int in_esz, int out_esz) {
+  const int te = kBulkSlot / (n_in * in_esz + out_esz) / 64 * 64;
+  return te < 64 ? 64 : te;
+}
+
+template <typename TableT>
+__device__ __forceinline__ int stream_find_op(const TableT* table, int count, long long item) {
+  int lo = 0, hi = count - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (table[mid].chunk_start <= item) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Staged elements [e0, e0 + cnt) of one op: input j's tile at
+// slot + j * tile elements. TS: the output tile goes to the stage (after the
+// n_in input tiles) for a bulk store; else it is stored to global memory
+// directly. Elements [e0 + cnt, e1) are read and written in global memory.
+template <int IDT, int ODT, bool TS, typename OpT>
+__device__ __forceinline__ void bulk_item(const OpT& o, uint8_t* slot, long long e0, int cnt, long long e1,
+                                          int ctid) {
+  constexpr int VW = IDT == 1 ? 8 : 4;
+  constexpr int ESZ = IDT == 1 ? 2 : 4;
+  const int kind = o.kind, nin = o.n_in, op = o.op, te = o.tile;
+  const bool kahan = o.kahan != 0;
+  const float p0 = o.p0, p1 = o.p1;
+  void* const out = o.out;
+  uint8_t* const oslot = slot + (size_t)nin * te * ESZ;
+  auto put = [&](int li, const float (&r)[VW]) {
+    if constexpr (TS) stv<ODT, VW>(oslot, li, r);
+    else stv<ODT, VW>(out, e0 + li, r);
+  };
+  if (kind == S_SUM) {
+    for (int li = ctid * VW; li < cnt; li += kBulkConsumers * VW) {
+      float a[VW], comp[VW];
+      ldv<IDT, VW>(slot, li, a);
+#pragma unroll
+      for (int u = 0; u < VW; ++u) comp[u] = 0.f;
+      for (int j = 1; j < nin; ++j) {
+        float b[VW];
+        ldv<IDT, VW>(slot + (size_t)j * te * ESZ, li, b);
+        fold_in(a, comp, b, kahan);
+      }
+      put(li, a);
+    }
+  } else if (kind == S_BINARY) {
+    const uint8_t* const slot_b = slot + (size_t)te * ESZ;
+    with_binary(op, p0, p1, [&](auto f) {
+      for (int li = ctid * VW; li < cnt; li += kBulkConsumers * VW) {
+        float a[VW], b[VW], r[VW];
+        ldv<IDT, VW>(slot, li, a);
+        ldv<IDT, VW>(slot_b, li, b);
+#pragma unroll
+        for (int u = 0; u < VW; ++u) r[u] = f(a[u], b[u]);
+        put(li, r);
+      }
+    });
+  } else {
+    // unary, or a cast (the identity)
+    with_unary(kind == S_UNARY ? op : -1, p0, [&](auto f) {
+      for (int li = ctid * VW; li < cnt; li += kBulkConsumers * VW) {
+        float a[VW], r[VW];
+        ldv<IDT, VW>(slot, li, a);
+#pragma unroll
+        for (int u = 0; u < VW; ++u) r[u] = f(a[u]);
+        put(li, r);
+      }
+    });
+  }
+  for (long long q = e0 + cnt + ctid; q < e1; q += kBulkConsumers) {
+    float x = ld1(o.in[0], IDT, q);
+    if (kind == S_SUM) {
+      float comp = 0.f;
+      for (int j = 1; j < nin; ++j) {
+        const float v = ld1(o.in[j], IDT, q);
+        if (kahan) {
+          const float y = __fsub_rn(v, comp), t = __fadd_rn(x, y);
+          comp = __fsub_rn(__fsub_rn(t, x), y);
+          x = t;
+        } else {
+          x = __fadd_rn(x, v);
+        }
+      }
+    } else if (kind == S_BINARY) {
+      x = apply_binary(op, x, ld1(o.in[1], IDT, q), p0, p1);
+    } else if (kind == S_UNARY) {
+      x = apply_unary(op, x, p0);
+    }
+    st1(out, ODT, q, x);
+  }
+}
+
+// Bounded wait that ignores the status word: used only to let copies already
+// issued land before the CTA exits after an error.
+__device__ __forceinline__ void mbar_drain(uint64_t* bar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - t0 > kWaitBudgetCycles) return;
+}
+
+// Global bulk store from this CTA's shared memory (bulk-group completion);
+// both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_store(void* gdst, const void* smem_src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(smem_u32(smem_src)),
+               "r"(bytes)
+               : "memory");
+}
+// at most one committed bulk-store group still reading shared memory
+__device__ __forceinline__ void bulk_wait_read_1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+__device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kBulkConsumers) : "memory"); }
+// Barrier over the consumer threads that also ANDs their flags: every consumer
+// takes the same branch after a bounded wait, so none is left at a barrier.
+__device__ __forceinline__ bool consumers_all(bool p) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, 1, %2, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)p), "n"(kBulkConsumers)
+      : "memory");
+  return r != 0;
+}
+
+// TS: output tiles leave by bulk store (the stage is handed back once the
+// store has read it); else consumers store them and hand the stage back
+// right away. Input tiles are copied in pieces of at most `piece` bytes so
+// several bulk copies are in flight even for a one-input op.
+template <bool TS, typename TableT>
+__device__ __forceinline__ void stream_bulk_body(const TableT* table, int count, long long total_items,
+                                                 uint32_t* status, uint32_t piece) {
+  extern __shared__ __align__(128) uint8_t bulk_smem[];
+  uint64_t* full = (uint64_t*)(bulk_smem + kBulkStages * kBulkSlot);
+  uint64_t* empty = full + kBulkStages;
+  int* stage_op = (int*)(empty + kBulkStages);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kBulkStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], TS ? 1 : kBulkConsumerWarps);
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+  volatile uint32_t* st = status;
+  if (warp == kBulkConsumerWarps) {
+    if (lane != 0) return;
+    int k = 0;
+    for (long long it = blockIdx.x; it < total_items; it += gridDim.x, ++k) {
+      const int s = k % kBulkStages;
+      const uint32_t ph = (uint32_t)(k / kBulkStages) & 1u;
+      if (!mbar_wait(&empty[s], ph ^ 1u, st, DEV_TIMEOUT_EMPTY)) break;
+      const int oi = stream_find_op(table, count, it);
+      const auto& o = table[oi];
+      const int esz = o.in_dtype == 1 ? 2 : 4;
+      const long long e0 = (it - o.chunk_start) * (long long)o.tile;
+      const long long e1 = min(e0 + (long long)o.tile, o.n);
+      const uint32_t nb = (uint32_t)((e1 - e0) & ~7LL) * esz;  // a multiple of 8 elements: 16-byte multiples
+      uint8_t* slot = bulk_smem + s * kBulkSlot;
+      stage_op[s] = oi;  // published by the arrive below (release)
+      if (nb) {
+        mbar_arrive_expect_tx(&full[s], nb * (uint32_t)o.n_in);
+        for (int j = 0; j < o.n_in; ++j) {
+          uint8_t* dst = slot + (size_t)j * o.tile * esz;
+          const uint8_t* src = (const uint8_t*)o.in[j] + e0 * esz;
+          for (uint32_t off = 0; off < nb; off += piece)
+            bulk_load(dst + off, src + off, min(piece, nb - off), &full[s]);
+        }
+      } else {
+        mbar_arrive(&full[s]);
+      }
+    }
+    // copies issued but never consumed (only after an error) land before exit
+    if (*st != DEV_OK)
+      for (int q = (k > kBulkStages ? k - kBulkStages : 0); q < k; ++q)
+        mbar_drain(&full[q % kBulkStages], (uint32_t)(q / kBulkStages) & 1u);
+    return;
+  }
+  const int ctid = threadIdx.x;
+  int k = 0;
+  for (long long it = blockIdx.x; it < total_items; it += gridDim.x, ++k) {
+    const int s = k % kBulkStages;
+    const uint32_t ph = (uint32_t)(k / kBulkStages) & 1u;
+    if (!consumers_all(mbar_wait(&full[s], ph, st, DEV_TIMEOUT_FULL))) break;
+    const auto& o = table[stage_op[s]];
+    const int esz = o.in_dtype == 1 ? 2 : 4, osz = o.out_dtype == 1 ? 2 : 4;
+    const long long e0 = (it - o.chunk_start) * (long long)o.tile;
+    const long long e1 = min(e0 + (long long)o.tile, o.n);
+    const int cnt = (int)((e1 - e0) & ~7LL);
+    uint8_t* slot = bulk_smem + s * kBulkSlot;
+    switch (o.in_dtype * 2 + o.out_dtype) {
+      case 0: bulk_item<0, 0, TS>(o, slot, e0, cnt, e1, ctid); break;
+      case 1: bulk_item<0, 1, TS>(o, slot, e0, cnt, e1, ctid); break;
+      case 2: bulk_item<1, 0, TS>(o, slot, e0, cnt, e1, ctid); break;
+      default: bulk_item<1, 1, TS>(o, slot, e0, cnt, e1, ctid); break;
+    }
+    if constexpr (TS) {
+      fence_proxy_async_smem();  // this thread's output-tile writes, visible to the bulk store
+      consumer_sync();
+      if (ctid == 0) {
+        if (cnt) bulk_store((uint8_t*)o.out + e0 * osz, slot + (size_t)o.n_in * o.tile * esz, (uint32_t)cnt * osz);
+        bulk_commit();
+        // the previous item's store has finished reading its stage: hand it back
+        bulk_wait_read_1();
+        if (k > 0) mbar_arrive(&empty[(k - 1) % kBulkStages]);
+      }
+    } else {
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+    }
+  }
+  if (TS && ctid == 0) {
+    bulk_wait_read_all();
+    bulk_wait_all();  // output tiles written before the CTA ends
+  }
+}
+
+template <bool TS>
+__global__ void __launch_bounds__(kBulkThreads, 1) k_stream_bulk(const StreamOp* __restrict__ table, int count,
+                                                                  long long total_items, uint32_t* status,
+                                                                  uint32_t piece) {
+  stream_bulk_body<TS>(table, count, total_items, status, piece);
+}
+
+template <bool TS>
+__global__ void __launch_bounds__(kBulkThreads, 1) k_stream_bulk_inline(const __grid_constant__ StreamInline args,
+                                                                         int count, long long total_items,
+                                                                         uint32_t* status, uint32_t piece) {
+  stream_bulk_body<TS>(args.ops, count, total_items, status, piece);
 }
 
 }  // namespace bbx

@@ -98,6 +98,65 @@ class TcPlan:
             pass
 
 
+S_SUM, S_UNARY, S_BINARY, S_CAST = range(4)
+
+
+class StreamOp(C.Structure):
+    """bbx_stream_op_t: one add / n-ary reduce / elementwise / cast block op."""
+    _fields_ = [("kind", C.c_int), ("op", C.c_int), ("in_dtype", C.c_int), ("out_dtype", C.c_int),
+                ("n_in", C.c_int), ("kahan", C.c_int), ("n", C.c_longlong), ("inp", C.c_void_p * 16),
+                ("out", C.c_void_p), ("p0", C.c_float), ("p1", C.c_float)]
+
+
+def stream_op(kind, inputs, out, op=0, kahan=True, p0=0.0, p1=0.0, n=None):
+    """A StreamOp over flat tensors (all inputs of one dtype)."""
+    o = StreamOp()
+    o.kind, o.op, o.n_in, o.kahan = kind, op, len(inputs), int(kahan)
+    o.in_dtype, o.out_dtype = _dtype_code(inputs[0]), _dtype_code(out)
+    o.n = out.numel() if n is None else n
+    for j, t in enumerate(inputs):
+        o.inp[j] = t.data_ptr()
+    o.out = out.data_ptr()
+    o.p0, o.p1 = p0, p1
+    return o
+
+
+def stream_group(ops):
+    """One grouped launch (or one per 8 ops) of independent streaming ops."""
+    arr = (StreamOp * len(ops))(*ops)
+    check(lib.bbx_stream_group(C.cast(arr, C.c_void_p), len(ops), _stream()))
+
+
+class StreamPlan:
+    """A grouped streaming launch built once (op table on the device) and replayed."""
+
+    def __init__(self, ops):
+        arr = (StreamOp * len(ops))(*ops)
+        self.h = C.c_void_p()
+        check(lib.bbx_stream_plan_create(C.cast(arr, C.c_void_p), len(ops), C.byref(self.h)))
+
+    def launch(self, stream=None):
+        check(lib.bbx_stream_plan_launch(self.h, stream if stream is not None else _stream()))
+
+    @property
+    def bulk(self):
+        """True when the plan runs the bulk-staged (cp.async.bulk) kernel."""
+        r = lib.bbx_stream_plan_bulk(self.h)
+        check(min(r, 0))
+        return r == 1
+
+    def close(self):
+        if self.h:
+            check(lib.bbx_stream_plan_destroy(self.h))
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def add(a, b, c):
     check(lib.bbx_add_f32(_p(a), _p(b), _p(c), a.numel(), _stream()))
     return c

@@ -203,6 +203,21 @@ class Runtime:
         """Worker streams of the per-op path (1 = the plain single-stream path)."""
         check(lib.bbx_rt_set_workers(self.h, int(n)))
 
+    SPILL_FIELDS = ("evictions", "reloads", "d2h_bytes", "h2d_bytes", "file_write_bytes", "file_read_bytes",
+                    "clean_evictions", "resident_bytes", "peak_resident_bytes", "host_bytes")
+
+    def set_storage_budget(self, device_bytes, host_bytes=1 << 62, spill_file=None):
+        """Keep resident block payloads within `device_bytes` by spilling the
+        least recently used blocks to pinned host memory (up to `host_bytes`)
+        and then to `spill_file`. 0 removes the budget."""
+        check(lib.bbx_rt_set_storage_budget(self.h, int(device_bytes), int(host_bytes),
+                                            spill_file.encode() if spill_file else None))
+
+    def spill_stats(self):
+        out = (C.c_ulonglong * 10)()
+        check(lib.bbx_rt_spill_stats(self.h, out, 10))
+        return dict(zip(self.SPILL_FIELDS, [int(x) for x in out]))
+
     def set_hint_predictor(self, a, b):
         """Predicted latency exp(a ln(hint) + b) us from the uds' complexity hints."""
         check(lib.bbx_rt_set_hint_predictor(self.h, float(a), float(b)))

@@ -49,9 +49,10 @@ def parse():
                    help="skip the FP64 accuracy check (outside the timed region; for profiler launch lists)")
     p.add_argument("--grid", type=int, default=8,
                    help="blocks per side of A/B (8 = the full workload; smaller only for profiling captures)")
-    p.add_argument("--workload", default="cpmm", choices=["cpmm", "bmm", "ffnn", "dag", "learned"],
+    p.add_argument("--workload", default="cpmm", choices=["cpmm", "bmm", "ffnn", "dag", "learned", "spill"],
                    help="cpmm: the headline line (cross-product blocked matmul); bmm / dag / learned: the "
-                        "blocked matmul, random 2000-op DAG and learned-scheduling configurations")
+                        "blocked matmul, random 2000-op DAG and learned-scheduling configurations; spill: the "
+                        "2000-op DAG on the per-op path under device budgets below its footprint")
     p.add_argument("--n-ops", type=int, default=0, help="DAG size override (dag: 2000, learned: 5000)")
     p.add_argument("--train-dags", type=int, default=100, help="learned: DAGs recorded for the training set")
     return p.parse_args()
@@ -393,8 +394,8 @@ def run_dag_workload(args):
         elif args.workload == "ffnn":
             info = workloads.ffnn(rt, seed=seed, dtype=dtype)
         else:
-            n_ops = args.n_ops or (2000 if args.workload == "dag" else 5000)
-            hi = 2048 if args.workload == "dag" else 4096
+            n_ops = args.n_ops or (5000 if args.workload == "learned" else 2000)
+            hi = 4096 if args.workload == "learned" else 2048
             info = workloads.random_dag(rt, n_ops=n_ops, depth=8, seed=seed, dtype=dtype, hi=hi, **kw)
         torch.cuda.synchronize()
         return rt, info
@@ -450,6 +451,50 @@ def run_dag_workload(args):
                                                  for k in ("grouped_bf16", "grouped_fp32", "plain_fp32_per_op")},
                          "detail": result,
                          "gpu_launches": st["tc_launches"] + st["stream_launches"] + st["other_launches"]})
+        elif args.workload == "spill":
+            # per-op path (4 worker streams) with the whole DAG resident, then
+            # under device budgets of a half and a quarter of its peak footprint
+            rt, info = build("bf16", 7)
+            rt.set_workers(4)
+            rt.run()
+            res_ms = float(np.median([_time_on(rt.stream.value, rt.run, 1) for _ in range(3)]))
+            foot = rt.spill_stats()["peak_resident_bytes"]
+            sample = sorted(info["finals"])[:: max(1, len(info["finals"]) // 24)]
+            want = {t: rt.get_bytes(t) for t in sample}
+            flops = info["flops"]
+            legs = {}
+            for frac in (0.5, 0.25):
+                budget = int(foot * frac)
+                rt.set_storage_budget(budget)
+                rt.run()  # first run under the budget: pinned host buffers are allocated here
+                runs = []
+                for _ in range(3):
+                    s0 = rt.spill_stats()
+                    ms = _time_on(rt.stream.value, rt.run, 1)
+                    s1 = rt.spill_stats()
+                    runs.append((ms, {k: s1[k] - s0[k] for k in ("evictions", "reloads", "d2h_bytes", "h2d_bytes",
+                                                                  "clean_evictions")}))
+                runs.sort(key=lambda r: r[0])
+                ms, d = runs[1]
+                st = rt.spill_stats()
+                same = all(np.array_equal(rt.get_bytes(t), v) for t, v in want.items())
+                legs["budget_%g" % frac] = {
+                    "budget_bytes": budget, "ms": round(ms, 3), "tflops": round(flops / ms / 1e9, 2),
+                    "slowdown_vs_resident": round(ms / res_ms, 3), "per_run": d,
+                    "copy_gbs": round((d["d2h_bytes"] + d["h2d_bytes"]) / ms / 1e6, 1),
+                    "peak_resident_bytes": st["peak_resident_bytes"], "host_bytes": st["host_bytes"],
+                    "sampled_blocks_identical_to_resident": same}
+            rt.set_storage_budget(0)
+            rt.close()
+            ms = legs["budget_0.5"]["ms"]
+            value = flops / ms / 1e9
+            line.update({"metric": "block-op DAG TFLOP/s on the per-op path under a device budget (spill to host)",
+                         "value": round(value, 2), "unit": "TFLOP/s", "ms_per_step": ms, "dtype": "bf16",
+                         "config": {"workload": "random DAG, 2000 ops, depth 8, sizes 128..2048, bf16, per-op path "
+                                                "on 4 worker streams, device budget = 0.5 of its peak footprint",
+                                    "flops_per_step": flops, "footprint_bytes": foot},
+                         "makespan_ms": {"resident": round(res_ms, 3), **{k: v["ms"] for k, v in legs.items()}},
+                         "detail": legs, "gpu_launches": None})
         else:
             # learned scheduling: train the MLP on timings the runtime records itself
             t0 = time.perf_counter()

@@ -210,6 +210,10 @@ typedef struct bbx_stream_plan bbx_stream_plan_t;
 int bbx_stream_plan_create(const bbx_stream_op_t* ops, int count, bbx_stream_plan_t** out);
 int bbx_stream_plan_launch(bbx_stream_plan_t* plan, void* stream);
 int bbx_stream_plan_destroy(bbx_stream_plan_t* plan);
+/* 1 when the plan runs the bulk-staged kernel (every pointer of every op
+ * 16-byte aligned: inputs staged in shared memory by cp.async.bulk), 0 for
+ * the register kernel, negative on error. */
+int bbx_stream_plan_bulk(const bbx_stream_plan_t* plan);
 
 /* einsum contraction of the reference's "cutensor" plugin
  * (libraries/cutensor/contraction.h:25-63 params, :131-202 semantics):
@@ -274,7 +278,28 @@ int bbx_rt_tensor_put(bbx_rt_t* rt, int tid, const void* meta, const void* src, 
                       int src_on_device);
 /* Copies tensor `tid`'s meta (260 bytes) and up to `cap` payload bytes out. */
 int bbx_rt_tensor_get(bbx_rt_t* rt, int tid, void* meta_out, void* dst, size_t cap, int dst_on_device);
+/* Device address of tensor `tid`'s payload (copied back first if it was
+ * spilled). The caller may read or write it with work queued on the runtime
+ * stream; with a storage budget set the address stays valid until the next
+ * call that creates, reloads or runs commands. */
 int bbx_rt_tensor_payload(bbx_rt_t* rt, int tid, void** ptr, size_t* bytes);
+/* Storage budget with spill (nvme_storage_t(com, max_allocated, file),
+ * src/storage/nvme_storage.h:121-135; set_max_storage, nvme_storage.cc:270-280).
+ * Resident block payloads stay within device_bytes: the least recently used
+ * blocks no command holds are copied to pinned host memory (up to host_bytes)
+ * and past that to `spill_file` (truncated here, removed when the runtime is
+ * destroyed; NULL = no file tier), and copied back when a command reads them.
+ * A single command needing more than device_bytes fails, as the reference's
+ * "Can not process this." does. device_bytes 0 = no budget (every block is
+ * brought back). The per-op path (bbx_rt_run) spills; a compiled DAG holds
+ * every block resident while it lives. */
+int bbx_rt_set_storage_budget(bbx_rt_t* rt, unsigned long long device_bytes, unsigned long long host_bytes,
+                              const char* spill_file);
+/* Spill counters since the budget was set, in this order: evictions, reloads,
+ * D2H bytes, H2D bytes, file bytes written, file bytes read, evictions that
+ * needed no copy (a valid copy existed), resident bytes, peak resident bytes,
+ * pinned host bytes held by spilled copies. Writes min(n, 10) values. */
+int bbx_rt_spill_stats(bbx_rt_t* rt, unsigned long long* out, int n);
 int bbx_rt_tensor_count(bbx_rt_t* rt);
 int bbx_rt_tensor_remove(bbx_rt_t* rt, int tid);
 /* command_t::create_apply / create_reduce / create_delete (src/commands/command.h:228-457);

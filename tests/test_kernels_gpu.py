@@ -92,6 +92,119 @@ def test_reduce_in_place_alias(T):
     assert np.array_equal(host(d[0]), oracle.reduce_fold(ins))
 
 
+# ----------------------------------------------------------------- grouped streaming ops
+def _kahan_fold(ins):
+    """Compensated left fold in f32 arithmetic, in the kernels' order."""
+    a = ins[0].astype(np.float32).copy()
+    comp = np.zeros_like(a)
+    for b in ins[1:]:
+        y = (b - comp).astype(np.float32)
+        t = (a + y).astype(np.float32)
+        comp = ((t - a) - y).astype(np.float32)
+        a = t
+    return a
+
+
+def _stream_specs(seed, n_ops, sizes):
+    """Seeded batch of independent ops: sums of 1..16 inputs (Kahan on/off),
+    bit-exact unary / binary ops and casts, f32 or bf16 in and out."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n_ops):
+        kind = [0, 0, 0, 1, 2, 3][i % 6]
+        n = int(sizes[i % len(sizes)])
+        n_in = int(rng.integers(1, 17)) if kind == 0 else (2 if kind == 2 else 1)
+        idt, odt = int(rng.integers(0, 2)), int(rng.integers(0, 2))
+        if kind == 3:
+            odt = 1 - idt
+        op = int(rng.choice([0, 1, 5, 7, 8])) if kind == 1 else int(rng.integers(0, 7)) if kind == 2 else 0
+        xs = [rng.standard_normal(n).astype(np.float32) for _ in range(n_in)]
+        specs.append(dict(kind=kind, op=op, idt=idt, odt=odt, kahan=bool(rng.integers(0, 2)), xs=xs, n=n))
+    return specs
+
+
+def _stream_materialise(torch, ops, specs, offset):
+    """Device tensors for the specs, each starting `offset` elements into its
+    allocation (offset 1 breaks 16-byte alignment: the register kernel)."""
+    dt = {0: torch.float32, 1: torch.bfloat16}
+    keep, outs, sops = [], [], []
+    for sp in specs:
+        ins = []
+        for x in sp["xs"]:
+            buf = torch.empty(sp["n"] + 16, dtype=dt[sp["idt"]], device="cuda")
+            v = buf[offset:offset + sp["n"]]
+            v.copy_(torch.from_numpy(x).to(dt[sp["idt"]]))
+            keep.append(buf)
+            ins.append(v)
+        obuf = torch.full((sp["n"] + 16,), 7.0, dtype=dt[sp["odt"]], device="cuda")
+        out = obuf[offset:offset + sp["n"]]
+        keep.append(obuf)
+        outs.append((out, obuf))
+        sops.append(ops.stream_op(sp["kind"], ins, out, op=sp["op"], kahan=sp["kahan"], p0=0.3, p1=-1.7))
+    return keep, outs, sops
+
+
+def _stream_expect(torch, sp):
+    """CPU result of one spec: inputs rounded to the input dtype, math in f32,
+    result rounded to the output dtype."""
+    rnd = (lambda a: a) if sp["idt"] == 0 else bf16_round
+    xs = [rnd(x) for x in sp["xs"]]
+    if sp["kind"] == 0:
+        r = _kahan_fold(xs) if sp["kahan"] else oracle.reduce_fold(xs)
+    elif sp["kind"] == 1:
+        r = oracle.unary(sp["op"], xs[0], 0.3)
+    elif sp["kind"] == 2:
+        r = oracle.binary(sp["op"], xs[0], xs[1], 0.3, -1.7)
+    else:
+        r = xs[0]
+    return r if sp["odt"] == 0 else bf16_round(r)
+
+
+@pytest.mark.parametrize("sizes", [[1, 7, 8, 15, 64, 1000, 4099, 100003], [1024 * 1024, 1536 * 704, 129 * 131]])
+def test_stream_group_bulk_and_register_paths(T, sizes):
+    """The bulk-staged kernel (aligned pointers) and the register kernel
+    (pointers offset by one element) give bit-identical results, equal to the
+    CPU fold in the same order; bytes past each output stay untouched."""
+    torch, ops = T
+    specs = _stream_specs(len(sizes), 24, sizes)
+    got = {}
+    for offset in (0, 1):
+        keep, outs, sops = _stream_materialise(torch, ops, specs, offset)
+        plan = ops.StreamPlan(sops)
+        assert plan.bulk == (offset == 0)
+        plan.launch()
+        res = [host(o) for o, _ in outs]
+        guard = [host(b) for _, b in outs]
+        # the one-shot (inline) launches give the same bits
+        for o, _ in outs:
+            o.fill_(0)
+        ops.stream_group(sops)
+        assert all(np.array_equal(r, host(o)) for r, (o, _) in zip(res, outs))
+        for sp, g in zip(specs, guard):
+            assert np.all(g[:offset] == 7.0) and np.all(g[offset + sp["n"]:] == 7.0)
+        got[offset] = res
+        plan.close()
+        del keep
+    for sp, a, b in zip(specs, got[0], got[1]):
+        assert np.array_equal(a, b)
+        assert np.array_equal(a, _stream_expect(torch, sp))
+
+
+def test_stream_plan_many_items_replay(T):
+    """Hundreds of items per CTA (every stage of the ring reused many times),
+    replayed: results stay bit-exact against the CPU fold."""
+    torch, ops = T
+    specs = _stream_specs(77, 30, [1024 * 1024, 512 * 768 + 8, 333 * 1000])
+    keep, outs, sops = _stream_materialise(torch, ops, specs, 0)
+    plan = ops.StreamPlan(sops)
+    assert plan.bulk
+    for _ in range(3):
+        plan.launch()
+    for sp, (o, _) in zip(specs, outs):
+        assert np.array_equal(host(o), _stream_expect(torch, sp))
+    plan.close()
+
+
 # ----------------------------------------------------------------- elementwise
 @pytest.mark.parametrize("op", [0, 1, 5, 7, 8])
 def test_unary_bit_exact(T, op):

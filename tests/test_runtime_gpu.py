@@ -485,3 +485,91 @@ def test_dag_profile_accounts_for_the_work(R):
     assert all(g["ms"] > 0 for g in prof)
     for t, v in first.items():
         assert np.array_equal(dag.read_bytes(t, v.nbytes), v)
+
+
+# ----------------------------------------------------------------- spill tier
+def _spill_dag(workloads, rt, seed=44, dtype="bf16"):
+    return workloads.random_dag(rt, n_ops=150, depth=6, seed=seed, dtype=dtype, lo=128, hi=768, step=64,
+                                contraction_dims=(16, 64), mix=(0.45, 0.2, 0.2, 0.15), max_inputs=12)
+
+
+@pytest.mark.parametrize("workers,dtype", [(1, "bf16"), (4, "bf16"), (4, "f32")])
+def test_spill_to_host_matches_resident(R, workers, dtype):
+    """With a device budget of a third of the DAG's footprint, the per-op path
+    evicts least recently used blocks to pinned host memory and copies them
+    back when read: every result block is byte-identical to the fully resident
+    run, resident bytes never exceed the budget, and a second run reuses the
+    host copies of unchanged inputs (evictions without a copy)."""
+    runtime, workloads = R
+    rt1 = runtime.Runtime()
+    info = _spill_dag(workloads, rt1, dtype=dtype)
+    rt1.run()
+    want = {t: rt1.get_bytes(t) for t in info["finals"]}
+    foot = rt1.spill_stats()["peak_resident_bytes"]
+    rt1.close()
+    budget = foot // 3
+    rt2 = runtime.Runtime()
+    rt2.set_storage_budget(budget)
+    _spill_dag(workloads, rt2, dtype=dtype)
+    rt2.set_workers(workers)
+    for run in range(2):
+        rt2.run()
+        st = rt2.spill_stats()
+        assert st["evictions"] > 0 and st["reloads"] > 0 and st["d2h_bytes"] > 0 and st["h2d_bytes"] > 0
+        assert st["peak_resident_bytes"] <= budget
+        for t, v in want.items():
+            assert np.array_equal(rt2.get_bytes(t), v), (run, t)
+    assert rt2.spill_stats()["clean_evictions"] > 0
+    # the budget lifted: every block comes back, and the grouped path reads them in place
+    rt2.set_storage_budget(0)
+    dag = rt2.build_dag(runtime.HEURISTIC)
+    dag.launch()
+    for t, v in want.items():
+        assert np.array_equal(dag.read_bytes(t, v.nbytes), v), t
+    dag.close()
+    rt2.close()
+
+
+def test_spill_to_file_tier(R, tmp_path):
+    """Host budget too small for the spilled set: blocks go on to the spill
+    file (pwrite through a pinned staging buffer) and come back by pread,
+    byte-identical."""
+    runtime, workloads = R
+    rt1 = runtime.Runtime()
+    info = _spill_dag(workloads, rt1, seed=45)
+    rt1.run()
+    want = {t: rt1.get_bytes(t) for t in info["finals"]}
+    foot = rt1.spill_stats()["peak_resident_bytes"]
+    rt1.close()
+    rt2 = runtime.Runtime()
+    path = str(tmp_path / "spill.bin")
+    rt2.set_storage_budget(foot // 3, host_bytes=4 << 20, spill_file=path)
+    _spill_dag(workloads, rt2, seed=45)
+    rt2.run()
+    st = rt2.spill_stats()
+    assert st["file_write_bytes"] > 0 and st["file_read_bytes"] > 0 and st["host_bytes"] <= 4 << 20
+    for t, v in want.items():
+        assert np.array_equal(rt2.get_bytes(t), v), t
+    rt2.close()
+    import os
+    assert not os.path.exists(path)  # scratch file removed with the runtime
+
+
+def test_spill_budget_errors(R):
+    """A command needing more than the whole budget fails on the host with the
+    reference's condition (no GPU work is issued for it), and a compiled DAG
+    whose blocks cannot all be resident within the budget is refused."""
+    runtime, workloads = R
+    from bbts_b200._lib import BbxError
+    rt = runtime.Runtime()
+    info = workloads.bmm(rt, n=1024, split=2, dtype="f32", seed=3, host=False)
+    rt.set_storage_budget(3 << 20)  # one 512x512 f32 block is 1 MiB; a matmul holds three
+    with pytest.raises(BbxError, match="device budget"):
+        rt.build_dag(runtime.HEURISTIC)
+    rt.set_storage_budget(2 << 20)
+    with pytest.raises(BbxError, match="device budget"):
+        rt.run()
+    rt.set_storage_budget(0)
+    rt.run()
+    assert all(rt.get_bytes(t).size for t in info["C"].values())
+    rt.close()
