@@ -681,9 +681,9 @@ namespace bbx {
 // aligned. Work is dealt as items, one op's `tile` consecutive elements, with
 // `tile` sized per op so that every item moves about kBulkSlot bytes (inputs +
 // output) whatever its fan-in. One CTA per SM:
-//  - a producer thread copies each item's input tiles into a shared-memory
-//    stage with cp.async.bulk (kBulkStages stages, completion on the stage's
-//    `full` mbarrier);
+//  - a producer warp copies each item's input tiles into a shared-memory
+//    stage with cp.async.bulk, one lane per input (kBulkStages stages,
+//    completion on the stage's `full` mbarrier);
 //  - kBulkConsumerWarps warps fold them in the same order as the register
 //    paths above (bit-identical results), with the element function chosen
 //    once per item (with_unary / with_binary), and store the output with
@@ -852,12 +852,14 @@ __device__ __forceinline__ void stream_bulk_body(const TableT* table, int count,
   __syncthreads();
   volatile uint32_t* st = status;
   if (warp == kBulkConsumerWarps) {
-    if (lane != 0) return;
+    // producer warp: lane 0 owns the barriers, lane j issues input j's copies
     int k = 0;
     for (long long it = blockIdx.x; it < total_items; it += gridDim.x, ++k) {
       const int s = k % kBulkStages;
       const uint32_t ph = (uint32_t)(k / kBulkStages) & 1u;
-      if (!mbar_wait(&empty[s], ph ^ 1u, st, DEV_TIMEOUT_EMPTY)) break;
+      bool ok = true;
+      if (lane == 0) ok = mbar_wait(&empty[s], ph ^ 1u, st, DEV_TIMEOUT_EMPTY);
+      if (!__shfl_sync(0xffffffffu, ok, 0)) break;
       const int oi = stream_find_op(table, count, it);
       const auto& o = table[oi];
       const int esz = o.in_dtype == 1 ? 2 : 4;
@@ -865,21 +867,23 @@ __device__ __forceinline__ void stream_bulk_body(const TableT* table, int count,
       const long long e1 = min(e0 + (long long)o.tile, o.n);
       const uint32_t nb = (uint32_t)((e1 - e0) & ~7LL) * esz;  // a multiple of 8 elements: 16-byte multiples
       uint8_t* slot = bulk_smem + s * kBulkSlot;
-      stage_op[s] = oi;  // published by the arrive below (release)
+      if (lane == 0) {
+        stage_op[s] = oi;  // published by the arrive below (release)
+        if (nb) mbar_arrive_expect_tx(&full[s], nb * (uint32_t)o.n_in);
+        else mbar_arrive(&full[s]);
+      }
+      __syncwarp();  // the expected bytes are registered before any copy is issued
       if (nb) {
-        mbar_arrive_expect_tx(&full[s], nb * (uint32_t)o.n_in);
-        for (int j = 0; j < o.n_in; ++j) {
+        for (int j = lane; j < o.n_in; j += 32) {
           uint8_t* dst = slot + (size_t)j * o.tile * esz;
           const uint8_t* src = (const uint8_t*)o.in[j] + e0 * esz;
           for (uint32_t off = 0; off < nb; off += piece)
             bulk_load(dst + off, src + off, min(piece, nb - off), &full[s]);
         }
-      } else {
-        mbar_arrive(&full[s]);
       }
     }
     // copies issued but never consumed (only after an error) land before exit
-    if (*st != DEV_OK)
+    if (lane == 0 && *st != DEV_OK)
       for (int q = (k > kBulkStages ? k - kBulkStages : 0); q < k; ++q)
         mbar_drain(&full[q % kBulkStages], (uint32_t)(q / kBulkStages) & 1u);
     return;
