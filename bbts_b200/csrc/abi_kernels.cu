@@ -156,7 +156,7 @@ static int get_encode_fn(EncodeTiledFn* fn) {
 // 2-D map over a row-major matrix with `rows` rows of `cols` elements and pitch
 // `ld` elements; box = box_cols x box_rows, 128-byte swizzle, zero OOB fill.
 static int make_map(CUtensorMap* map, const void* base, int dtype, long long rows, long long cols,
-                    long long ld, int box_cols, int box_rows) {
+                    long long ld, int box_cols, int box_rows, bool swizzle = true) {
   EncodeTiledFn enc;
   int rc = get_encode_fn(&enc);
   if (rc) return rc;
@@ -169,7 +169,7 @@ static int make_map(CUtensorMap* map, const void* base, int dtype, long long row
   cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = enc(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS)
     return set_error(BBX_ERR_INVALID,
@@ -248,7 +248,8 @@ static int build_problem(int in_dtype, const bbx_tc_problem_t& q, int bn_code, T
     rc = make_map(&out->tmap_b, q.b, in_dtype, q.k, q.n, q.ldb, mnbox, bk);
   }
   if (rc) return rc;
-  if (q.ldc < q.n) return set_error(BBX_ERR_INVALID, "ldc < n");
+  const bool c_col = (q.flags & BBX_EPI_C_COLMAJOR) != 0;
+  if (q.ldc < (c_col ? q.m : q.n)) return set_error(BBX_ERR_INVALID, c_col ? "ldc < m" : "ldc < n");
   if ((q.flags & BBX_EPI_BIAS) && !q.bias) return set_error(BBX_ERR_INVALID, "bias flag without bias");
   out->c = q.c;
   out->bias = q.bias;
@@ -261,11 +262,30 @@ static int build_problem(int in_dtype, const bbx_tc_problem_t& q, int bn_code, T
   out->alpha = q.alpha;
   out->beta = q.beta;
   out->flags = q.flags & (EPI_RELU | EPI_OUT_BF16 | EPI_BIAS | EPI_BETA);
-  // C through TMA stores when its base and pitch meet the 16-byte rules and the
-  // epilogue does not read C: 32-row boxes of 128 bytes (32 f32 / 64 bf16)
   const bool c_bf16 = (out->flags & EPI_OUT_BF16) != 0;
   const int c_esz = c_bf16 ? 2 : 4;
-  if (!(out->flags & EPI_BETA) && (((uintptr_t)q.c) & 15) == 0 && ((q.ldc * c_esz) & 15) == 0) {
+  if (c_col) {
+    // column-major C: stored n rows of m. With the 16-byte rules met, each
+    // epilogue warp stores its 32 rows of C as TMA boxes of 32 columns x 32
+    // m-elements (no swizzle); otherwise by coalesced stores from registers.
+    if (out->flags & EPI_BETA) return set_error(BBX_ERR_UNSUPPORTED, "column-major C with beta");
+    out->flags |= EPI_C_TRANS;
+    if ((((uintptr_t)q.c) & 15) == 0 && ((q.ldc * c_esz) & 15) == 0 && ((q.m * c_esz) & 15) == 0) {
+      rc = make_map(&out->tmap_c, q.c, c_bf16 ? BBX_BF16 : BBX_F32, q.n, q.m, q.ldc, 32, 32, false);
+      if (rc) return rc;
+      out->flags |= EPI_TMA_STORE;
+    }
+    return BBX_OK;
+  }
+  // C through TMA stores when its base, pitch and row length meet the 16-byte
+  // rules and the epilogue does not read C: 32-row boxes of 128 bytes (32 f32 /
+  // 64 bf16). A TMA store clips the box at the tensor's edge in whole 16-byte
+  // pieces of a row (measured: with m = 1031 f32 rows stored column-major,
+  // element 1031 of a 16-byte piece holding 1028..1031 was written), so a row
+  // length that is not a multiple of 16 bytes would write into the pitch
+  // padding: such C goes through the staged stores.
+  if (!(out->flags & EPI_BETA) && (((uintptr_t)q.c) & 15) == 0 && ((q.ldc * c_esz) & 15) == 0 &&
+      ((q.n * c_esz) & 15) == 0) {
     rc = make_map(&out->tmap_c, q.c, c_bf16 ? BBX_BF16 : BBX_F32, q.m, q.n, q.ldc, 128 / c_esz, 32);
     if (rc) return rc;
     out->flags |= EPI_TMA_STORE;

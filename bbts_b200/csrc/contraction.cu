@@ -381,31 +381,34 @@ int lower_contraction(int rank_l, const long long* dims_l, const int* modes_l, i
 
 ContractionGemm contraction_gemm(const ContractionLowering& L, const void* lc, const void* rc, void* ct, long long b) {
   ContractionGemm g{};
-  const char* l = (const char*)lc;
-  const char* r = (const char*)rc;
-  if (L.rc_mn) {  // Rc[b][k][n]: A stored k x n, MN-major
-    g.a = r + 2 * b * L.kdim * L.pn;
-    g.trans_a = 1;
-    g.lda = L.pn;
-  } else {        // Rc[b][n][k]: A stored n x k, K-major
-    g.a = r + 2 * b * L.nn * L.pk;
-    g.trans_a = 0;
-    g.lda = L.pk;
-  }
-  if (L.lc_mn) {  // Lc[b][k][m]: op(B) = k x m stored as is
-    g.b = l + 2 * b * L.kdim * L.pm;
-    g.trans_b = 0;
-    g.ldb = L.pm;
-  } else {        // Lc[b][m][k]: B stored m x k, transposed
-    g.b = l + 2 * b * L.nm * L.pk;
-    g.trans_b = 1;
-    g.ldb = L.pk;
-  }
+  const char* lb = (const char*)lc + 2 * b * (L.lc_mn ? L.kdim * L.pm : L.nm * L.pk);  // this batch's Lc
+  const char* rb = (const char*)rc + 2 * b * (L.rc_mn ? L.kdim * L.pn : L.nn * L.pk);  // this batch's Rc
   g.c = (char*)ct + 4 * b * L.nn * L.nm;
-  g.m = (int)L.nn;
-  g.n = (int)L.nm;
   g.k = (int)L.kdim;
   g.ldc = L.nm;
+  if (L.nm > L.nn) {
+    // A = Lc (m = nm), B = Rc (n = nn), C column-major
+    g.a = lb;
+    g.trans_a = L.lc_mn ? 1 : 0;  // Lc[k][m]: MN-major; Lc[m][k]: K-major
+    g.lda = L.lc_mn ? L.pm : L.pk;
+    g.b = rb;
+    g.trans_b = L.rc_mn ? 0 : 1;  // Rc[k][n]: op(B) stored as is; Rc[n][k]: transposed
+    g.ldb = L.rc_mn ? L.pn : L.pk;
+    g.m = (int)L.nm;
+    g.n = (int)L.nn;
+    g.flags = BBX_EPI_C_COLMAJOR;
+    return g;
+  }
+  // A = Rc (m = nn), B = Lc (n = nm), C row-major
+  g.a = rb;
+  g.trans_a = L.rc_mn ? 1 : 0;  // Rc[k][n]: A stored k x n, MN-major; Rc[n][k]: K-major
+  g.lda = L.rc_mn ? L.pn : L.pk;
+  g.b = lb;
+  g.trans_b = L.lc_mn ? 0 : 1;  // Lc[k][m]: op(B) = k x m stored as is; Lc[m][k]: transposed
+  g.ldb = L.lc_mn ? L.pm : L.pk;
+  g.m = (int)L.nn;
+  g.n = (int)L.nm;
+  g.flags = 0;
   return g;
 }
 
@@ -503,6 +506,7 @@ extern "C" int bbx_contraction(const float* lhs, int rank_l, const long long* di
         q.m = g.m; q.n = g.n; q.k = g.k;
         q.trans_a = g.trans_a; q.trans_b = g.trans_b;
         q.lda = g.lda; q.ldb = g.ldb; q.ldc = g.ldc;
+        q.flags = g.flags;
         q.alpha = alpha; q.beta = 0.f;
       }
       rc = bbx_matmul_tc(BBX_BF16, probs.data(), (int)L.nb, 0, stream);

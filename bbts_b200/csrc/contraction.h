@@ -34,12 +34,16 @@ struct ContractionLowering {
 };
 
 // The batched GEMM of a bf16 lowering as tensor-core problem fields for batch
-// b: A = Rc (rows n), B = Lc (columns m), C = Ct[b] (f32, ldc = nm).
+// b. C = Ct[b] holds the output n-major (f32, element (m, n) at m + n * nm).
+// When nm > nn the GEMM is M = nm, N = nn with A = Lc, B = Rc and a
+// column-major C (BBX_EPI_C_COLMAJOR), so the long dimension fills the
+// 128-row tiles; otherwise M = nn, N = nm with A = Rc, B = Lc and C row-major
+// with ldc = nm.
 struct ContractionGemm {
   const void* a;
   const void* b;
   void* c;
-  int m, n, k, trans_a, trans_b;
+  int m, n, k, trans_a, trans_b, flags;
   long long lda, ldb, ldc;
 };
 ContractionGemm contraction_gemm(const ContractionLowering& L, const void* lc, const void* rc, void* ct, long long b);

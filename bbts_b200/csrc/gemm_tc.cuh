@@ -34,6 +34,8 @@ enum : int {
   EPI_BIAS = 4,      // add bias[col]
   EPI_BETA = 8,      // read C and add beta * C
   EPI_TMA_STORE = 16,  // set by the host: C is written by TMA stores through tmap_c
+  EPI_C_TRANS = 32,    // C is column-major: with EPI_TMA_STORE through tmap_c (boxes of 32 columns x 32
+                       // rows of C), else by coalesced stores from registers
 };
 
 // One block product. 64-byte alignment is required by the tensor maps.
@@ -162,6 +164,46 @@ __device__ __forceinline__ void tc_epi_rows(const TcProblem* pr, uint32_t t_row,
   const bool has_bias = (flags & EPI_BIAS) != 0;
   const bool has_beta = (flags & EPI_BETA) != 0;
   const bool relu = (flags & EPI_RELU) != 0;
+  if (flags & EPI_C_TRANS) {
+    // column-major C without TMA stores: lane l holds row row0 + l, so for each
+    // column the warp's 32 stores go to consecutive addresses (coalesced)
+    const bool bf16 = (flags & EPI_OUT_BF16) != 0;
+    const int row = row0 + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 32) {
+      const int col = col_base + c0;
+      if (col >= n || row0 >= m) break;  // warp-uniform
+      uint32_t r0[16], r1[16];
+      tmem_ld16_nowait(t_row + c0, r0);
+      tmem_ld16_nowait(t_row + c0 + 16, r1);
+      tmem_ld_wait();
+      float v[32];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        v[i] = __uint_as_float(r0[i]) * alpha;
+        v[16 + i] = __uint_as_float(r1[i]) * alpha;
+      }
+      if (has_bias) {
+#pragma unroll
+        for (int i = 0; i < 32; ++i)
+          if (col + i < n) v[i] += pr->bias[col + i];
+      }
+      if (relu) {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) v[i] = fmaxf(v[i], 0.f);
+      }
+      if (row < m) {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+          if (col + i >= n) break;
+          const long long idx = (long long)row + (long long)(col + i) * ldc;
+          if (bf16) ((__nv_bfloat16*)pr->c)[idx] = __float2bfloat16_rn(v[i]);
+          else ((float*)pr->c)[idx] = v[i];
+        }
+      }
+    }
+    return;
+  }
   float* srow = stage + lane * kTcEpiPitch;
   // the buffer shares its slot with the TMA-store box of earlier tiles (a group
   // can mix problems with and without TMA stores): let those stores read it first
@@ -268,8 +310,12 @@ __device__ __forceinline__ void tc_epi_rows(const TcProblem* pr, uint32_t t_row,
 // values from TMEM, applies alpha, bias and ReLU, converts, and writes its 128
 // bytes into the warp's box with the 128-byte swizzle (16-byte chunk j of row r
 // at chunk j ^ (r & 7): conflict-free); one lane then issues the TMA store of
-// the 32 x 128-byte box, which clips rows >= m and columns >= n. The box is
-// rewritten only after the previous store has read it.
+// the 32 x 128-byte box, which clips rows >= m and columns >= n (the host
+// takes this path only when a row of C is a whole number of 16-byte pieces,
+// the granularity of the clip). The box is rewritten only after the previous
+// store has read it. With EPI_C_TRANS (column-major C) the box is 32 columns x
+// the warp's 32 rows, unswizzled, and m is the dimension a whole number of
+// 16-byte pieces.
 template <int BN>
 __device__ __forceinline__ void tc_epi_rows_tma(const TcProblem* pr, uint32_t t_row, int row0, int lane,
                                                 uint8_t* box, int col_base) {
@@ -282,6 +328,50 @@ __device__ __forceinline__ void tc_epi_rows_tma(const TcProblem* pr, uint32_t t_
   const int step = bf16 ? 64 : 32;  // columns per 128-byte row of the box
   uint8_t* myrow = box + lane * 128;
   if (row0 >= pr->m) return;  // warp-uniform: this warp's rows are all past the matrix, no box to store
+  if (flags & EPI_C_TRANS) {
+    // column-major C: per 32 columns, the box holds column c's 32 rows (this
+    // warp's) contiguously; lane l writes element l of every box row
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 32) {
+      const int col = col_base + c0;
+      if (col >= n) break;  // warp-uniform
+      uint32_t r0[16], r1[16];
+      tmem_ld16_nowait(t_row + c0, r0);
+      tmem_ld16_nowait(t_row + c0 + 16, r1);
+      tmem_ld_wait();
+      float v[32];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        v[i] = __uint_as_float(r0[i]) * alpha;
+        v[16 + i] = __uint_as_float(r1[i]) * alpha;
+      }
+      if (has_bias) {
+#pragma unroll
+        for (int i = 0; i < 32; ++i)
+          if (col + i < n) v[i] += pr->bias[col + i];
+      }
+      if (relu) {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) v[i] = fmaxf(v[i], 0.f);
+      }
+      if (lane == 0) bulk_wait_read_all();  // the previous store has read the box
+      __syncwarp();
+      if (bf16) {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) ((__nv_bfloat16*)box)[i * 32 + lane] = __float2bfloat16_rn(v[i]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) ((float*)box)[i * 32 + lane] = v[i];
+      }
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) {
+        tma_store_2d(&pr->tmap_c, box, row0, col);
+        bulk_commit();
+      }
+    }
+    return;
+  }
 #pragma unroll 1
   for (int c0 = 0; c0 < BN; c0 += step) {
     const int col = col_base + c0;

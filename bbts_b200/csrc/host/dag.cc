@@ -190,14 +190,15 @@ bool g_tune_loaded = false;
 
 std::string tune_key(int dtype, bool ta, bool tb, const std::vector<bbx_tc_problem_t>& ps) {
   double fl = 0;
-  int maxn = 0, maxm = 0;
+  int maxn = 0, maxm = 0, ccol = 0;
   for (auto& q : ps) {
     fl += 2.0 * q.m * q.n * (double)q.k;
     maxn = std::max(maxn, q.n);
     maxm = std::max(maxm, q.m);
+    ccol |= (q.flags & BBX_EPI_C_COLMAJOR) ? 1 : 0;
   }
   char buf[128];
-  std::snprintf(buf, sizeof(buf), "d%d_a%d_b%d_p%d_f%d_n%d_m%d", dtype, (int)ta, (int)tb,
+  std::snprintf(buf, sizeof(buf), "d%d_a%d_b%d_c%d_p%d_f%d_n%d_m%d", dtype, (int)ta, (int)tb, ccol,
                 (int)std::ceil(std::log2((double)ps.size() + 1)), (int)std::log2(fl + 1), (int)std::log2(maxn + 1),
                 (int)std::log2(maxm + 1));
   return buf;
@@ -573,7 +574,9 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
           // A = Rc, B = Lc in their staging layouts. Contraction problems get
           // groups of their own (key bit 8): they wait for the wave's gathers,
           // while the matmul groups can start as soon as their inputs exist
-          const int key = 256 + ELEM_BF16 * 4 + (L.rc_mn ? 2 : 0) + (L.lc_mn ? 0 : 1);
+          // operand layouts (hence the kernel variant) depend on the GEMM's orientation
+          const bbx::ContractionGemm g0 = bbx::contraction_gemm(L, tl.payload, tr.payload, C, 0);
+          const int key = 256 + ELEM_BF16 * 4 + (g0.trans_a ? 2 : 0) + (g0.trans_b ? 1 : 0);
           for (long long b = 0; b < L.nb; ++b) {
             const bbx::ContractionGemm g = bbx::contraction_gemm(L, tl.payload, tr.payload, C, b);
             bbx_tc_problem_t q{};
@@ -581,6 +584,7 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
             q.m = g.m; q.n = g.n; q.k = g.k;
             q.trans_a = g.trans_a; q.trans_b = g.trans_b;
             q.lda = g.lda; q.ldb = g.ldb; q.ldc = g.ldc;
+            q.flags = g.flags;
             q.alpha = cs.p.alpha;
             tc_groups[key].push_back(q);
           }

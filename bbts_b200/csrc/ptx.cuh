@@ -171,7 +171,9 @@ __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.
 
 // 2-D tiled TMA store from this CTA's shared memory (bulk-group completion).
 // The box's innermost coordinate x keeps x * elem_size % 16 == 0 and neither
-// coordinate is negative; parts of the box outside the tensor are not written.
+// coordinate is negative. Parts of the box outside the tensor are not written,
+// at the granularity of 16-byte pieces of the innermost dimension: a piece
+// that holds any in-bounds element is written whole.
 __device__ __forceinline__ void tma_store_2d(const void* tmap, const void* smem_src, int32_t x, int32_t y) {
   asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%2, %3}], [%1];" ::"l"(tmap),
                "r"(smem_u32(smem_src)), "r"(x), "r"(y)

@@ -10,7 +10,7 @@ from ._lib import lib, check, TcProblem
 F32, BF16, E4M3 = 0, 1, 2
 U_RELU, U_RELU_DIF, U_SIGMOID_REF, U_SIGMOID, U_EXP, U_SQUARE, U_SQRT, U_ADD_SCALAR, U_SCALE = range(9)
 B_ADD, B_WEIGHTED, B_HADAMARD, B_MAX, B_MIN, B_SUB, B_DIV = range(7)
-EPI_RELU, EPI_OUT_BF16, EPI_BIAS, EPI_BETA = 1, 2, 4, 8
+EPI_RELU, EPI_OUT_BF16, EPI_BIAS, EPI_BETA, EPI_C_COLMAJOR = 1, 2, 4, 8, 32
 
 
 def _stream():
@@ -42,13 +42,16 @@ def matmul_f32(a, b, c, trans_a=False, trans_b=False, alpha=1.0, beta=0.0, bias=
     return c
 
 
-def tc_problem(a, b, c, trans_a=False, trans_b=False, alpha=1.0, beta=0.0, bias=None, relu=False):
+def tc_problem(a, b, c, trans_a=False, trans_b=False, alpha=1.0, beta=0.0, bias=None, relu=False,
+               c_colmajor=False):
+    """c_colmajor: c holds C column-major, i.e. the n x m tensor C^T row-major."""
     import torch
     m = a.shape[1] if trans_a else a.shape[0]
     k = a.shape[0] if trans_a else a.shape[1]
     n = b.shape[0] if trans_b else b.shape[1]
     flags = (EPI_RELU if relu else 0) | (EPI_BIAS if bias is not None else 0) | \
-            (EPI_BETA if beta != 0.0 else 0) | (EPI_OUT_BF16 if c.dtype == torch.bfloat16 else 0)
+            (EPI_BETA if beta != 0.0 else 0) | (EPI_OUT_BF16 if c.dtype == torch.bfloat16 else 0) | \
+            (EPI_C_COLMAJOR if c_colmajor else 0)
     return TcProblem(a.data_ptr(), b.data_ptr(), c.data_ptr(), bias.data_ptr() if bias is not None else None,
                      m, n, k, int(trans_a), int(trans_b), flags, a.stride(0), b.stride(0), c.stride(0),
                      alpha, beta)

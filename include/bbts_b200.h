@@ -68,6 +68,9 @@ extern "C" {
 #define BBX_EPI_OUT_BF16 2
 #define BBX_EPI_BIAS 4
 #define BBX_EPI_BETA 8
+/* tensor-core problems only: C is column-major, element (i, j) at
+ * c[i + j * ldc] (ldc >= m); not with BBX_EPI_BETA (BBX_ERR_UNSUPPORTED) */
+#define BBX_EPI_C_COLMAJOR 32
 
 /* ------------------------------------------------------------------ misc */
 const char* bbx_version(void);

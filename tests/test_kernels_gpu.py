@@ -592,3 +592,112 @@ def test_matmul_tc_mixed_store_paths(T, tile_n):
         for i, ref in enumerate(refs):
             assert rel_err(host(keep[3 * i + 2]), ref) <= 1e-5, i
     plan.close()
+
+
+@pytest.mark.parametrize("tile_n", [128, 256, 512])
+@pytest.mark.parametrize("out_bf16", [False, True])
+def test_matmul_tc_c_colmajor(T, tile_n, out_bf16):
+    """Column-major C (BBX_EPI_C_COLMAJOR, the contraction lowering's skinny
+    GEMMs), on the TMA-store path: integer-valued inputs make the f32
+    accumulation exact, so every problem equals the int64 product, transposed
+    in memory, and matches the row-major store of the same group bit for bit.
+    Problems mix ragged m, n from 32 to 264, both layouts of A, and bias / relu
+    epilogues; the 8 elements of pitch padding stay untouched."""
+    torch, ops = T
+    rng = np.random.default_rng(51 + tile_n)
+    odt = torch.bfloat16 if out_bf16 else torch.float32
+    col, row, keep, refs = [], [], [], []
+    for i in range(36):
+        m = int(rng.choice([40, 128, 200, 264, 520, 1032]))
+        n = int(rng.choice([32, 64, 96, 200, 256, 264]))
+        k = int(rng.choice([32, 64, 128, 192]))
+        a = rng.integers(-3, 4, (m, k)).astype(np.float32)
+        b = rng.integers(-3, 4, (k, n)).astype(np.float32)
+        bias = rng.integers(-8, 9, n).astype(np.float32) if i % 3 == 0 else None
+        relu = i % 4 == 1
+        ta = i % 2 == 1
+        mp = m + 8  # pitches along m: 16-byte multiples, with 8 elements of padding to watch
+        if ta:  # A stored k x m (MN-major) with pitch mp
+            A = torch.zeros(k, mp, dtype=torch.bfloat16, device="cuda")
+            A[:, :m] = dev(torch, a.T.copy(), torch.bfloat16)
+            A = A[:, :m]
+        else:
+            A = dev(torch, a, torch.bfloat16)
+        B = dev(torch, b, torch.bfloat16)
+        cbuf = torch.full((n, mp), float("nan"), dtype=odt, device="cuda")
+        cc = cbuf[:, :m]
+        cr = torch.full((m, n + (8 - n % 8) % 8), float("nan"), dtype=odt, device="cuda")[:, :n]
+        bt = dev(torch, bias) if bias is not None else None
+        keep += [A, B, cbuf, cc, cr, bt]
+        col.append(ops.tc_problem(A, B, cc, trans_a=ta, bias=bt, relu=relu, c_colmajor=True))
+        row.append(ops.tc_problem(A, B, cr, trans_a=ta, bias=bt, relu=relu))
+        r = a.astype(np.int64) @ b.astype(np.int64)
+        if bias is not None:
+            r = r + bias.astype(np.int64)[None, :]
+        if relu:
+            r = np.maximum(r, 0)
+        refs.append(r.astype(np.float64))
+    for group in (col, row):
+        by_layout = {}
+        for i, q in enumerate(group):
+            by_layout.setdefault(q.trans_a, []).append(i)
+        for idx in by_layout.values():
+            plan = ops.TcPlan([group[i] for i in idx], tile_n=tile_n)
+            plan.launch()
+            plan.close()
+    for i, ref in enumerate(refs):
+        cc, cr = keep[6 * i + 3], keep[6 * i + 4]
+        got_c, got_r = host(cc), host(cr)
+        want = bf16_round(ref) if out_bf16 else ref
+        assert np.array_equal(got_c.T, want), i
+        assert np.array_equal(got_c.T, got_r), i
+        pad = host(keep[6 * i + 2])[:, cc.shape[1]:]
+        assert np.all(np.isnan(pad)), i  # pitch padding untouched
+
+
+def test_matmul_tc_padded_pitch_untouched(T):
+    """C rows whose length is not a whole number of 16-byte pieces, inside a
+    padded pitch: the epilogue must not write the padding (TMA stores clip in
+    16-byte pieces, so such C takes the staged stores); column-major C of such
+    a length goes through stores from registers, exact, padding untouched."""
+    torch, ops = T
+    from bbts_b200._lib import BbxError
+    rng = np.random.default_rng(61)
+    cases = [(300, 510, torch.float32), (300, 500, torch.bfloat16), (300, 504, torch.bfloat16),
+             (131, 508, torch.float32)]
+    for m, n, odt in cases:
+        k = 128
+        a = rng.integers(-3, 4, (m, k)).astype(np.float32)
+        b = rng.integers(-3, 4, (k, n)).astype(np.float32)
+        A = dev(torch, a, torch.bfloat16)
+        Bp = torch.zeros(k, 512, dtype=torch.bfloat16, device="cuda")
+        Bp[:, :n] = dev(torch, b, torch.bfloat16)
+        cbuf = torch.full((m, 512), float("nan"), dtype=odt, device="cuda")
+        c = cbuf[:, :n]
+        plan = ops.TcPlan([ops.tc_problem(A, Bp[:, :n], c)], tile_n=256)
+        plan.launch()
+        plan.close()
+        ref = a.astype(np.int64) @ b.astype(np.int64)
+        want = bf16_round(ref.astype(np.float32)) if odt == torch.bfloat16 else ref
+        got = host(cbuf)
+        assert np.array_equal(got[:, :n], want), (m, n)
+        assert np.all(np.isnan(got[:, n:])), (m, n)
+    for m, n, ldc, odt in [(1031, 64, 1040, torch.float32), (1031, 96, 1031, torch.float32),
+                           (333, 200, 340, torch.bfloat16), (77, 40, 77, torch.bfloat16)]:
+        a = rng.integers(-3, 4, (m, 64)).astype(np.float32)
+        b = rng.integers(-3, 4, (64, n)).astype(np.float32)
+        A, B = dev(torch, a, torch.bfloat16), dev(torch, b, torch.bfloat16)
+        cbuf = torch.full((n, ldc), float("nan"), dtype=odt, device="cuda")
+        for tile in (128, 256, 512):
+            cbuf.fill_(float("nan"))
+            plan = ops.TcPlan([ops.tc_problem(A, B, cbuf[:, :m], c_colmajor=True)], tile_n=tile)
+            plan.launch()
+            plan.close()
+            ref = a.astype(np.int64) @ b.astype(np.int64)
+            want = bf16_round(ref.astype(np.float32)) if odt == torch.bfloat16 else ref
+            got = host(cbuf)
+            assert np.array_equal(got[:, :m].T, want), (m, n, ldc, tile)
+            assert np.all(np.isnan(got[:, m:])), (m, n, ldc, tile)
+    cf = torch.empty(40, 77, device="cuda")
+    with pytest.raises(BbxError, match="beta"):
+        ops.matmul_tc([ops.tc_problem(A, B, cf, beta=1.0, c_colmajor=True)])
