@@ -42,7 +42,8 @@ def parse():
     p.add_argument("--steps", type=int, default=30)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--tile-n", type=int, default=0)
+    p.add_argument("--tile-n", type=int, default=0,
+                   help="tensor-core tile (128, 256, 512); 0 = automatic (cpmm) / autotuned (DAG workloads)")
     p.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparator leg")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-accuracy", action="store_true",
@@ -405,7 +406,7 @@ def run_dag_workload(args):
         if args.workload in ("bmm", "dag", "ffnn"):
             # fast path: bf16 blocks, grouped + graph, autotuned tiles, heuristic and learned-free policy
             rt, info = build("bf16", 7)
-            dag = rt.build_dag(runtime.HEURISTIC, tile_n=-1)
+            dag = rt.build_dag(runtime.HEURISTIC, tile_n=args.tile_n or -1)
             st = dag.stats()
             for _ in range(args.warmup):
                 dag.launch()
@@ -427,7 +428,7 @@ def run_dag_workload(args):
             rt.close()
             # the FP32 variant through the grouped graph path
             rt, info32 = build("f32", 7)
-            dag = rt.build_dag(runtime.HEURISTIC, tile_n=-1)
+            dag = rt.build_dag(runtime.HEURISTIC, tile_n=args.tile_n or -1)
             for _ in range(args.warmup):
                 dag.launch()
             gms = _time_on(rt.stream.value, dag.launch, max(1, min(5, args.steps)))
