@@ -591,6 +591,18 @@ int bbx_cast(int src_dtype, const void* in, int dst_dtype, void* out, long long 
   return BBX_OK;
 }
 
+int bbx_relu_split(const float* z, void* hi, void* lo, long long n, void* stream) {
+  if (!z || !hi || !lo || n < 0) return set_error(BBX_ERR_INVALID, "bad relu_split arguments");
+  if (n == 0) return BBX_OK;
+  DeviceState* d;
+  int rc = device_state(&d);
+  if (rc) return rc;
+  k_relu_split<<<grid_for((n + 3) / 4, 256, d->sms), 256, 0, (cudaStream_t)stream>>>(
+      z, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo, n);
+  BBX_CHECK_LAUNCH("relu_split");
+  return BBX_OK;
+}
+
 int bbx_quantize_e4m3(int src_dtype, const void* in, void* out, int rows, int cols, int transpose,
                       float* scale_out, void* stream) {
   if (!in || !out || !scale_out || rows <= 0 || cols <= 0) return set_error(BBX_ERR_INVALID, "bad quantize arguments");

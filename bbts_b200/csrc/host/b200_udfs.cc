@@ -313,6 +313,32 @@ void register_b200_udfs(udf_manager_t& udm) {
       },
       ew_hint, same_meta));
 
+  // relu of an f32 block split into hi = bf16(relu(z)) and lo = bf16(relu(z) - hi)
+  // (new ud, no reference counterpart): the activation of a layer followed by
+  // another ReLU layer, whose masks would flip on a bf16-rounded operand; the
+  // next layer multiplies both parts and sums them in f32. (The impl name does
+  // not start with "b200_dense_relu": the DAG executor runs it through its fn,
+  // not as a one-output streaming relu.)
+  register_ud(udm, "matrix_relu_split", false, false, 1, 2);
+  add_impl(udm, std::make_unique<b200_impl_t>(
+      "b200_dense_split_relu", "matrix_relu_split", V{"dense"}, V{"dense_bf16", "dense_bf16"},
+      std::vector<int32_t>{},
+      [](const params_t& p, const targs_t& in, targs_t& out) {
+        auto& z = in.get<0>().as<dense_tensor_t>();
+        auto& hi = out.get<0>().as<dense_tensor_t>();
+        auto& lo = out.get<1>().as<dense_tensor_t>();
+        auto& mz = dm(z._meta);
+        dm(hi._meta) = {mz.num_rows, mz.num_cols, 1.0f};
+        dm(lo._meta) = {mz.num_rows, mz.num_cols, 1.0f};
+        ok(bbx_relu_split(z.data(), hi.raw(), lo.raw(), (long long)mz.num_rows * mz.num_cols, p.stream));
+      },
+      ew_hint,
+      [](const params_t&, const margs_t& in, margs_t& out) {
+        auto& mz = dm(in.get<0>());
+        dm(out.get<0>()) = {mz.num_rows, mz.num_cols, 1.0f};
+        dm(out.get<1>()) = {mz.num_rows, mz.num_cols, 1.0f};
+      }));
+
   // ---- FNN application uds (applications/fnn/ffnn_lib_init.cc:20-177)
   register_ud(udm, "ffnn_act_mult", false, false, 2, 1);
   register_ud(udm, "ffnn_add", true, true, 2, 1);

@@ -231,6 +231,41 @@ __global__ void k_f32_to_bf16(const float* __restrict__ in, __nv_bfloat16* out, 
     out[i] = __float2bfloat16_rn(in[i]);
 }
 
+// hi = bf16(relu(z)), lo = bf16(relu(z) - hi): hi + lo carries relu(z) to
+// about 16 significant bits, so a tensor-core product of hi and of lo with
+// the same bf16 operand sums to nearly the f32-operand product.
+__global__ void k_relu_split(const float* __restrict__ z, __nv_bfloat16* hi, __nv_bfloat16* lo, long long n) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long i0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if ((((uintptr_t)z) & 15) == 0 && (((uintptr_t)hi | (uintptr_t)lo) & 7) == 0) {
+    const long long n4 = n >> 2;
+    for (long long i = i0; i < n4; i += stride) {
+      const float4 v = ((const float4*)z)[i];
+      const float a[4] = {v.x, v.y, v.z, v.w};
+      __nv_bfloat16 h[4], l[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const float r = a[u] > 0.f ? a[u] : 0.f;
+        h[u] = __float2bfloat16_rn(r);
+        l[u] = __float2bfloat16_rn(__fsub_rn(r, __bfloat162float(h[u])));
+      }
+      ((uint2*)hi)[i] = *(const uint2*)h;
+      ((uint2*)lo)[i] = *(const uint2*)l;
+    }
+    for (long long i = (n4 << 2) + i0; i < n; i += stride) {
+      const float r = z[i] > 0.f ? z[i] : 0.f;
+      hi[i] = __float2bfloat16_rn(r);
+      lo[i] = __float2bfloat16_rn(__fsub_rn(r, __bfloat162float(hi[i])));
+    }
+    return;
+  }
+  for (long long i = i0; i < n; i += stride) {
+    const float r = z[i] > 0.f ? z[i] : 0.f;
+    hi[i] = __float2bfloat16_rn(r);
+    lo[i] = __float2bfloat16_rn(__fsub_rn(r, __bfloat162float(hi[i])));
+  }
+}
+
 __global__ void k_bf16_to_f32(const __nv_bfloat16* __restrict__ in, float* out, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)

@@ -191,6 +191,12 @@ def colsum(x, out, accumulate=False):
     return out
 
 
+def relu_split(z, hi, lo):
+    """hi = bf16(relu(z)), lo = bf16(relu(z) - hi) for an f32 tensor z."""
+    check(lib.bbx_relu_split(_p(z), _p(hi), _p(lo), z.numel(), _stream()))
+    return hi, lo
+
+
 def cast(x, out):
     check(lib.bbx_cast(_dtype_code(x), _p(x), _dtype_code(out), _p(out), x.numel(), _stream()))
     return out

@@ -136,7 +136,7 @@ def cpmm(rt, rows=8, cols=8, bs=4096, dtype="bf16", seed=0, host=False):
 
 
 def ffnn(rt, batch=16384, d_in=8192, h1=8192, h2=4096, classes=1024, bs=2048, seed=0, host=False,
-         dtype="bf16"):
+         dtype="bf16", split_a1=False):
     """One forward + backward step of a blocked 3-layer network:
     A1 = relu(X W1), A2 = relu(A1 W2), Z3 = A2 W3, loss = softmax-CE(Z3, labels);
     backward dW3 = A2^T G3, dA2 = G3 W3^T, dZ2 = dA2 * relu'(A2), dW2 = A1^T dZ2,
@@ -145,7 +145,15 @@ def ffnn(rt, batch=16384, d_in=8192, h1=8192, h2=4096, classes=1024, bs=2048, se
     weight gradients f32; every matmul over the block grid is split into block
     products plus a matrix_add REDUCE. Weights are N(0, 1/fan_in), X N(0, 1),
     labels uniform over the classes. Returns tids of the weights, dW blocks and
-    per-row-block losses and the algorithmic FLOPs (2 * sum m n k)."""
+    per-row-block losses and the algorithmic FLOPs (2 * sum m n k).
+
+    split_a1 (bf16 only): the first activation is kept as two bf16 blocks,
+    hi = bf16(relu(Z1)) and lo = bf16(relu(Z1) - hi) (ud matrix_relu_split),
+    and Z2 sums the products of both with W2. A bf16-rounded A1 moves enough
+    layer-2 pre-activations across 0 to flip ~0.1 % of the layer-2 ReLU masks,
+    which puts ~3 % of error into dW1 and dW2; hi + lo keeps ~16 bits. The
+    extra products (2 * batch * h1 * h2 FLOP) are not counted as algorithmic
+    FLOPs."""
     e = Emitter(rt)
     rng = _rng(seed)
     # dtype="f32" runs the same network on FP32 blocks (the plain path)
@@ -159,6 +167,8 @@ def ffnn(rt, batch=16384, d_in=8192, h1=8192, h2=4096, classes=1024, bs=2048, se
     drelu = rt.impl("matrix_relu_dif", [B16], [B16])
     had = rt.impl("matrix_matrix_hadamard", [B16, B16], [B16])
     sce = rt.impl("matrix_softmax_ce", [F32, "labels"], [B16, F32])
+    split_a1 = split_a1 and dtype == "bf16"
+    split = rt.impl("matrix_relu_split", [F32], [B16, B16]) if split_a1 else None
     host_vals = {}
     dead = []
 
@@ -217,9 +227,34 @@ def ffnn(rt, batch=16384, d_in=8192, h1=8192, h2=4096, classes=1024, bs=2048, se
     # forward: pre-activations accumulate in f32 (so the ReLU masks come from
     # f32 values), activations are stored bf16 for the next tensor-core matmul
     Z1 = blocked_mm(lambda i, k: X[(i, k)], lambda k, j: W1[(k, j)], R, K1, KI, mm_f, add_f)
-    A1 = {key: ew(relu, [t]) for key, t in Z1.items()}
+    if split_a1:
+        A1, A1lo = {}, {}
+        for key, t in Z1.items():
+            hi, lo = e.tid(), e.tid()
+            rt.apply(split, [t], [hi, lo])
+            A1[key], A1lo[key] = hi, lo
+    else:
+        A1 = {key: ew(relu, [t]) for key, t in Z1.items()}
     dead.extend(Z1.values())
-    Z2 = blocked_mm(lambda i, k: A1[(i, k)], lambda k, j: W2[(k, j)], R, K2, K1, mm_f, add_f)
+    if split_a1:
+        # Z2[i, j] = sum over k of A1hi[i, k] W2[k, j] + A1lo[i, k] W2[k, j], one REDUCE in f32
+        Z2 = {}
+        for i in range(R):
+            for j in range(K2):
+                parts = []
+                for kk in range(K1):
+                    for src in (A1, A1lo):
+                        t = e.tid()
+                        rt.apply(mm_f, [src[(i, kk)], W2[(kk, j)]], [t], params=[False, False])
+                        parts.append(t)
+                    e.flops += 2.0 * bs * bs * bs
+                t = e.tid()
+                rt.reduce(add_f, parts, t)
+                dead.extend(parts)
+                Z2[(i, j)] = t
+        dead.extend(A1lo.values())
+    else:
+        Z2 = blocked_mm(lambda i, k: A1[(i, k)], lambda k, j: W2[(k, j)], R, K2, K1, mm_f, add_f)
     A2 = {key: ew(relu, [t]) for key, t in Z2.items()}
     dead.extend(Z2.values())
     Z3 = blocked_mm(lambda i, k: A2[(i, k)], lambda k, j: W3[k], R, 1, K2, mm_f, add_f, n=classes)
@@ -246,7 +281,7 @@ def ffnn(rt, batch=16384, d_in=8192, h1=8192, h2=4096, classes=1024, bs=2048, se
     rt.delete(sorted(set(dead)))
     return {"X": X, "W1": W1, "W2": W2, "W3": W3, "labels": labels, "dW1": dW1, "dW2": dW2, "dW3": dW3,
             "loss": loss, "flops": e.flops, "host": host_vals, "bs": bs,
-            "dims": (batch, d_in, h1, h2, classes)}
+            "dims": (batch, d_in, h1, h2, classes), "split_a1": split_a1}
 
 
 def random_dag(rt, n_ops=2000, depth=8, seed=0, dtype="bf16", lo=128, hi=2048, step=64,

@@ -152,6 +152,12 @@ int bbx_colsum_f32(const float* in, float* out, int rows, int cols, long long ld
 
 /* Element-type conversion f32 <-> bf16. */
 int bbx_cast(int src_dtype, const void* in, int dst_dtype, void* out, long long n, void* stream);
+/* New (no reference counterpart): relu of an f32 block split into two bf16
+ * blocks, hi = bf16(relu(z)) and lo = bf16(relu(z) - hi). A layer whose
+ * activation feeds another ReLU layer multiplies both by the next weights, so
+ * its tensor-core operand carries ~16 significant bits instead of 8 (ud
+ * matrix_relu_split). */
+int bbx_relu_split(const float* z, void* hi, void* lo, long long n, void* stream);
 
 /* Per-block absmax FP8-E4M3 quantisation: out = e4m3(in * 448/absmax(in)),
  * *scale_out (device f32) = absmax/448. transpose=1 writes cols x rows. Uses a

@@ -356,8 +356,11 @@ def _ffnn_reference(info, emulate_bf16):
     y = np.concatenate([hv[("y", i)] for i in range(batch // bs)])
     # bf16 storage is emulated exactly where the DAG stores bf16: activations,
     # the softmax gradient, each block product of dA1 and the reduced dA1
-    A1 = rb(np.maximum(X @ W1, 0))
-    A2 = rb(np.maximum(A1 @ W2, 0))
+    A1f = np.maximum(X @ W1, 0)
+    A1 = rb(A1f)
+    # a split first activation (matrix_relu_split) enters Z2 as hi + lo
+    A1z = A1 + rb(A1f - A1) if info.get("split_a1") else A1
+    A2 = rb(np.maximum(A1z @ W2, 0))
     Z3 = A2 @ W3
     P = np.exp(Z3 - Z3.max(1, keepdims=True))
     P /= P.sum(1, keepdims=True)
@@ -405,6 +408,64 @@ def test_ffnn_step_vs_f64(R, path):
         # up in the max norm of dW2 at ~0.15 for these seeded inputs); the
         # kernels add at most 1e-2 on top of it
         assert rel_err(g, p) <= rel_err(e, p) + 1e-2, name
+
+
+@pytest.mark.parametrize("path", ["per_op", "dag"])
+def test_ffnn_split_first_activation(R, path):
+    """The FFN step with its first activation split into bf16 hi + lo
+    (matrix_relu_split): within 1e-2 of FP64 arithmetic on the same storage
+    points, and much closer to the all-FP64 network than the same step with a
+    bf16-rounded activation, whose layer-2 ReLU masks flip."""
+    runtime, workloads = R
+    errs = {}
+    for split in (False, True):
+        rt = runtime.Runtime()
+        info = workloads.ffnn(rt, batch=512, d_in=256, h1=256, h2=256, classes=128, bs=128, seed=4, host=True,
+                              split_a1=split)
+        assert info["split_a1"] == split
+        dag = None
+        if path == "per_op":
+            rt.run()
+            get = lambda t: read_dense(rt, t)
+        else:
+            dag = rt.build_dag(runtime.HEURISTIC, tile_n=-1)
+            assert dag.stats()["other_launches"] == (12 if split else 4)  # 8 split relus, 4 softmax-CEs
+            dag.launch()
+            get = lambda t: read_dense(rt, t, dag)
+        loss = np.concatenate([get(info["loss"][i]).ravel() for i in range(4)])
+        dW1 = np.block([[get(info["dW1"][(k, j)]) for j in range(2)] for k in range(2)])
+        dW2 = np.block([[get(info["dW2"][(k, j)]) for j in range(2)] for k in range(2)])
+        dW3 = np.vstack([get(info["dW3"][(k, 0)]) for k in range(2)])
+        got = (loss, dW1, dW2, dW3)
+        emul = _ffnn_reference(info, True)
+        pure = _ffnn_reference(info, False)
+        for name, g, e in zip(("loss", "dW1", "dW2", "dW3"), got, emul):
+            assert rel_err(g, e) <= 1e-2, (split, name)
+        errs[split] = max(rel_err(g, p) for g, p in zip(got, pure))
+        if dag is not None:
+            dag.close()
+        rt.close()
+    assert errs[True] <= errs[False] / 3, errs
+
+
+def test_relu_split_exact(R):
+    """hi = bf16(relu(z)) and lo = bf16(relu(z) - hi), bit for bit, on aligned
+    and unaligned tensors (vector and scalar paths)."""
+    import torch
+    from bbts_b200 import ops
+    rng = np.random.default_rng(12)
+    for n, off in ((1 << 20, 0), (100003, 1)):
+        z = rng.standard_normal(n + off).astype(np.float32) * 10.0 ** rng.uniform(-3, 3, n + off).astype(np.float32)
+        zt = torch.from_numpy(z).cuda()[off:]
+        hi = torch.empty(n + off, dtype=torch.bfloat16, device="cuda")[off:]
+        lo = torch.empty(n + off, dtype=torch.bfloat16, device="cuda")[off:]
+        ops.relu_split(zt, hi, lo)
+        torch.cuda.synchronize()
+        r = torch.relu(torch.from_numpy(z[off:]))
+        h = r.to(torch.bfloat16)
+        lo_ref = (r - h.float()).to(torch.bfloat16)
+        assert torch.equal(hi.cpu().view(torch.int16), h.view(torch.int16))
+        assert torch.equal(lo.cpu().view(torch.int16), lo_ref.view(torch.int16))
 
 
 @pytest.mark.parametrize("policy", [0, 1])
