@@ -113,6 +113,9 @@ SIGNATURES = {
     "bbx_mlp_get_params": (i32, [vp, vp]),
     "bbx_mlp_set_params": (i32, [vp, vp]),
     "bbx_rt_set_predictor": (i32, [vp, vp]),
+    "bbx_tile_record": (i32, [i32]),
+    "bbx_tile_samples": (i32, [vp, vp, i32, C.POINTER(i32)]),
+    "bbx_rt_set_tile_predictor": (i32, [vp, vp]),
 }
 
 for _name, (_res, _args) in SIGNATURES.items():

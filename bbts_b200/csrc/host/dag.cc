@@ -204,10 +204,54 @@ std::string tune_key(int dtype, bool ta, bool tb, const std::vector<bbx_tc_probl
   return buf;
 }
 
+// Features of a grouped tensor-core launch run with tile `tn` (the input of the
+// learned tile choice, same 12-wide layout as the per-op features): tile
+// one-hot (128, 256, 512), log2 of the problem count, of the FLOPs, of the
+// largest m and n, of the tiles the launch runs, of the mean k, dtype (0 bf16,
+// 1 e4m3), operand layouts.
+op_features_t tile_features(int dtype, bool ta, bool tb, const std::vector<bbx_tc_problem_t>& ps, int tn) {
+  op_features_t f{};
+  double fl = 0, ksum = 0, tiles = 0;
+  int maxm = 0, maxn = 0;
+  for (auto& q : ps) {
+    fl += 2.0 * q.m * q.n * (double)q.k;
+    ksum += q.k;
+    maxm = std::max(maxm, q.m);
+    maxn = std::max(maxn, q.n);
+    const int bm = tn == 512 ? 256 : 128, bn = tn == 512 ? 256 : tn;
+    tiles += (double)((q.m + bm - 1) / bm) * ((q.n + bn - 1) / bn);
+  }
+  f.f[0] = tn == 128 ? 1.f : 0.f;
+  f.f[1] = tn == 256 ? 1.f : 0.f;
+  f.f[2] = tn == 512 ? 1.f : 0.f;
+  f.f[3] = (float)std::log2((double)ps.size());
+  f.f[4] = (float)std::log2(std::max(1.0, fl));
+  f.f[5] = (float)std::log2(std::max(1, maxm));
+  f.f[6] = (float)std::log2(std::max(1, maxn));
+  f.f[7] = (float)std::log2(std::max(1.0, tiles));
+  f.f[8] = (float)std::log2(std::max(1.0, ksum / std::max<size_t>(1, ps.size())));
+  f.f[9] = dtype == ELEM_E4M3 ? 1.f : 0.f;
+  f.f[10] = ta ? 1.f : 0.f;
+  f.f[11] = tb ? 1.f : 0.f;
+  return f;
+}
+
+// Samples of the autotuner's own timings, (group features for a tile, us per
+// launch), recorded while tile_record(true) is on: the training set of the
+// learned tile choice.
+std::mutex g_tile_mu;
+bool g_tile_rec = false;
+std::vector<std::pair<op_features_t, float>> g_tile_samples;
+
 int autotune_tile_n(int dtype, bool ta, bool tb, const std::vector<bbx_tc_problem_t>& ps) {
   const std::string key = tune_key(dtype, ta, tb, ps);
   const char* path = std::getenv("BBX_TUNE_CACHE");
+  bool recording;
   {
+    std::lock_guard<std::mutex> lk(g_tile_mu);
+    recording = g_tile_rec;
+  }
+  if (!recording) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     if (!g_tune_loaded && path) {
       FILE* f = std::fopen(path, "r");
@@ -255,12 +299,17 @@ int autotune_tile_n(int dtype, bool ta, bool tb, const std::vector<bbx_tc_proble
       float ms = 0;
       cudaEventElapsedTime(&ms, e0, e1);
       if (ms < best_ms) { best_ms = ms; best = c.first; }
+      if (recording) {
+        std::lock_guard<std::mutex> lk(g_tile_mu);
+        g_tile_samples.push_back({tile_features(dtype, ta, tb, ps, c.first), ms * 1000.f / 3.f});
+      }
     }
   } catch (...) {
     release();
     throw;
   }
   release();
+  if (recording) return best;  // samples are being taken: the cache is neither read nor written
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune[key] = best;
   if (path) {
@@ -271,6 +320,20 @@ int autotune_tile_n(int dtype, bool ta, bool tb, const std::vector<bbx_tc_proble
     }
   }
   return best;
+}
+
+// The tile whose launch the runtime's tile model predicts fastest.
+int learned_tile_n(const runtime_t& rt, int dtype, bool ta, bool tb, const std::vector<bbx_tc_problem_t>& ps) {
+  std::vector<int> cand;
+  for (int tn : {512, 256, 128})
+    if (!(tn == 512 && dtype == ELEM_E4M3)) cand.push_back(tn);
+  std::vector<op_features_t> fs;
+  for (int tn : cand) fs.push_back(tile_features(dtype, ta, tb, ps, tn));
+  const std::vector<double> t = rt.tile_predictor(fs);
+  size_t best = 0;
+  for (size_t i = 1; i < cand.size() && i < t.size(); ++i)
+    if (t[i] < t[best]) best = i;
+  return cand[best];
 }
 
 // Contraction params: rank_l, rank_r, rank_o, modes_l..., modes_r..., modes_o..., alpha.
@@ -682,8 +745,12 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
     for (auto& kv : tc_groups) {
       group_t g{G_TC, w};
       const int dt = (kv.first & 0xff) / 4;
-      // tile_n < 0: autotune per group; 0: size heuristic; 128 / 256: forced
-      const int tn = tile_n < 0 ? autotune_tile_n(dt, (kv.first & 2) != 0, (kv.first & 1) != 0, kv.second) : tile_n;
+      // tile_n -1: autotune per group; -2: the learned tile model (the size
+      // heuristic without one); 0: size heuristic; 128 / 256 / 512: forced
+      const bool ta = (kv.first & 2) != 0, tb = (kv.first & 1) != 0;
+      int tn = tile_n;
+      if (tile_n == -2) tn = rt->tile_predictor ? learned_tile_n(*rt, dt, ta, tb, kv.second) : 0;
+      else if (tile_n < 0) tn = autotune_tile_n(dt, ta, tb, kv.second);
       dag_bbx(bbx_tc_plan_create(dt == ELEM_E4M3 ? BBX_E4M3 : BBX_BF16, kv.second.data(), (int)kv.second.size(), tn,
                                  &g.tc_plan));
       g.flops = tc_group_flops(kv.second);
@@ -729,6 +796,13 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
   dag_cuda(cudaStreamCreateWithFlags(&s_tc, cudaStreamNonBlocking), "cudaStreamCreate");
   std::vector<cudaEvent_t> ev(d->groups.size() + 1);
   for (auto& e : ev) dag_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+  // the library's per-device state (status word, kernel attributes) is set up
+  // on its first use and allocates: never inside the capture below
+  if (bbx_num_sms() < 0) {
+    char msg[512];
+    bbx_last_error(msg, sizeof msg);
+    throw std::runtime_error(std::string("DAG build: device set-up failed: ") + msg);
+  }
   dag_cuda(cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
   bool ok = false;
   try {
@@ -836,6 +910,17 @@ void* dag_tensor(const dag_t* d, tid_t tid, tensor_meta_t* meta) {
 size_t dag_payload_bytes(const dag_t* d, tid_t tid) {
   auto it = d->tensors.find(tid);
   return it == d->tensors.end() ? 0 : it->second.bytes;
+}
+
+void tile_record(bool on) {
+  std::lock_guard<std::mutex> lk(g_tile_mu);
+  g_tile_rec = on;
+  if (on) g_tile_samples.clear();
+}
+
+std::vector<std::pair<op_features_t, float>> tile_samples() {
+  std::lock_guard<std::mutex> lk(g_tile_mu);
+  return g_tile_samples;
 }
 
 }  // namespace bbts

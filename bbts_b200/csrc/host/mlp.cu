@@ -329,6 +329,26 @@ extern "C" int bbx_rt_set_predictor(bbx_rt_t* rt, bbx_mlp_t* mlp) {
   return BBX_OK;
 }
 
+// Installs an MLP trained on tile_features rows as the runtime's tile model
+// (dag_build with tile_n = -2 picks the tile of least predicted time).
+extern "C" int bbx_rt_set_tile_predictor(bbx_rt_t* rt, bbx_mlp_t* mlp) {
+  if (!rt) return bbx::set_error(BBX_ERR_INVALID, "null runtime");
+  bbts::runtime_t* r = bbts::rt_of(rt);
+  if (!mlp) {
+    r->tile_predictor = nullptr;
+    return BBX_OK;
+  }
+  r->tile_predictor = [mlp](const std::vector<bbts::op_features_t>& fs) {
+    std::vector<float> x(fs.size() * IN), y(fs.size());
+    for (size_t i = 0; i < fs.size(); ++i) std::memcpy(&x[i * IN], fs[i].f, sizeof(float) * IN);
+    bk(bbx_mlp_predict(mlp, x.data(), (int)fs.size(), y.data()));
+    std::vector<double> out(fs.size());
+    for (size_t i = 0; i < fs.size(); ++i) out[i] = std::exp((double)y[i]);
+    return out;
+  };
+  return BBX_OK;
+}
+
 // The heuristic cost, calibrated: the ud's get_complexity_hint mapped to
 // microseconds by a fit of log latency on log hint.
 extern "C" int bbx_rt_set_hint_predictor(bbx_rt_t* rt, double a, double b) {

@@ -344,6 +344,22 @@ int bbx_dag_build(bbx_rt_t* rt, int policy, int tile_n, bbx_dag_t** out) {
   });
 }
 
+int bbx_tile_record(int on) {
+  bbts::tile_record(on != 0);
+  return BBX_OK;
+}
+
+int bbx_tile_samples(float* features, float* latency_us, int cap, int* n_out) {
+  auto v = bbts::tile_samples();
+  const int n = (int)v.size();
+  for (int i = 0; i < n && i < cap; ++i) {
+    if (features) std::memcpy(features + 12 * (size_t)i, v[i].first.f, sizeof(float) * 12);
+    if (latency_us) latency_us[i] = v[i].second;
+  }
+  if (n_out) *n_out = n;
+  return BBX_OK;
+}
+
 int bbx_dag_launch(bbx_dag_t* dag, void* stream) {
   if (!dag) return bbx::set_error(BBX_ERR_INVALID, "null dag");
   RT_TRY(dag_launch(dag->d, (cudaStream_t)stream));

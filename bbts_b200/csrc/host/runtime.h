@@ -177,6 +177,9 @@ class runtime_t {
   // predicted latency (us) for a node / a batch of nodes, installed by the learned cost model
   std::function<double(const op_features_t&)> predictor;
   std::function<std::vector<double>(const std::vector<op_features_t>&)> batch_predictor;
+  // predicted time of a grouped tensor-core launch per tile (dag_build with
+  // tile_n = -2), from tile_features rows; installed from a trained MLP
+  std::function<std::vector<double>(const std::vector<op_features_t>&)> tile_predictor;
 
   // Worker streams of the per-op path: the reference pulls ready commands from
   // the reservation station with num_threads workers (src/server/node.cc:67-69);
@@ -206,6 +209,10 @@ int elem_of(const tensor_factory_t& tf, tfid_t id);
 void execute_command(runtime_t& rt, command_t& cmd, cudaStream_t st);
 
 dag_t* dag_build(runtime_t* rt, int policy, int tile_n);
+// Recording of the autotuner's timings as learned-tile training samples
+// (features of a group run with one tile, us per launch); on clears them.
+void tile_record(bool on);
+std::vector<std::pair<op_features_t, float>> tile_samples();
 void dag_launch(dag_t* d, cudaStream_t st);
 void dag_destroy(dag_t* d);
 struct dag_stats_t {

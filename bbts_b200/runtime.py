@@ -15,6 +15,9 @@ from ._lib import lib, check
 
 META_BYTES = 260
 HEURISTIC, LEARNED = 0, 1
+# build_dag tile_n: AUTOTUNE times every candidate tile per group; LEARNED_TILES
+# asks the runtime's tile model (set_tile_predictor); 0 = size heuristic
+AUTOTUNE, LEARNED_TILES = -1, -2
 _NP_OF_FMT = {"dense": np.float32, "ffnn_dense": np.float32, "cutensor": np.float32, "labels": np.int32}
 
 
@@ -229,6 +232,12 @@ class Runtime:
         check(lib.bbx_rt_set_predictor(self.h, mlp.h if mlp is not None else None))
         self._predictor = mlp
 
+    def set_tile_predictor(self, mlp):
+        """An MLP trained on tile samples (tile_samples) becomes the tile model
+        of build_dag(tile_n=LEARNED_TILES); the runtime keeps a reference."""
+        check(lib.bbx_rt_set_tile_predictor(self.h, mlp.h if mlp is not None else None))
+        self._tile_predictor = mlp
+
     def build_dag(self, policy=HEURISTIC, tile_n=0):
         return Dag(self, policy, tile_n)
 
@@ -242,6 +251,23 @@ class Runtime:
             self.close()
         except Exception:
             pass
+
+
+def tile_record(on):
+    """Record the DAG autotuner's timings as tile samples (on clears them)."""
+    check(lib.bbx_tile_record(int(bool(on))))
+
+
+def tile_samples():
+    """(features n x 12 float32, us per launch n) recorded by the autotuner."""
+    n = C.c_int()
+    check(lib.bbx_tile_samples(None, None, 0, C.byref(n)))
+    cap = n.value
+    f = np.empty((cap, 12), np.float32)
+    t = np.empty(cap, np.float32)
+    check(lib.bbx_tile_samples(f.ctypes.data, t.ctypes.data, cap, C.byref(n)))
+    k = min(cap, n.value)
+    return f[:k].copy(), t[:k].copy()
 
 
 class Dag:

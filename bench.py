@@ -56,6 +56,8 @@ def parse():
                         "2000-op DAG on the per-op path under device budgets below its footprint")
     p.add_argument("--n-ops", type=int, default=0, help="DAG size override (dag: 2000, learned: 5000)")
     p.add_argument("--train-dags", type=int, default=100, help="learned: DAGs recorded for the training set")
+    p.add_argument("--tile-dags", type=int, default=16,
+                   help="learned: DAGs whose autotuner timings train the tile model")
     return p.parse_args()
 
 
@@ -551,6 +553,30 @@ def run_dag_workload(args):
             A = np.stack([H[n_hold:], np.ones(len(y) - n_hold)], 1)
             ha, hb = np.linalg.lstsq(A, y[n_hold:], rcond=None)[0]
             hint_mse = float(np.mean((ha * H[:n_hold] + hb - y[:n_hold]) ** 2))
+            # tile model: the DAG autotuner's own timings (every candidate tile of
+            # every group) on config-4-style training DAGs
+            t3 = time.perf_counter()
+            runtime.tile_record(True)
+            try:
+                for d in range(args.tile_dags):
+                    rt_t = runtime.Runtime()
+                    workloads.random_dag(rt_t, n_ops=2000, depth=8, seed=3000 + d, dtype="bf16", hi=4096, reuse=0.8)
+                    torch.cuda.synchronize()
+                    runtime.Dag(rt_t, runtime.HEURISTIC, runtime.AUTOTUNE).close()
+                    rt_t.close()
+            finally:
+                runtime.tile_record(False)
+            tf, tt = runtime.tile_samples()
+            ty = np.log(np.maximum(tt, 1e-3))
+            tile_rec_s = time.perf_counter() - t3
+            th = max(1, len(ty) // 10)
+            tmlp = runtime.Mlp(seed=7)
+            tmlp.set_norm(tf[th:].mean(0), tf[th:].std(0) + 1e-6)
+            tile_loss = tmlp.train(tf[th:], ty[th:], epochs=100, batch=64, lr=1e-3)
+            tile_mse = float(np.mean((tmlp.predict(tf[:th]) - ty[:th]) ** 2))
+            tid = tf[:, :3].argmax(1)
+            tmean = {k: ty[th:][tid[th:] == k].mean() for k in set(tid[th:].tolist())}
+            tile_base_mse = float(np.mean((np.array([tmean.get(k, ty[th:].mean()) for k in tid[:th]]) - ty[:th]) ** 2))
             # held-out DAG: makespans on the same kernels under each cost source
             rt, info = build("bf16", 4242, reuse=0.8)
             preds = {"heuristic": None, "hint": ("hint", ha, hb), "learned": ("mlp", mlp)}
@@ -573,6 +599,19 @@ def run_dag_workload(args):
                 make[nm] = _time_on(rt.stream.value, dag.launch, args.steps)
                 waves[nm] = dag.stats()["waves"]
                 dag.close()
+            # tiles of the learned schedule's graph: size rule (above), autotuner, tile model
+            tiles, build_s = {"size_rule": make["learned"]}, {}
+            install(preds["learned"])
+            rt.set_tile_predictor(tmlp)
+            for nm, tn in (("autotuned", runtime.AUTOTUNE), ("learned", runtime.LEARNED_TILES)):
+                tb0 = time.perf_counter()
+                dag = rt.build_dag(runtime.LEARNED, tile_n=tn)
+                build_s[nm] = round(time.perf_counter() - tb0, 2)
+                for _ in range(args.warmup):
+                    dag.launch()
+                tiles[nm] = _time_on(rt.stream.value, dag.launch, args.steps)
+                dag.close()
+            rt.set_tile_predictor(None)
             # per-op path through the reservation station on 4 worker streams:
             # LIFO + round-robin vs critical-path priority + earliest-finish stream
             per_op = {}
@@ -587,10 +626,11 @@ def run_dag_workload(args):
             one_stream = float(np.median([_time_on(rt.stream.value, lambda: rt.run(runtime.HEURISTIC), 1)
                                           for _ in range(3)]))
             flops = info["flops"]
-            value = flops / make["learned"] / 1e9
+            # the learned path: learned schedule and learned tiles
+            value = flops / tiles["learned"] / 1e9
             r3 = lambda v: round(v, 3)
             line.update({"metric": "block-op DAG makespan, learned vs heuristic schedule", "value": round(value, 2),
-                         "unit": "TFLOP/s", "ms_per_step": r3(make["learned"]), "dtype": "bf16",
+                         "unit": "TFLOP/s", "ms_per_step": r3(tiles["learned"]), "dtype": "bf16",
                          "config": {"workload": "held-out random DAG, %d ops, sizes 128..4096" % info["n_ops"],
                                     "flops_per_step": flops, "train_timings": int(len(y) - n_hold),
                                     "train_dags": args.train_dags},
@@ -600,8 +640,16 @@ def run_dag_workload(args):
                                          "per_op_4_streams_lifo": r3(per_op["heuristic"]),
                                          "per_op_4_streams_hint": r3(per_op["hint"]),
                                          "per_op_4_streams_learned": r3(per_op["learned"]),
-                                         "per_op_1_stream_lifo": r3(one_stream)},
+                                         "per_op_1_stream_lifo": r3(one_stream),
+                                         "grouped_learned_autotuned_tiles": r3(tiles["autotuned"]),
+                                         "grouped_learned_learned_tiles": r3(tiles["learned"])},
                          "waves": waves,
+                         "tile_model": {"samples": int(len(ty)), "holdout_mse_log_time": round(tile_mse, 4),
+                                        "per_tile_mean_mse_log_time": round(tile_base_mse, 4),
+                                        "train_loss": round(float(tile_loss), 4), "record_s": round(tile_rec_s, 1),
+                                        "build_s": build_s,
+                                        "learned_vs_size_rule": round(tiles["size_rule"] / tiles["learned"], 4),
+                                        "learned_vs_autotuned": round(tiles["autotuned"] / tiles["learned"], 4)},
                          "learned_gain": {"grouped_vs_heuristic": round(make["heuristic"] / make["learned"], 4),
                                           "grouped_vs_hint": round(make["hint"] / make["learned"], 4),
                                           "per_op_vs_heuristic": round(per_op["heuristic"] / per_op["learned"], 4),
@@ -614,6 +662,7 @@ def run_dag_workload(args):
                          "gpu_launches": None})
             rt.close()
             mlp.close()
+            tmlp.close()
     line["clocks"] = clk.summary()
     rc = bbts_b200.lib.bbx_check_device_status(None, None)
     if rc != 0:

@@ -76,7 +76,11 @@ extern "C" {
 const char* bbx_version(void);
 /* Copies the calling thread's last error message into buf; returns its length. */
 int bbx_last_error(char* buf, size_t len);
-/* Number of SMs of the current device (grids are sized to multiples of it). */
+/* Number of SMs of the current device (grids are sized to multiples of it).
+ * The library sets up per-device state (a status word, kernel attributes) on
+ * the first call that needs it on a device; that set-up allocates, so the
+ * first call should not come inside a stream capture: calling this function
+ * once per device first does it. */
 int bbx_num_sms(void);
 /* Synchronises `stream`, then reads and clears the device status word written
  * by kernels whose bounded waits ran out. Returns 0 or BBX_ERR_DEVICE. */
@@ -398,6 +402,18 @@ int bbx_mlp_get_params(bbx_mlp_t* mlp, float* out);
 int bbx_mlp_set_params(bbx_mlp_t* mlp, const float* in);
 /* install the MLP as the runtime's latency predictor (policy BBX_SCHED_LEARNED) */
 int bbx_rt_set_predictor(bbx_rt_t* rt, bbx_mlp_t* mlp);
+/* New (no reference counterpart): learned tile choice. While recording is on,
+ * the DAG autotuner (bbx_dag_build with tile_n = -1) logs one sample per group
+ * and candidate tile: 12 features of the grouped launch run with that tile
+ * (tile one-hot 128/256/512, log2 problem count, FLOPs, largest m, largest n,
+ * tiles, mean k, dtype, operand layouts) and its time in us. Turning it on
+ * clears the samples; recording bypasses the tune cache. An MLP trained on
+ * them and installed with bbx_rt_set_tile_predictor makes bbx_dag_build with
+ * tile_n = -2 pick each group's tile of least predicted time, with no timing
+ * launches (without a tile model, -2 is the size heuristic of tile_n = 0). */
+int bbx_tile_record(int on);
+int bbx_tile_samples(float* features, float* latency_us, int cap, int* n_out);
+int bbx_rt_set_tile_predictor(bbx_rt_t* rt, bbx_mlp_t* mlp);
 /* install the calibrated complexity-hint model exp(a * ln(max(hint, 1)) + b) us
  * as the predictor instead: the reference's get_complexity_hint, fit to
  * recorded latencies, driving the same list scheduling as the MLP. */

@@ -280,6 +280,81 @@ def test_mlp_training_fits(R):
     assert loss < 0.1 * l0
 
 
+def _small_dag(workloads, rt, seed, dtype="bf16"):
+    return workloads.random_dag(rt, n_ops=160, depth=6, seed=seed, dtype=dtype, lo=128, hi=1024, step=64,
+                                contraction_dims=(16, 64))
+
+
+def test_latency_model_beats_complexity_hint(R):
+    """What the trained network gains over the method without it: on a held-out
+    DAG, the MLP trained on the runtime's own per-op timings predicts log
+    latency with less than 0.7x the error of the reference's complexity hint
+    calibrated by a least-squares fit on the same training timings."""
+    runtime, workloads = R
+    F, L, H = [], [], []
+    for seed in range(6):
+        rt = runtime.Runtime()
+        _small_dag(workloads, rt, 400 + seed, "bf16" if seed % 2 == 0 else "f32")
+        f, lat, h = rt.record(with_hints=True)
+        F.append(f), L.append(lat), H.append(h)
+        rt.close()
+    X, y = np.concatenate(F[:-1]), np.log(np.maximum(np.concatenate(L[:-1]), 1e-3))
+    hx = np.log(np.maximum(np.concatenate(H[:-1]), 1.0))
+    Xt, yt = F[-1], np.log(np.maximum(L[-1], 1e-3))
+    ht = np.log(np.maximum(H[-1], 1.0))
+    a, b = np.linalg.lstsq(np.stack([hx, np.ones_like(hx)], 1), y, rcond=None)[0]
+    hint_mse = float(np.mean((a * ht + b - yt) ** 2))
+    mlp = runtime.Mlp(seed=6)
+    mlp.set_norm(X.mean(0), X.std(0) + 1e-6)
+    mlp.train(X, y, epochs=60, batch=128, lr=1e-3)
+    mlp_mse = float(np.mean((mlp.predict(Xt) - yt) ** 2))
+    assert mlp_mse < 0.7 * hint_mse, (mlp_mse, hint_mse)
+
+
+def test_learned_tile_choice(R):
+    """The tile model: the DAG autotuner's own timings (recorded per group and
+    candidate tile) train an MLP that predicts held-out group times far better
+    than the per-tile mean; installed as the runtime's tile model it picks
+    every group's tile with no timing launch, and the DAG gives the same bytes
+    as the per-op path."""
+    runtime, workloads = R
+    runtime.tile_record(True)
+    try:
+        for seed in range(5):
+            rt = runtime.Runtime()
+            _small_dag(workloads, rt, 300 + seed)
+            dag = rt.build_dag(runtime.HEURISTIC, tile_n=runtime.AUTOTUNE)
+            dag.close()
+            rt.close()
+    finally:
+        runtime.tile_record(False)
+    f, t = runtime.tile_samples()
+    assert len(t) >= 40 and np.all(t > 0)
+    assert np.all(f[:, :3].sum(1) == 1)  # one tile per sample
+    y = np.log(t)
+    n = len(y) * 3 // 4
+    mlp = runtime.Mlp(seed=4)
+    mlp.set_norm(f[:n].mean(0), f[:n].std(0) + 1e-6)
+    mlp.train(f[:n], y[:n], epochs=200, batch=32, lr=2e-3)
+    mse = float(np.mean((mlp.predict(f[n:]) - y[n:]) ** 2))
+    tile_of = f[:, :3].argmax(1)
+    means = {k: y[:n][tile_of[:n] == k].mean() for k in set(tile_of[:n])}
+    base = float(np.mean((np.array([means.get(k, y[:n].mean()) for k in tile_of[n:]]) - y[n:]) ** 2))
+    assert mse < 0.5 * base, (mse, base)
+    rt1 = runtime.Runtime()
+    info = _small_dag(workloads, rt1, 350)
+    rt1.run()
+    rt2 = runtime.Runtime()
+    _small_dag(workloads, rt2, 350)
+    rt2.set_tile_predictor(mlp)
+    dag = rt2.build_dag(runtime.HEURISTIC, tile_n=runtime.LEARNED_TILES)
+    dag.launch()
+    for tid in info["finals"]:
+        want = rt1.get_bytes(tid)
+        assert np.array_equal(dag.read_bytes(tid, want.nbytes), want), tid
+    dag.close()
+
+
 # ------------------------------------------------------------------ program files
 def test_bbts_program_bmm(R, tmp_path):
     """A .bbts program in the reference's binary format (the single-node form of
