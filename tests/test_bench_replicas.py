@@ -52,3 +52,21 @@ def test_single_rank_needs_no_process_group():
     import bench
     assert bench.max_over_ranks(3.5, 1, None) == 3.5
     assert bench.job_tflops(1e12, 1, 1000.0) == pytest.approx(1.0)
+
+
+def test_cpu_step_sample():
+    """The CPU baseline's step sample: every block product in order within the
+    budget, C[0][0] returned for the cross-check, and a stop once the budget
+    has passed (at least one product is always done)."""
+    import numpy as np
+    sys.path.insert(0, ROOT)
+    import bench
+    import oracle
+    rng = np.random.default_rng(3)
+    a = [rng.uniform(-1, 1, (64, 48)).astype(np.float32) for _ in range(2)]
+    b = [rng.uniform(-1, 1, (48, 80)).astype(np.float32) for _ in range(3)]
+    tf, done, dt, c00 = bench.cpu_step_tflops(a, b, threads=2)
+    assert done == 6 and tf > 0 and dt > 0
+    assert np.array_equal(c00, oracle.sgemm(a[0], b[0], threads=1))
+    tf, done, dt, c00 = bench.cpu_step_tflops(a, b, threads=2, budget_s=0.0)
+    assert done == 1 and c00 is not None
