@@ -13,8 +13,10 @@
 #include <thread>
 #include <sstream>
 #include <tuple>
+#include "bbts_b200.h"
 #include "command.h"
 #include "compiler.h"
+#include "contraction.h"
 #include "reservation_station.h"
 #include "tensor.h"
 #include "ud_function.h"
@@ -317,7 +319,53 @@ static void test_bbts_roundtrip() {
   std::remove(path);
 }
 
+// The bf16 contraction lowering's GEMM orientation: the longer of the lhs-only
+// (nm) and rhs-only (nn) output extents becomes M. With nm > nn the GEMM is
+// A = Lc, B = Rc, column-major C; otherwise A = Rc, B = Lc, row-major C. Both
+// keep the staging layouts, pitches and per-batch offsets.
+static void test_contraction_orientation() {
+  char* lc = (char*)0x100000;
+  char* rc = (char*)0x200000;
+  char* ct = (char*)0x400000;
+  {  // 'ijk,kl->ijl': i, j lhs-only (nm = 960), l rhs-only (nn = 32), k summed
+    const long long dl[3] = {40, 24, 16}, dr[2] = {16, 32};
+    const int ml[3] = {0, 1, 2}, mr[2] = {2, 3}, mo[3] = {0, 1, 3};
+    bbx::ContractionLowering L;
+    EXPECT(bbx::lower_contraction(3, dl, ml, 2, dr, mr, 3, mo, true, &L) == 0);
+    EXPECT(L.nm == 960 && L.nn == 32 && L.kdim == 16 && L.nb == 1);
+    EXPECT(L.lc_mn && !L.rc_mn && L.direct);
+    const bbx::ContractionGemm g = bbx::contraction_gemm(L, lc, rc, ct, 0);
+    EXPECT(g.m == 960 && g.n == 32 && g.k == 16);
+    EXPECT(g.flags == BBX_EPI_C_COLMAJOR && g.ldc == 960 && g.c == ct);
+    EXPECT(g.a == lc && g.trans_a == 1 && g.lda == L.pm);  // Lc[k][m]
+    EXPECT(g.b == rc && g.trans_b == 1 && g.ldb == L.pk);  // Rc[n][k]
+  }
+  {  // batched 'ikb,klb->ilb' (b = 3): nm = 40 > nn = 32, offsets of batch 2
+    const long long dl[3] = {40, 16, 3}, dr[3] = {16, 32, 3};
+    const int ml[3] = {0, 2, 4}, mr[3] = {2, 3, 4}, mo[3] = {0, 3, 4};
+    bbx::ContractionLowering L;
+    EXPECT(bbx::lower_contraction(3, dl, ml, 3, dr, mr, 3, mo, true, &L) == 0);
+    EXPECT(L.nb == 3 && L.nm == 40 && L.nn == 32);
+    const bbx::ContractionGemm g = bbx::contraction_gemm(L, lc, rc, ct, 2);
+    EXPECT(g.flags == BBX_EPI_C_COLMAJOR && g.m == 40 && g.n == 32);
+    EXPECT(g.a == lc + 2 * 2 * L.kdim * L.pm);   // bf16 Lc[b][k][m]
+    EXPECT(g.b == rc + 2 * 2 * L.nn * L.pk);     // bf16 Rc[b][n][k]
+    EXPECT(g.c == ct + 4 * 2 * L.nn * L.nm);     // f32 Ct[b][n][m]
+  }
+  {  // 'ik,kl->il' with the rhs side longer (nm = 16 < nn = 64): row-major C
+    const long long dl[2] = {16, 8}, dr[2] = {8, 64};
+    const int ml[2] = {0, 2}, mr[2] = {2, 3}, mo[2] = {0, 3};
+    bbx::ContractionLowering L;
+    EXPECT(bbx::lower_contraction(2, dl, ml, 2, dr, mr, 2, mo, true, &L) == 0);
+    const bbx::ContractionGemm g = bbx::contraction_gemm(L, lc, rc, ct, 0);
+    EXPECT(g.m == 64 && g.n == 16 && g.k == 8 && g.flags == 0 && g.ldc == 16);
+    EXPECT(g.a == rc && g.trans_a == 0 && g.lda == L.pk);  // Rc[n][k]
+    EXPECT(g.b == lc && g.trans_b == 0 && g.ldb == L.pm);  // Lc[k][m]
+  }
+}
+
 int main() {
+  test_contraction_orientation();
   test_sbbts_compile();
   test_bbts_roundtrip();
   test_dense_format();
