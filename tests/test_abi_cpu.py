@@ -36,3 +36,24 @@ def test_no_cpu_fallback_symbols():
     from bbts_b200 import _lib
     for name in ("oracle_add", "oracle_matmul_f64", "oracle_sgemm_mt"):
         assert not hasattr(_lib.lib, name)
+
+
+def test_tile_recording_api_without_a_gpu():
+    # recording state and the sample buffer are host-side: on, no samples yet
+    # (no DAG was built), off again
+    from bbts_b200 import runtime
+    runtime.tile_record(True)
+    f, t = runtime.tile_samples()
+    assert f.shape == (0, 12) and t.shape == (0,)
+    runtime.tile_record(False)
+    assert runtime.AUTOTUNE == -1 and runtime.LEARNED_TILES == -2
+
+
+def test_host_arguments_rejected_before_cuda():
+    # these entry points validate their arguments on the host and return an
+    # error code with a message, without touching a device
+    from bbts_b200 import lib, last_error
+    assert lib.bbx_relu_split(None, None, None, 10, None) == -1
+    assert "relu_split" in last_error()
+    assert lib.bbx_stream_plan_bulk(None) == -1
+    assert "stream plan" in last_error()
