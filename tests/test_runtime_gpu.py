@@ -280,7 +280,7 @@ def test_mlp_training_fits(R):
     assert loss < 0.1 * l0
 
 
-def _small_dag(workloads, rt, seed, dtype="bf16"):
+def _tile_dag(workloads, rt, seed, dtype="bf16"):
     return workloads.random_dag(rt, n_ops=160, depth=6, seed=seed, dtype=dtype, lo=128, hi=1024, step=64,
                                 contraction_dims=(16, 64))
 
@@ -294,7 +294,7 @@ def test_latency_model_beats_complexity_hint(R):
     F, L, H = [], [], []
     for seed in range(6):
         rt = runtime.Runtime()
-        _small_dag(workloads, rt, 400 + seed, "bf16" if seed % 2 == 0 else "f32")
+        _tile_dag(workloads, rt, 400 + seed, "bf16" if seed % 2 == 0 else "f32")
         f, lat, h = rt.record(with_hints=True)
         F.append(f), L.append(lat), H.append(h)
         rt.close()
@@ -322,7 +322,7 @@ def test_learned_tile_choice(R):
     try:
         for seed in range(5):
             rt = runtime.Runtime()
-            _small_dag(workloads, rt, 300 + seed)
+            _tile_dag(workloads, rt, 300 + seed)
             dag = rt.build_dag(runtime.HEURISTIC, tile_n=runtime.AUTOTUNE)
             dag.close()
             rt.close()
@@ -342,10 +342,10 @@ def test_learned_tile_choice(R):
     base = float(np.mean((np.array([means.get(k, y[:n].mean()) for k in tile_of[n:]]) - y[n:]) ** 2))
     assert mse < 0.5 * base, (mse, base)
     rt1 = runtime.Runtime()
-    info = _small_dag(workloads, rt1, 350)
+    info = _tile_dag(workloads, rt1, 350)
     rt1.run()
     rt2 = runtime.Runtime()
-    _small_dag(workloads, rt2, 350)
+    _tile_dag(workloads, rt2, 350)
     rt2.set_tile_predictor(mlp)
     dag = rt2.build_dag(runtime.HEURISTIC, tile_n=runtime.LEARNED_TILES)
     dag.launch()
