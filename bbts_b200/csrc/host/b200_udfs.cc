@@ -124,8 +124,8 @@ void dense_stream(const params_t& p, int kind, int op, const std::vector<const t
   s.n_in = (int)ins.size(); s.kahan = 1;
   const auto& m = dm(ins[0]->_meta);
   s.n = (long long)m.num_rows * m.num_cols;
-  for (size_t i = 0; i < ins.size(); ++i) s.in[i] = ins[i]->_meta.payload();
-  s.out = out._meta.payload();
+  for (size_t i = 0; i < ins.size(); ++i) s.in[i] = ins[i]->payload();
+  s.out = out.payload();
   s.p0 = p0; s.p1 = p1;
   ok(bbx_stream_group(&s, 1, p.stream));
   dm(out._meta) = {m.num_rows, m.num_cols, 1.0f};
@@ -156,8 +156,11 @@ unsigned long long next_seed() {
   return 0x5eedull + 0x9E3779B97F4A7C15ull * (ctr++ + 1);
 }
 
+// Registers a ud function unless one of that name exists (register_udf then
+// returns -1 and drops the new one, here and in the reference,
+// udf_manager.cc:78-95). Only the reference's own member functions are called
+// on the manager, so this also runs against a reference node's manager.
 void register_ud(udf_manager_t& udm, const char* name, bool ass, bool com, size_t nin, size_t nout) {
-  if (udm.get_udf(name)) return;
   auto f = std::make_unique<ud_func_t>();
   f->ud_name = name;
   f->is_ass = ass;
@@ -553,8 +556,8 @@ void register_b200_udfs(udf_manager_t& udm) {
         so.rank = (uint32_t)ord.size();
         for (size_t r = 0; r < ord.size(); ++r) so.dims[r] = si.dims[ord[r]];
         std::vector<long long> d(si.dims, si.dims + si.rank);
-        ok(bbx_cu_reduction((const float*)in.get<0>()._meta.payload(), (int)si.rank, d.data(), p.get_raw(0).i,
-                            p.get_raw(1).f, ord.data(), (int)ord.size(), (float*)out.get<0>()._meta.payload(), p.stream));
+        ok(bbx_cu_reduction((const float*)in.get<0>().payload(), (int)si.rank, d.data(), p.get_raw(0).i,
+                            p.get_raw(1).f, ord.data(), (int)ord.size(), (float*)out.get<0>().payload(), p.stream));
       },
       [cu_shape, cu_elems](const params_t&, const margs_t& in) -> size_t { return cu_elems(cu_shape(in.get<0>())); },
       [cu_shape, ints_from](const params_t& p, const margs_t& in, margs_t& out) {
@@ -586,8 +589,8 @@ void register_b200_udfs(udf_manager_t& udm) {
         so.rank = si.rank;
         for (size_t r = 0; r < ord.size(); ++r) so.dims[r] = si.dims[ord[r]];
         std::vector<long long> d(si.dims, si.dims + si.rank);
-        ok(bbx_cu_ew((const float*)in.get<0>()._meta.payload(), (int)si.rank, d.data(), uop, sc, al, ord.data(),
-                     (float*)out.get<0>()._meta.payload(), p.stream));
+        ok(bbx_cu_ew((const float*)in.get<0>().payload(), (int)si.rank, d.data(), uop, sc, al, ord.data(),
+                     (float*)out.get<0>().payload(), p.stream));
       },
       [cu_shape, cu_elems](const params_t&, const margs_t& in) -> size_t { return cu_elems(cu_shape(in.get<0>())); },
       [cu_shape, ew_parse](const params_t& p, const margs_t& in, margs_t& out) {
@@ -631,9 +634,9 @@ void register_b200_udfs(udf_manager_t& udm) {
         const auto &sl = cu_shape(in.get<0>()._meta), &sr = cu_shape(in.get<1>()._meta);
         ewb_meta(ol, orr, in.get<0>()._meta, in.get<1>()._meta, out.get<0>().as<cu_t>().meta().m());
         std::vector<long long> dl(sl.dims, sl.dims + sl.rank), dr(sr.dims, sr.dims + sr.rank);
-        ok(bbx_cu_ewb((const float*)in.get<0>()._meta.payload(), (int)sl.rank, dl.data(), ol.data(),
-                      (const float*)in.get<1>()._meta.payload(), (int)sr.rank, dr.data(), orr.data(), op, al, be,
-                      (float*)out.get<0>()._meta.payload(), nullptr, nullptr, p.stream));
+        ok(bbx_cu_ewb((const float*)in.get<0>().payload(), (int)sl.rank, dl.data(), ol.data(),
+                      (const float*)in.get<1>().payload(), (int)sr.rank, dr.data(), orr.data(), op, al, be,
+                      (float*)out.get<0>().payload(), nullptr, nullptr, p.stream));
       },
       [cu_shape, cu_elems](const params_t&, const margs_t& in) -> size_t {
         return std::max(cu_elems(cu_shape(in.get<0>())), cu_elems(cu_shape(in.get<1>())));
@@ -660,9 +663,9 @@ void register_b200_udfs(udf_manager_t& udm) {
         int op = p.get_raw(0).i;
         if (op < 0 || op > 3) throw std::invalid_argument("is not a castable operator");
         std::vector<long long> d(sl.dims, sl.dims + sl.rank);
-        ok(bbx_cu_ewb((const float*)in.get<0>()._meta.payload(), (int)sl.rank, d.data(), ord.data(),
-                      (const float*)in.get<1>()._meta.payload(), (int)sr.rank, d.data(), ord.data(), op, 1.f, 1.f,
-                      (float*)out.get<0>()._meta.payload(), nullptr, nullptr, p.stream));
+        ok(bbx_cu_ewb((const float*)in.get<0>().payload(), (int)sl.rank, d.data(), ord.data(),
+                      (const float*)in.get<1>().payload(), (int)sr.rank, d.data(), ord.data(), op, 1.f, 1.f,
+                      (float*)out.get<0>().payload(), nullptr, nullptr, p.stream));
       },
       [cu_shape, cu_elems](const params_t&, const margs_t& in) -> size_t { return cu_elems(cu_shape(in.get<0>())); },
       [cu_shape](const params_t&, const margs_t& in, margs_t& out) {
@@ -679,8 +682,8 @@ void register_b200_udfs(udf_manager_t& udm) {
         auto& so = out.get<0>().as<cu_t>().meta().m();
         so.rank = (uint32_t)rank;
         for (int i = 0; i < rank; ++i) so.dims[i] = q[5 * i + 1];
-        ok(bbx_cu_expand((const float*)in.get<0>()._meta.payload(), q.data(), rank,
-                         (float*)out.get<0>()._meta.payload(), p.stream));
+        ok(bbx_cu_expand((const float*)in.get<0>().payload(), q.data(), rank,
+                         (float*)out.get<0>().payload(), p.stream));
       },
       [](const params_t& p, const margs_t&) -> size_t {
         size_t t = 1;

@@ -117,7 +117,6 @@ tfid_t tensor_factory_t::register_fmt(const std::string& name, const tensor_crea
   tfid_t id = (tfid_t)_fmt_fs.size();
   _reg_fmts[name] = id;
   _fmt_fs.push_back(fs);
-  _names.push_back(name);
   return id;
 }
 
@@ -152,7 +151,9 @@ tensor_t& tensor_factory_t::init_tensor(tensor_t* here, const tensor_meta_t& met
 
 const std::string& tensor_factory_t::fmt_name(tfid_t id) const {
   static const std::string none = "";
-  return (id >= 0 && (size_t)id < _names.size()) ? _names[id] : none;
+  for (const auto& kv : _reg_fmts)
+    if (kv.second == id) return kv.first;
+  return none;
 }
 
 }  // namespace bbts

@@ -3,10 +3,15 @@
 // format-specific meta blob (sizeof(tensor_meta_t) == 260).
 //
 // B200 residency: a block's payload lives in HBM, not behind its header. The
-// last 8 bytes of the meta blob hold the payload address ("payload slot").
-// tensor_factory_t::init_tensor sets the slot to the bytes right after the
-// header, which reproduces the reference's contiguous host layout
-// (builtin_formats.cc:18-21); block storage overrides it with a device address.
+// last 8 bytes of the meta blob hold the payload address ("payload slot") and
+// the 8 bytes before them a tag (the address XOR a constant) that marks the
+// slot as set by this library. tensor_factory_t::init_tensor sets the slot to
+// the bytes right after the header, which reproduces the reference's
+// contiguous layout (builtin_formats.cc:18-21); block storage overrides it
+// with a device address. A tensor whose slot is not tagged -- one that a
+// reference node created and initialised itself -- has its payload right
+// after the 260-byte header, as in the reference (dense_tensor_t::data(),
+// builtin_formats.h:36-39); tensor_t::payload() resolves both cases.
 #pragma once
 #include <cstddef>
 #include <cstdint>
@@ -27,6 +32,8 @@ using tfid_t = int32_t;
 struct tensor_meta_t {
   static const size_t MAX_META_SIZE = 256;
   static const size_t PAYLOAD_SLOT = MAX_META_SIZE - sizeof(void*);  // offset of the payload address
+  static const size_t PAYLOAD_TAG = PAYLOAD_SLOT - sizeof(uint64_t);  // offset of the slot's tag
+  static constexpr uint64_t kPayloadMagic = 0x62627862323030ull;      // "bbxb200"
 
   template <class T>
   T& as() const { return *((T*)this); }
@@ -34,12 +41,19 @@ struct tensor_meta_t {
   tfid_t fmt_id;
   char _blob[MAX_META_SIZE];
 
+  // The payload address this library set, or nullptr when the slot is not
+  // tagged (a meta this library did not place).
   void* payload() const {
-    void* p;
+    uint64_t p, tag;
     std::memcpy(&p, _blob + PAYLOAD_SLOT, sizeof(p));
-    return p;
+    std::memcpy(&tag, _blob + PAYLOAD_TAG, sizeof(tag));
+    return (tag ^ p) == kPayloadMagic ? (void*)p : nullptr;
   }
-  void set_payload(void* p) { std::memcpy(_blob + PAYLOAD_SLOT, &p, sizeof(p)); }
+  void set_payload(void* p) {
+    const uint64_t v = (uint64_t)p, tag = v ^ kPayloadMagic;
+    std::memcpy(_blob + PAYLOAD_SLOT, &v, sizeof(v));
+    std::memcpy(_blob + PAYLOAD_TAG, &tag, sizeof(tag));
+  }
 };
 static_assert(sizeof(tensor_meta_t) == 260, "tensor_meta_t must keep the reference layout");
 
@@ -49,6 +63,13 @@ struct tensor_t {
 
   template <class T>
   T& as() const { return *((T*)this); }
+
+  // The payload: the tagged slot's address, else the bytes after the header
+  // (the reference's layout).
+  void* payload() const {
+    void* p = _meta.payload();
+    return p ? p : (void*)((const char*)this + sizeof(tensor_meta_t));
+  }
 
   tensor_meta_t _meta;
   char _blob[0];
@@ -83,8 +104,8 @@ struct dense_tensor_meta_t : public tensor_meta_t {
 
 struct dense_tensor_t : public tensor_t {
   dense_tensor_meta_t& meta() const { return *((dense_tensor_meta_t*)&_meta); }
-  float* data() const { return (float*)_meta.payload(); }
-  void* raw() const { return _meta.payload(); }
+  float* data() const { return (float*)payload(); }
+  void* raw() const { return payload(); }
 };
 
 // "ffnn_dense": row-major FP32 with an optional bias row stored after the data
@@ -105,7 +126,7 @@ struct ffnn_dense_meta_t : public tensor_meta_t {
 
 struct ffnn_dense_t : public tensor_t {
   ffnn_dense_meta_t& meta() const { return *((ffnn_dense_meta_t*)&_meta); }
-  float* data() const { return (float*)_meta.payload(); }
+  float* data() const { return (float*)payload(); }
   float* bias() const { return data() + (size_t)meta().m().num_rows * meta().m().num_cols; }
 };
 
@@ -130,11 +151,14 @@ struct cu_meta_t : public tensor_meta_t {
 };
 struct cu_t : public tensor_t {
   cu_meta_t& meta() const { return *((cu_meta_t*)&_meta); }
-  void* data() const { return _meta.payload(); }
+  void* data() const { return payload(); }
 };
 
-// Registry of formats by name (src/tensor/tensor_factory.h:12-41). Unlike the
-// reference, register_fmt returns the new id (the reference always returns -1).
+// Registry of formats by name (src/tensor/tensor_factory.h:12-41), with the
+// reference's data members in the reference's order, so that code of this
+// library running on a reference node's factory sees the same layout.
+// register_fmt keeps the first registration of a name, as the reference does,
+// but returns the format's id (the reference always returns -1).
 class tensor_factory_t {
  public:
   tensor_factory_t();
@@ -150,7 +174,6 @@ class tensor_factory_t {
  private:
   std::unordered_map<std::string, tfid_t> _reg_fmts;
   std::vector<tensor_creation_fs_t> _fmt_fs;
-  std::vector<std::string> _names;
 };
 using tensor_factory_ptr_t = std::shared_ptr<tensor_factory_t>;
 

@@ -2,10 +2,17 @@
 // (src/ud_functions/ud_function.h:33-265, src/commands/command_utils.h:8-13),
 // kept so that a plugin written against the reference registers unchanged.
 //
+// The classes a plugin touches keep the reference's data members, in the
+// reference's order and sizes, so the plugin entry points can run against a
+// reference node's objects: ud_impl_t, ud_func_t, tensor_params_t (its cuTENSOR
+// 1.x handle is a 4 KiB struct held by value, ud_function.h:164) and
+// udf_manager_t (whose first member is the node's GPU scheduler,
+// udf_manager.h:55-66).
+//
 // Differences from the reference, by design:
 //  * tensor_params_t keeps the `stream` / `cublas_handle` / `cutensor_handle`
-//    fields for layout compatibility, but the handles are always null: no
-//    cuBLAS or cuTENSOR is used.
+//    fields, but this library never reads the handles: no cuBLAS or cuTENSOR
+//    is used.
 //  * a GPU impl's `fn` is called directly and is stream-ordered on
 //    params.stream (it returns after enqueueing), instead of being funnelled
 //    through the reference's blocking 3-stream GPU scheduler
@@ -16,6 +23,7 @@
 #include <functional>
 #include <memory>
 #include <string>
+#include <unordered_map>
 #include <vector>
 #include "tensor.h"
 
@@ -45,6 +53,12 @@ using ud_impl_local_t = int32_t;
 struct ud_impl_id_t {
   ud_id_t ud_id;
   ud_impl_local_t impl_id;
+};
+
+// Stand-in with the size and alignment of cuTENSOR 1.x's cutensorHandle_t,
+// an opaque struct of 512 int64 words passed by address to the library.
+struct cutensor_handle_t {
+  int64_t fields[512];
 };
 
 struct ud_impl_t {
@@ -86,8 +100,8 @@ struct ud_impl_t {
 
     command_param_list_t _params;
     cudaStream_t stream = nullptr;
-    void* cublas_handle = nullptr;    // always null in this build
-    void* cutensor_handle = nullptr;  // always null in this build
+    void* cublas_handle = nullptr;       // never read by this library
+    cutensor_handle_t cutensor_handle{};  // never read by this library
   };
 
   using ud_impl_callable =
@@ -161,6 +175,9 @@ class udf_manager_t {
   const tensor_factory_ptr_t& factory() const { return _tensor_factory; }
 
  private:
+  // the reference node's GPU scheduler (gpu_scheduler_ptr_t); this library
+  // schedules on streams and leaves it empty
+  std::shared_ptr<void> _gpu_scheduler;
   tensor_factory_ptr_t _tensor_factory;
   std::vector<ud_func_ptr_t> _udfs;
   std::unordered_map<std::string, ud_id_t> _udfs_name_to_id;
