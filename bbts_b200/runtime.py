@@ -112,6 +112,16 @@ class Runtime:
         arr = np.ascontiguousarray(arr, dtype=np.float32)
         self.put(tid, dense_meta(self.fmt(fmt), arr.shape[0], arr.shape[1]), arr)
 
+    def fill_philox(self, tid, seed, dist=0, a=0.0, b=1.0):
+        """Fills tensor `tid`'s payload on the device with the seeded Philox
+        generator: dist 0 = U(a, b), 1 = N(a, b^2), in the block's element type
+        (f32 unless the format is dense_bf16)."""
+        ptr, nbytes = self.payload(tid)
+        fmt_id = struct.unpack_from("<i", self.meta(tid), 0)[0]
+        bf16 = fmt_id == self.fmt("dense_bf16")
+        check(lib.bbx_fill_philox(1 if bf16 else 0, ptr, nbytes // (2 if bf16 else 4), int(seed), int(dist),
+                                  float(a), float(b), self.stream))
+
     def meta(self, tid):
         m = C.create_string_buffer(META_BYTES)
         check(lib.bbx_rt_tensor_get(self.h, tid, m, None, 0, 0))
@@ -317,6 +327,26 @@ class Dag:
         buf = np.empty(nbytes, np.uint8)
         check(lib.bbx_dag_read(self.h, tid, buf.ctypes.data, nbytes))
         return buf
+
+    def write(self, tid, src_ptr, nbytes, on_device=False, stream=None):
+        """Enqueues a copy of `nbytes` at address `src_ptr` (host, or device
+        with on_device) into input block `tid` on `stream` (default: the
+        runtime's). Pinned host memory makes it asynchronous."""
+        check(lib.bbx_dag_write(self.h, tid, C.c_void_p(src_ptr), nbytes, int(on_device),
+                                stream if stream is not None else self.rt.stream))
+
+    def fetch(self, tid, dst_ptr, cap, on_device=False, stream=None):
+        """Enqueues a copy of up to `cap` payload bytes of `tid` to `dst_ptr`."""
+        check(lib.bbx_dag_fetch(self.h, tid, C.c_void_p(dst_ptr), cap, int(on_device),
+                                stream if stream is not None else self.rt.stream))
+
+    def group_tiles(self):
+        """Tile of each launch group, in profile order (0 for non-tensor-core groups)."""
+        n = C.c_int()
+        check(lib.bbx_dag_group_tiles(self.h, 0, None, C.byref(n)))
+        out = (C.c_int * max(1, n.value))()
+        check(lib.bbx_dag_group_tiles(self.h, n.value, out, C.byref(n)))
+        return [int(x) for x in out[:n.value]]
 
     def close(self):
         if self.h:

@@ -42,13 +42,9 @@ def _dtype_fmt(dtype):
 def fill_block(rt, tid, rows, cols, fmt, seed, dist="normal"):
     """Registers a rows x cols block filled on the device by the seeded Philox
     generator: N(0,1) (dist="normal") or U(-1,1) (dist="uniform")."""
-    from ._lib import lib, check
-    fid = rt.fmt(fmt)
-    rt.put(tid, dense_meta(fid, rows, cols))
-    ptr, _ = rt.payload(tid)
-    dt = 1 if fmt == "dense_bf16" else 0
+    rt.put(tid, dense_meta(rt.fmt(fmt), rows, cols))
     d, a, b = (1, 0.0, 1.0) if dist == "normal" else (0, -1.0, 1.0)
-    check(lib.bbx_fill_philox(dt, ptr, rows * cols, int(seed), d, a, b, rt.stream))
+    rt.fill_philox(tid, int(seed), d, a, b)
 
 
 def put_block(rt, tid, arr, fmt):
@@ -103,27 +99,27 @@ def bmm(rt, n=4096, split=4, dtype="f32", out_dtype=None, seed=0, host=True, dis
     return {"A": A, "B": B, "C": C, "hostA": hostA, "hostB": hostB, "flops": e.flops, "bs": bs, "split": split}
 
 
-def cpmm(rt, rows=8, cols=8, bs=4096, dtype="bf16", seed=0, host=False):
-    """C = A.B with A an (rows x 1) and B a (1 x cols) grid of bs x bs blocks:
-    rows*cols independent matrix_mult ops, no reduce."""
+def cpmm_seeds(seed, rows, cols):
+    """Philox seeds of the A row blocks and the B column blocks of cpmm."""
+    return [seed + i for i in range(rows)], [seed + 1000 + j for j in range(cols)]
+
+
+def cpmm(rt, rows=8, cols=8, bs=4096, dtype="bf16", seed=0):
+    """C = A.B with A an (rows x 1) and B a (1 x cols) grid of bs x bs blocks
+    (applications/cpmm/generate_cpmm.cc:228-274 on one node, without its
+    shuffle): rows*cols independent matrix_mult APPLYs, no reduce, FP32
+    output blocks. Inputs are U(-1,1) from the seeded Philox generator on the
+    device (cpmm_seeds), rounded to the input format."""
     e = Emitter(rt)
     fmt = _dtype_fmt(dtype)
-    rng = _rng(seed)
-    A, B, hA, hB = {}, {}, {}, {}
+    sa, sb = cpmm_seeds(seed, rows, cols)
+    A, B = {}, {}
     for i in range(rows):
-        t = e.tid()
-        x = rng.uniform(-1, 1, (bs, bs)).astype(np.float32)
-        put_block(rt, t, x, fmt)
-        A[i] = t
-        if host:
-            hA[i] = x
+        A[i] = e.tid()
+        fill_block(rt, A[i], bs, bs, fmt, seed=sa[i], dist="uniform")
     for j in range(cols):
-        t = e.tid()
-        x = rng.uniform(-1, 1, (bs, bs)).astype(np.float32)
-        put_block(rt, t, x, fmt)
-        B[j] = t
-        if host:
-            hB[j] = x
+        B[j] = e.tid()
+        fill_block(rt, B[j], bs, bs, fmt, seed=sb[j], dist="uniform")
     mm = rt.impl("matrix_mult", [fmt, fmt], ["dense"])
     C = {}
     for i in range(rows):
@@ -132,7 +128,7 @@ def cpmm(rt, rows=8, cols=8, bs=4096, dtype="bf16", seed=0, host=False):
             rt.apply(mm, [A[i], B[j]], [t])
             C[(i, j)] = t
             e.flops += 2.0 * bs ** 3
-    return {"A": A, "B": B, "C": C, "hostA": hA, "hostB": hB, "flops": e.flops}
+    return {"A": A, "B": B, "C": C, "flops": e.flops, "bs": bs, "seeds": (sa, sb), "fmt": fmt}
 
 
 def ffnn(rt, batch=16384, d_in=8192, h1=8192, h2=4096, classes=1024, bs=2048, seed=0, host=False,
@@ -179,11 +175,8 @@ def ffnn(rt, batch=16384, d_in=8192, h1=8192, h2=4096, classes=1024, bs=2048, se
             put_block(rt, t, x, B16)
             host_vals[t] = x
         else:
-            from ._lib import lib, check
             rt.put(t, dense_meta(rt.fmt(B16), rows, cols))
-            ptr, _ = rt.payload(t)
-            check(lib.bbx_fill_philox(1 if B16 == "dense_bf16" else 0, ptr, rows * cols, int(rng.integers(1 << 62)),
-                                      1, 0.0, float(std), rt.stream))
+            rt.fill_philox(t, int(rng.integers(1 << 62)), 1, 0.0, float(std))
         return t
 
     X = {(i, k): inp(bs, bs, 1.0) for i in range(R) for k in range(KI)}
@@ -326,10 +319,8 @@ def random_dag(rt, n_ops=2000, depth=8, seed=0, dtype="bf16", lo=128, hi=2048, s
             rt.put(t, cutensor_meta(cfmt, dims), x)
             host_inputs[t] = x
         else:
-            from ._lib import lib, check
             rt.put(t, cutensor_meta(cfmt, dims))
-            ptr, _ = rt.payload(t)
-            check(lib.bbx_fill_philox(0, ptr, int(np.prod(dims)), int(rng.integers(1 << 62)), 1, 0.0, 1.0, rt.stream))
+            rt.fill_philox(t, int(rng.integers(1 << 62)), 1, 0.0, 1.0)
         return t
 
     def pick(pool, pred):

@@ -384,6 +384,64 @@ def test_bbts_program_bmm(R, tmp_path):
             assert rel_err(get(t), ref[i * 256:(i + 1) * 256, j * 256:(j + 1) * 256]) <= 1e-5
 
 
+def test_bbts_program_cpmm(R, tmp_path):
+    """The cross-product blocked matmul program (single-node form of
+    applications/cpmm/generate_cpmm.cc, k-grid 2 so it reduces) in the .bbts
+    format: inputs generated in-program by the uniform ud from explicit seeds,
+    run per-op and as a grouped DAG, against FP64 of the stored inputs."""
+    runtime, _ = R
+    from bbts_b200 import programs
+    path = str(tmp_path / "cpmm.bbts")
+    bs = 256
+    A, B, C = programs.cpmm_bbts(path, rows=2, cols=3, bs=bs, k=2)
+    for mode in ("per_op", "dag"):
+        rt = runtime.Runtime()
+        assert rt.load_program(path) == 4 + 6 + 12 + 6 + 1
+        if mode == "per_op":
+            rt.run()
+            get = lambda t: rt.get_dense(t)
+        else:
+            dag = rt.build_dag(runtime.HEURISTIC, tile_n=runtime.AUTOTUNE)
+            dag.launch()
+            get = lambda t: dag.read_bytes(t, bs * bs * 4).view(np.float32).reshape(bs, bs)
+        a = {key: read_dense(rt, t) for key, t in A.items()}
+        b = {key: read_dense(rt, t) for key, t in B.items()}
+        assert a[(0, 0)].min() >= -1.0 and a[(0, 0)].max() < 1.0 and not np.array_equal(a[(0, 0)], a[(1, 0)])
+        for (i, j), t in C.items():
+            ref = sum(oracle.matmul_f64(a[(i, kk)], b[(kk, j)]) for kk in range(2))
+            assert rel_err(get(t), ref) <= 1e-5, (mode, i, j)
+        if mode == "dag":
+            dag.close()
+        rt.close()
+
+
+def test_bbts_program_ffnn_matches_the_emitter(R, tmp_path):
+    """The blocked FFN step written as a .bbts program (ffnn_bbts) and loaded
+    into a runtime that holds the same input blocks gives exactly the blocks
+    of the same step queued directly by the emitter."""
+    runtime, workloads = R
+    from bbts_b200 import programs
+    args = dict(batch=512, d_in=256, h1=256, h2=256, classes=128, bs=128, seed=3, dtype="bf16", split_a1=True)
+    path = str(tmp_path / "ffnn.bbts")
+    _, inputs = programs.ffnn_bbts(path, **args)
+    rt1 = runtime.Runtime()
+    info = workloads.ffnn(rt1, **args)
+    rt1.run()
+    rt2 = runtime.Runtime()
+    workloads.ffnn(rt2, **args)   # the same input blocks (same seeds); its queued commands are dropped
+    rt2.clear_commands()
+    n = rt2.load_program(path)
+    assert n > 0 and set(inputs) == set(info["X"].values()) | set(info["W1"].values()) | set(info["W2"].values()) \
+        | set(info["W3"].values()) | set(info["labels"].values())
+    rt2.run()
+    outs = list(info["dW1"].values()) + list(info["dW2"].values()) + list(info["dW3"].values()) + \
+        list(info["loss"].values())
+    for t in outs:
+        assert np.array_equal(rt1.get_bytes(t), rt2.get_bytes(t)), t
+    rt1.close()
+    rt2.close()
+
+
 def test_sbbts_program(R, tmp_path):
     runtime, _ = R
     from bbts_b200 import programs
