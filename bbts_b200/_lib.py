@@ -102,6 +102,11 @@ SIGNATURES = {
                             C.POINTER(i32), C.POINTER(i32), C.POINTER(sz)]),
     "bbx_dag_tensor": (i32, [vp, i32, C.POINTER(vp), vp]),
     "bbx_dag_read": (i32, [vp, i32, vp, sz]),
+    "bbx_stream_plan_create_kernel": (i32, [vp, i32, i32, C.POINTER(vp)]),
+    "bbx_rt_set_dag_stream_kernel": (i32, [vp, i32]),
+    "bbx_dag_write": (i32, [vp, i32, vp, sz, i32, vp]),
+    "bbx_dag_fetch": (i32, [vp, i32, vp, sz, i32, vp]),
+    "bbx_dag_group_tiles": (i32, [vp, i32, vp, C.POINTER(i32)]),
     # learned cost model
     "bbx_mlp_create": (i32, [u64, C.POINTER(vp)]),
     "bbx_mlp_destroy": (i32, [vp]),

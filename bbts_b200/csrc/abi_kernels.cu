@@ -110,7 +110,8 @@ int device_state(DeviceState** out) {
   DeviceState& d = g_dev[dev];
   if (!d.ready) {
     BBX_CUDA(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
-    BBX_CUDA(cudaMalloc(&d.status, 256));
+    // a failed earlier set-up keeps its status buffer: allocate it only once
+    if (!d.status) BBX_CUDA(cudaMalloc(&d.status, 256));
     BBX_CUDA(cudaMemset(d.status, 0, 256));
     // Dynamic shared-memory opt-in for every tcgen05 variant, once, here: never
     // inside a stream capture.
@@ -387,7 +388,16 @@ int bbx_matmul_f32(const float* a, const float* b, float* c, int m, int n, int k
   g.alpha = alpha; g.beta = beta; g.relu = relu;
   dim3 grid((n + F32_BN - 1) / F32_BN, (m + F32_BM - 1) / F32_BM, batch);
   if (grid.y > 65535) return set_error(BBX_ERR_INVALID, "m too large");
-  k_gemm_f32<<<grid, 256, 0, (cudaStream_t)stream>>>(g);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (f32_gemm_vector_ok(g)) {
+    if (!trans_a && !trans_b) k_gemm_f32_v<false, false><<<grid, 256, 0, st>>>(g);
+    else if (!trans_a) k_gemm_f32_v<false, true><<<grid, 256, 0, st>>>(g);
+    else if (!trans_b) k_gemm_f32_v<true, false><<<grid, 256, 0, st>>>(g);
+    else k_gemm_f32_v<true, true><<<grid, 256, 0, st>>>(g);
+    BBX_CHECK_LAUNCH("k_gemm_f32_v");
+    return BBX_OK;
+  }
+  k_gemm_f32<<<grid, 256, 0, st>>>(g);
   BBX_CHECK_LAUNCH("k_gemm_f32");
   return BBX_OK;
 }
@@ -611,21 +621,16 @@ int bbx_quantize_e4m3(int src_dtype, const void* in, void* out, int rows, int co
   int rc = device_state(&d);
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
-  const long long n = (long long)rows * cols;
-  const int grid = grid_for(n, 256, d->sms);
   // the absmax word is stream-ordered scratch of this call, so quantisations
   // on different streams never share it
   unsigned int* amax = nullptr;
   BBX_CUDA(cudaMallocAsync((void**)&amax, 4, st));
   BBX_CUDA(cudaMemsetAsync(amax, 0, 4, st));
-  if (src_dtype == BBX_F32) {
-    k_absmax<float><<<grid, 256, 0, st>>>((const float*)in, n, amax);
-    k_quant_e4m3<float><<<grid, 256, 0, st>>>((const float*)in, (__nv_fp8_e4m3*)out, rows, cols, amax, scale_out, transpose);
-  } else {
-    k_absmax<__nv_bfloat16><<<grid, 256, 0, st>>>((const __nv_bfloat16*)in, n, amax);
-    k_quant_e4m3<__nv_bfloat16><<<grid, 256, 0, st>>>((const __nv_bfloat16*)in, (__nv_fp8_e4m3*)out, rows, cols, amax, scale_out, transpose);
-  }
-  cudaError_t le = cudaGetLastError();
+  cudaError_t le = src_dtype == BBX_F32
+                       ? launch_quantize_block((const float*)in, (uint8_t*)out, rows, cols, transpose, amax,
+                                               scale_out, d->sms, st)
+                       : launch_quantize_block((const __nv_bfloat16*)in, (uint8_t*)out, rows, cols, transpose,
+                                               amax, scale_out, d->sms, st);
   cudaFreeAsync(amax, st);
   if (le != cudaSuccess) return set_error(BBX_ERR_CUDA, "quantize_e4m3: %s", cudaGetErrorString(le));
   return BBX_OK;
@@ -721,7 +726,7 @@ namespace bbx {
 // aligned); the table then counts items of bulk_tile elements instead of
 // kStreamChunk chunks.
 static int build_stream_table(const bbx_stream_op_t* ops, int count, std::vector<StreamOp>* out,
-                              long long* total, bool* bulk) {
+                              long long* total, bool* bulk, bool allow_bulk = true) {
   static_assert(kStreamMaxIn == BBX_STREAM_MAX_IN, "stream op fan-in mismatch");
   out->resize(count);
   // Blocks stride over the chunk list (block b takes chunks b, b + grid, ...),
@@ -765,8 +770,8 @@ static int build_stream_table(const bbx_stream_op_t* ops, int count, std::vector
   *total = chunks;
   bool all16 = true;
   for (const StreamOp& o : *out) all16 = all16 && (o.n == 0 || o.vec == 2);
-  *bulk = all16;
-  if (all16) {
+  *bulk = all16 && allow_bulk;
+  if (*bulk) {
     long long items = 0;
     for (StreamOp& o : *out) {
       o.tile = bulk_tile(o.n_in, o.in_dtype == BBX_BF16 ? 2 : 4, o.out_dtype == BBX_BF16 ? 2 : 4);
@@ -782,11 +787,17 @@ static int build_stream_table(const bbx_stream_op_t* ops, int count, std::vector
 extern "C" {
 
 int bbx_stream_plan_create(const bbx_stream_op_t* ops, int count, bbx_stream_plan_t** out) {
+  return bbx_stream_plan_create_kernel(ops, count, BBX_STREAM_KERNEL_AUTO, out);
+}
+
+int bbx_stream_plan_create_kernel(const bbx_stream_op_t* ops, int count, int kernel, bbx_stream_plan_t** out) {
   if (!ops || count <= 0 || !out) return set_error(BBX_ERR_INVALID, "bad stream plan arguments");
+  if (kernel != BBX_STREAM_KERNEL_AUTO && kernel != BBX_STREAM_KERNEL_REGISTER)
+    return set_error(BBX_ERR_INVALID, "stream plan kernel %d", kernel);
   std::vector<StreamOp> table;
   long long total = 0;
   bool bulk = false;
-  int rc = build_stream_table(ops, count, &table, &total, &bulk);
+  int rc = build_stream_table(ops, count, &table, &total, &bulk, kernel == BBX_STREAM_KERNEL_AUTO);
   if (rc) return rc;
   auto* p = new bbx_stream_plan();
   p->count = count;

@@ -161,4 +161,164 @@ __global__ void __launch_bounds__(256) k_gemm_f32(const __grid_constant__ F32Gem
   }
 }
 
+// ---------------------------------------------------------------------------
+// Vector-load variant for aligned operands (the blocks of the plain FP32 path):
+// 128x128 tile, BK = 16, 256 threads, the same 8x8 outputs per thread.
+// Every global load is one 16-byte load along the operand's contiguous
+// dimension; the K-contiguous operands (A row-major, B transposed) are stored
+// transposed into shared memory, the MN-contiguous ones directly. Rows of the
+// shared tiles are padded by 4 floats so the transposed stores spread over the
+// banks and float4 reads stay 16-byte aligned. Two CTAs fit on an SM
+// (33 KB shared memory, <= 128 registers). The epilogue stores float4 rows of
+// C when C's rows allow it.
+// Requirements (checked by the host): a, b 16-byte aligned; lda, ldb and the
+// batch strides multiples of 4; the contiguous extent of each operand (k for
+// row-major A / transposed B, m for transposed A, n for row-major B) a
+// multiple of 4, so a 16-byte piece is either wholly inside the matrix or
+// wholly outside.
+constexpr int F32V_BK = 16, F32V_LD = F32_BM + 4;
+
+__device__ __forceinline__ float4 ldg4_or_zero(const float* p, bool ok) {
+  return ok ? __ldg((const float4*)p) : make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(256, 1) k_gemm_f32_v(const __grid_constant__ F32GemmArgs g) {
+  __shared__ __align__(16) float As[2][F32V_BK][F32V_LD];
+  __shared__ __align__(16) float Bs[2][F32V_BK][F32V_LD];
+
+  const int bz = blockIdx.z;
+  const float* A = g.a + bz * g.stride_a;
+  const float* B = g.b + bz * g.stride_b;
+  float* Cp = g.c + bz * g.stride_c;
+  const int m0 = blockIdx.y * F32_BM;
+  const int n0 = blockIdx.x * F32_BN;
+  const int tid = threadIdx.x;
+  const int tx = tid & 15, ty = tid >> 4;
+
+  // 128 x 16 (A) and 16 x 128 (B) tiles = 512 float4 each: two per thread.
+  // K-contiguous: piece f -> row f / 4, k-quad (f % 4) * 4.
+  // MN-contiguous: piece f -> k f / 32, quad (f % 32) * 4.
+  float4 ra[2], rb[2];
+  auto load = [&](int k0) {
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int f = tid + 256 * i;
+      if (!TA) {
+        const int gm = m0 + (f >> 2), gk = k0 + (f & 3) * 4;
+        ra[i] = ldg4_or_zero(A + (long long)gm * g.lda + gk, gm < g.m && gk < g.k);
+      } else {
+        const int gk = k0 + (f >> 5), gm = m0 + (f & 31) * 4;
+        ra[i] = ldg4_or_zero(A + (long long)gk * g.lda + gm, gk < g.k && gm < g.m);
+      }
+      if (!TB) {
+        const int gk = k0 + (f >> 5), gn = n0 + (f & 31) * 4;
+        rb[i] = ldg4_or_zero(B + (long long)gk * g.ldb + gn, gk < g.k && gn < g.n);
+      } else {
+        const int gn = n0 + (f >> 2), gk = k0 + (f & 3) * 4;
+        rb[i] = ldg4_or_zero(B + (long long)gn * g.ldb + gk, gn < g.n && gk < g.k);
+      }
+    }
+  };
+  auto store = [&](int buf) {
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int f = tid + 256 * i;
+      if (!TA) {
+        const int r = f >> 2, kq = (f & 3) * 4;
+        As[buf][kq][r] = ra[i].x; As[buf][kq + 1][r] = ra[i].y;
+        As[buf][kq + 2][r] = ra[i].z; As[buf][kq + 3][r] = ra[i].w;
+      } else {
+        *(float4*)&As[buf][f >> 5][(f & 31) * 4] = ra[i];
+      }
+      if (!TB) {
+        *(float4*)&Bs[buf][f >> 5][(f & 31) * 4] = rb[i];
+      } else {
+        const int r = f >> 2, kq = (f & 3) * 4;
+        Bs[buf][kq][r] = rb[i].x; Bs[buf][kq + 1][r] = rb[i].y;
+        Bs[buf][kq + 2][r] = rb[i].z; Bs[buf][kq + 3][r] = rb[i].w;
+      }
+    }
+  };
+
+  float acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+
+  const int ktiles = (g.k + F32V_BK - 1) / F32V_BK;
+  load(0);
+  store(0);
+  __syncthreads();
+  for (int kt = 0; kt < ktiles; ++kt) {
+    const int buf = kt & 1;
+    if (kt + 1 < ktiles) load((kt + 1) * F32V_BK);
+#pragma unroll
+    for (int kk = 0; kk < F32V_BK; ++kk) {
+      const float4 a0 = *(const float4*)&As[buf][kk][ty * 4];
+      const float4 a1 = *(const float4*)&As[buf][kk][ty * 4 + 64];
+      const float4 b0 = *(const float4*)&Bs[buf][kk][tx * 4];
+      const float4 b1 = *(const float4*)&Bs[buf][kk][tx * 4 + 64];
+      const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+      const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+    }
+    if (kt + 1 < ktiles) store(buf ^ 1);
+    __syncthreads();
+  }
+
+  const bool vec_c = ((((uintptr_t)Cp) & 15) == 0) && (g.ldc & 3) == 0 && (g.n & 3) == 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int gm = m0 + ty * 4 + (i & 3) + (i >> 2) * 64;
+    if (gm >= g.m) continue;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int gn = n0 + tx * 4 + h * 64;
+      if (gn >= g.n) continue;
+      float v[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) v[q] = g.alpha * acc[i][4 * h + q];
+      float* cp = Cp + (long long)gm * g.ldc + gn;
+      if (vec_c) {  // n % 4 == 0: the four columns are all inside
+        if (g.beta != 0.f) {
+          const float4 o = *(const float4*)cp;
+          v[0] += g.beta * o.x; v[1] += g.beta * o.y; v[2] += g.beta * o.z; v[3] += g.beta * o.w;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if (g.bias) v[q] += g.bias[gn + q];
+          if (g.relu) v[q] = v[q] > 0.f ? v[q] : 0.f;
+        }
+        *(float4*)cp = make_float4(v[0], v[1], v[2], v[3]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if (gn + q >= g.n) break;
+          float x = v[q];
+          if (g.beta != 0.f) x += g.beta * cp[q];
+          if (g.bias) x += g.bias[gn + q];
+          if (g.relu) x = x > 0.f ? x : 0.f;
+          cp[q] = x;
+        }
+      }
+    }
+  }
+}
+
+// True when k_gemm_f32_v's requirements hold for these operands.
+inline bool f32_gemm_vector_ok(const F32GemmArgs& g) {
+  auto a16 = [](const void* p) { return (((uintptr_t)p) & 15) == 0; };
+  if (!a16(g.a) || !a16(g.b) || (g.lda & 3) || (g.ldb & 3) || (g.stride_a & 3) || (g.stride_b & 3)) return false;
+  if (!g.trans_a && (g.k & 3)) return false;
+  if (g.trans_a && (g.m & 3)) return false;
+  if (!g.trans_b && (g.n & 3)) return false;
+  if (g.trans_b && (g.k & 3)) return false;
+  return true;
+}
+
 }  // namespace bbx

@@ -731,7 +731,8 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
     for (size_t ph = 0; ph < phases.size(); ++ph) {
       if (phases[ph].empty()) continue;
       group_t g{G_STREAM, w};
-      dag_bbx(bbx_stream_plan_create(phases[ph].data(), (int)phases[ph].size(), &g.stream_plan));
+      dag_bbx(bbx_stream_plan_create_kernel(phases[ph].data(), (int)phases[ph].size(), rt->dag_stream_kernel,
+                                            &g.stream_plan));
       g.bytes = stream_group_bytes(phases[ph]);
       g.reads = phase_rw[ph].first;
       g.writes = phase_rw[ph].second;
@@ -910,6 +911,21 @@ void* dag_tensor(const dag_t* d, tid_t tid, tensor_meta_t* meta) {
 size_t dag_payload_bytes(const dag_t* d, tid_t tid) {
   auto it = d->tensors.find(tid);
   return it == d->tensors.end() ? 0 : it->second.bytes;
+}
+
+// 1 when `tid` is a block the DAG reads in place from storage (an input that
+// no command of the DAG writes), 0 otherwise.
+int dag_is_input(const dag_t* d, tid_t tid) {
+  auto it = d->tensors.find(tid);
+  return it != d->tensors.end() && it->second.external && it->second.def < 0 ? 1 : 0;
+}
+
+// Tile of each launch group (128, 256, 512 = 2-SM pair) for tensor-core
+// groups, 0 for the others.
+std::vector<int> dag_group_tiles(const dag_t* d) {
+  std::vector<int> out;
+  for (auto& g : d->groups) out.push_back(g.kind == G_TC && g.tc_plan ? bbx_tc_plan_tile_n(g.tc_plan) : 0);
+  return out;
 }
 
 void tile_record(bool on) {

@@ -21,6 +21,8 @@ struct bbx_dag {
 namespace bbts {
 void* dag_tensor(const dag_t* d, tid_t tid, tensor_meta_t* meta);
 size_t dag_payload_bytes(const dag_t* d, tid_t tid);
+int dag_is_input(const dag_t* d, tid_t tid);
+std::vector<int> dag_group_tiles(const dag_t* d);
 runtime_t* rt_of(bbx_rt* rt) { return &rt->rt; }
 }
 
@@ -429,6 +431,48 @@ int bbx_dag_read(bbx_dag_t* dag, int tid, void* host_dst, size_t cap) {
     if (e == cudaSuccess) e = cudaMemcpy(host_dst, p, n, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) throw std::runtime_error(std::string("dag_read: ") + cudaGetErrorString(e));
   });
+}
+
+int bbx_rt_set_dag_stream_kernel(bbx_rt_t* rt, int kernel) {
+  if (!rt) return bbx::set_error(BBX_ERR_INVALID, "null runtime");
+  if (kernel != BBX_STREAM_KERNEL_AUTO && kernel != BBX_STREAM_KERNEL_REGISTER)
+    return bbx::set_error(BBX_ERR_INVALID, "dag stream kernel %d", kernel);
+  rt->rt.dag_stream_kernel = kernel;
+  return BBX_OK;
+}
+
+int bbx_dag_write(bbx_dag_t* dag, int tid, const void* src, size_t bytes, int src_on_device, void* stream) {
+  if (!dag || (!src && bytes)) return bbx::set_error(BBX_ERR_INVALID, "null argument");
+  void* p = dag_tensor(dag->d, tid, nullptr);
+  if (!p) return bbx::set_error(BBX_ERR_NOT_FOUND, "DAG has no tensor %d", tid);
+  if (!dag_is_input(dag->d, tid))
+    return bbx::set_error(BBX_ERR_INVALID, "tensor %d is not an input the DAG reads in place", tid);
+  if (bytes > dag_payload_bytes(dag->d, tid))
+    return bbx::set_error(BBX_ERR_INVALID, "dag_write: %zu bytes into a %zu-byte block", bytes,
+                          dag_payload_bytes(dag->d, tid));
+  if (!bytes) return BBX_OK;
+  cudaError_t e = cudaMemcpyAsync(p, src, bytes, src_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                  (cudaStream_t)stream);
+  return e == cudaSuccess ? BBX_OK : bbx::set_error(BBX_ERR_CUDA, "dag_write: %s", cudaGetErrorString(e));
+}
+
+int bbx_dag_fetch(bbx_dag_t* dag, int tid, void* dst, size_t cap, int dst_on_device, void* stream) {
+  if (!dag || (!dst && cap)) return bbx::set_error(BBX_ERR_INVALID, "null argument");
+  void* p = dag_tensor(dag->d, tid, nullptr);
+  if (!p) return bbx::set_error(BBX_ERR_NOT_FOUND, "DAG has no tensor %d", tid);
+  const size_t n = std::min(cap, dag_payload_bytes(dag->d, tid));
+  if (!n) return BBX_OK;
+  cudaError_t e = cudaMemcpyAsync(dst, p, n, dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                  (cudaStream_t)stream);
+  return e == cudaSuccess ? BBX_OK : bbx::set_error(BBX_ERR_CUDA, "dag_fetch: %s", cudaGetErrorString(e));
+}
+
+int bbx_dag_group_tiles(bbx_dag_t* dag, int cap, int* tiles, int* n_out) {
+  if (!dag) return bbx::set_error(BBX_ERR_INVALID, "null dag");
+  auto t = dag_group_tiles(dag->d);
+  for (int i = 0; i < cap && i < (int)t.size(); ++i) tiles[i] = t[i];
+  if (n_out) *n_out = (int)t.size();
+  return BBX_OK;
 }
 
 }  // extern "C"

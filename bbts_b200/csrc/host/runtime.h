@@ -180,6 +180,8 @@ class runtime_t {
   // predicted time of a grouped tensor-core launch per tile (dag_build with
   // tile_n = -2), from tile_features rows; installed from a trained MLP
   std::function<std::vector<double>(const std::vector<op_features_t>&)> tile_predictor;
+  // kernel of a compiled DAG's grouped streaming launches (BBX_STREAM_KERNEL_*)
+  int dag_stream_kernel = 0;
 
   // Worker streams of the per-op path: the reference pulls ready commands from
   // the reservation station with num_threads workers (src/server/node.cc:67-69);

@@ -66,6 +66,7 @@ using namespace bbx;
 extern "C" int bbx_quantize_e4m3_batched_noalloc(int src_dtype, const void* const* in, void* const* out,
                                                  int count, int rows, int cols, int transpose,
                                                  float* scales_out, void* stream) {
+  if (count == 0) return BBX_OK;  // an empty batch touches nothing, null arrays included
   if (!in || !out || !scales_out || rows <= 0 || cols <= 0 || count < 0)
     return set_error(BBX_ERR_INVALID, "bad no-alloc quantize arguments");
   if (count > kNoAllocMaxBlocks)
@@ -76,7 +77,6 @@ extern "C" int bbx_quantize_e4m3_batched_noalloc(int src_dtype, const void* cons
   if (src_dtype != BBX_F32 && src_dtype != BBX_BF16) return set_error(BBX_ERR_UNSUPPORTED, "quantize source dtype");
   for (int i = 0; i < count; ++i)
     if (!in[i] || !out[i]) return set_error(BBX_ERR_INVALID, "null block pointer %d", i);
-  if (count == 0) return BBX_OK;
   unsigned int* scratch = nullptr;
   int sms = 0;
   int rc = noalloc_scratch(&scratch, &sms);
@@ -85,20 +85,13 @@ extern "C" int bbx_quantize_e4m3_batched_noalloc(int src_dtype, const void* cons
   // the array keeps the previous call's words: clear the ones this call uses
   cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(unsigned int) * count, st);
   if (e != cudaSuccess) return set_error(BBX_ERR_CUDA, "cudaMemsetAsync(no-alloc scratch): %s", cudaGetErrorString(e));
-  const long long n = (long long)rows * cols;
-  long long blocks = (n + 255) / 256;
-  if (blocks > (long long)sms * 8) blocks = (long long)sms * 8;
-  const int grid = (int)(blocks < 1 ? 1 : blocks);
   for (int i = 0; i < count; ++i) {
-    if (src_dtype == BBX_F32) {
-      k_absmax<float><<<grid, 256, 0, st>>>((const float*)in[i], n, scratch + i);
-      k_quant_e4m3<float><<<grid, 256, 0, st>>>((const float*)in[i], (__nv_fp8_e4m3*)out[i], rows, cols,
-                                                 scratch + i, scales_out + i, transpose);
-    } else {
-      k_absmax<__nv_bfloat16><<<grid, 256, 0, st>>>((const __nv_bfloat16*)in[i], n, scratch + i);
-      k_quant_e4m3<__nv_bfloat16><<<grid, 256, 0, st>>>((const __nv_bfloat16*)in[i], (__nv_fp8_e4m3*)out[i], rows,
-                                                         cols, scratch + i, scales_out + i, transpose);
-    }
+    e = src_dtype == BBX_F32
+            ? launch_quantize_block((const float*)in[i], (uint8_t*)out[i], rows, cols, transpose, scratch + i,
+                                    scales_out + i, sms, st)
+            : launch_quantize_block((const __nv_bfloat16*)in[i], (uint8_t*)out[i], rows, cols, transpose,
+                                    scratch + i, scales_out + i, sms, st);
+    if (e != cudaSuccess) return set_error(BBX_ERR_CUDA, "no-alloc quantize launch: %s", cudaGetErrorString(e));
   }
   e = cudaGetLastError();
   if (e != cudaSuccess) return set_error(BBX_ERR_CUDA, "no-alloc quantize launch: %s", cudaGetErrorString(e));

@@ -248,6 +248,12 @@ class Runtime:
         check(lib.bbx_rt_set_tile_predictor(self.h, mlp.h if mlp is not None else None))
         self._tile_predictor = mlp
 
+    def set_dag_stream_kernel(self, kernel):
+        """Streaming kernel of DAGs built afterwards: 0 = bulk-staged where
+        aligned (default), 1 = the register kernel (shares SMs with tensor-core
+        launches)."""
+        check(lib.bbx_rt_set_dag_stream_kernel(self.h, int(kernel)))
+
     def build_dag(self, policy=HEURISTIC, tile_n=0):
         return Dag(self, policy, tile_n)
 

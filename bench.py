@@ -1,18 +1,22 @@
 """Block-op DAG throughput on one B200 (or N independent replicas).
 
-Workload (cross-product blocked matmul): C = A.B with A 32768x4096 and B
-4096x32768 split into 4096x4096 blocks (8x1 and 1x8 grids), entries U(-1,1),
-BF16 inputs, FP32 accumulation and FP32 output: 64 independent matrix_mult
-block ops, 2*32768^2*4096 = 8.796 TFLOP per step. A step runs the whole DAG
-(all 64 block products) as ONE grouped persistent tcgen05 launch.
+Headline workload (cross-product blocked matmul): C = A.B with A 32768x4096
+and B 4096x32768 split into 4096x4096 blocks (8x1 and 1x8 grids), entries
+U(-1,1), BF16 inputs, FP32 accumulation and FP32 output: 64 independent
+matrix_mult block ops, 2*32768^2*4096 = 8.796 TFLOP per step. The command
+list is compiled by bbx_dag_build into one grouped persistent tcgen05 launch
+in a captured CUDA graph; a step is one bbx_dag_launch replay.
 
 Reported (one JSON line on rank 0):
-  value       TFLOP/s of the grouped tensor-core path, inputs resident in HBM
-  e2e         the same through the C ABI with pinned HOST blocks: H2D of the
-              16 input blocks + the launch + D2H of the 64 output blocks
-  plain_fp32  the plain FP32 per-op path (one SIMT launch per block op)
-  roofline    dominant kernel vs the measured bf16 tensor peak
+  value       TFLOP/s of the graph replay, inputs resident in HBM
+  e2e         the same through the public API with pinned HOST blocks:
+              bbx_dag_write of the 16 input blocks, bbx_dag_launch,
+              bbx_dag_fetch of the 64 output blocks, every step
+  plain_fp32  the plain FP32 per-op path (bbx_rt_run: one SIMT launch per command)
+  roofline    the grouped tcgen05 kernel vs the measured bf16 tensor peak
   cpu_baseline  the CPU restatement of the reference's SGEMM on host cores
+  configs     the blocked matmul (bmm), FFN step (ffnn) and 2000-op random
+              DAG (dag) through the runtime, each vs its plain FP32 path
 `--impl reference` times the reference's CPU block matmul (the oracle port) instead.
 """
 import argparse
@@ -29,11 +33,17 @@ sys.path.insert(0, ROOT)
 GRID = 8            # 8 row blocks of A, 8 column blocks of B
 BS = 4096           # block edge
 FLOP_PER_STEP = 2.0 * (GRID * BS) ** 2 * BS
+# A and B read once (bf16) + C written once (f32)
+ALG_BYTES_PER_STEP = 2 * GRID * BS * BS * 2 + GRID * GRID * BS * BS * 4
+CPMM_SEED = 1000    # Philox seeds: A row block i = CPMM_SEED + i, B column block j = CPMM_SEED + 1000 + j
+CPMM_NAME = ("cpmm 32768x4096 . 4096x32768 in 4096^2 blocks (64 matrix_mult ops), bf16 in, f32 accumulate/out, "
+             "one grouped launch per step")
+REF_BUDGET_S = 150.0  # the reference arm's whole run (warm-up + timed steps)
 # DRAM bytes (read + write) of one full grouped launch per tile: ncu's
-# dram__bytes_read.sum + dram__bytes_write.sum on the 2x2-block capture (4 problems:
-# 548 MB with the 1-SM 128x256 tile, 627 MB with the 2-SM 256x256 pair) scaled by the
-# 64/4 problems of the full launch (the tc_gemm ncu summaries kept under profiles/).
+# dram__bytes_read.sum + dram__bytes_write.sum of one launch of the 4x4-block
+# case (16 problems) scaled by the 64/16 problems of the full launch.
 TRAFFIC_BYTES_PER_LAUNCH = {256: 8.77e9, 512: 10.03e9}
+TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum, 2x2-block capture scaled x16"
 
 
 def parse():
@@ -43,7 +53,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--tile-n", type=int, default=0,
-                   help="tensor-core tile (128, 256, 512); 0 = automatic (cpmm) / autotuned (DAG workloads)")
+                   help="tensor-core tile (128, 256, 512); 0 = the autotuner")
     p.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparator leg")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-accuracy", action="store_true",
@@ -54,6 +64,12 @@ def parse():
                    help="cpmm: the headline line (cross-product blocked matmul); bmm / dag / learned: the "
                         "blocked matmul, random 2000-op DAG and learned-scheduling configurations; spill: the "
                         "2000-op DAG on the per-op path under device budgets below its footprint")
+    p.add_argument("--configs", default="bmm,ffnn,dag",
+                   help="cpmm line: other configurations run through the runtime as sub-objects "
+                        "(comma list of bmm, ffnn, dag; none to skip)")
+    p.add_argument("--stream-kernel", type=int, default=0, choices=[0, 1],
+                   help="DAG streaming launches: 0 = bulk-staged kernel where aligned, 1 = register kernel "
+                        "(shares SMs with the wave's tensor-core launch)")
     p.add_argument("--n-ops", type=int, default=0, help="DAG size override (dag: 2000, learned: 5000)")
     p.add_argument("--train-dags", type=int, default=100, help="learned: DAGs recorded for the training set")
     p.add_argument("--tile-dags", type=int, default=16,
@@ -130,24 +146,6 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
-def cpu_sample_tflops(threads, a=None, b=None, want_result=False):
-    """One 4096x4096 output block with K=4096 (137 GFLOP) through the oracle's
-    blocked FP32 SGEMM, the CPU restatement of dense_matrix_mult (one block op).
-    a / b: the block inputs as FP32 arrays (seeded U(-1,1) when not given)."""
-    import numpy as np
-    import oracle
-    if a is None:
-        rng = np.random.default_rng(0)
-        a = rng.uniform(-1, 1, (BS, BS)).astype(np.float32)
-        b = rng.uniform(-1, 1, (BS, BS)).astype(np.float32)
-    t0 = time.perf_counter()
-    c = oracle.sgemm(a, b, threads=threads)
-    dt = time.perf_counter() - t0
-    if want_result:
-        return 2.0 * BS ** 3 / dt / 1e12, dt, c
-    return 2.0 * BS ** 3 / dt / 1e12, dt
-
-
 def cpu_step_tflops(a_blocks, b_blocks, threads, budget_s=30.0):
     """The step's block products C[i][j] = A[i] . B[j] through the oracle's
     FP32 SGEMM on host cores, in row-major block order, stopping once
@@ -192,32 +190,6 @@ def dist_setup(args):
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return world, rank, local
-
-
-def run_reference(args):
-    world, rank, _ = dist_setup(args)
-    if rank != 0:
-        return
-    threads = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        pass  # the CPU path has no warm-up state beyond the first call
-    vals, ts = [], []
-    for _ in range(args.steps):
-        v, dt = cpu_sample_tflops(threads)
-        vals.append(v)
-        ts.append(dt)
-    v = sum(vals) / len(vals)
-    line = {"impl": "reference", "metric": "block-op DAG TFLOP/s (cross-product blocked matmul)",
-            "value": round(v, 5), "unit": "TFLOP/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(1000 * FLOP_PER_STEP / (v * 1e12), 1),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic U(-1,1), seeded",
-            "config": {"workload": "cpmm 32768x4096 . 4096x32768 in 4096^2 blocks (64 matrix_mult ops)",
-                       "sample": "1 of 64 block products per step (4096^3), extrapolated per step"},
-            "cpu_baseline": {"value": round(v, 5), "unit": "TFLOP/s", "cores": threads, "kind": "port",
-                             "sample": "one 4096^3 FP32 block matmul per step (oracle blocked SGEMM)"},
-            "e2e": {"value": round(v, 5), "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
 
 
 def _time_on(stream_ptr, fn, reps):
@@ -405,6 +377,108 @@ def group_rooflines(prof, hbm_gbs, bf16_tflops):
     return out
 
 
+DAG_NAMES = {
+    "bmm": "blocked matmul 4096^2 in 1024^2 blocks (64 matrix_mult + 16 4-input reduces)",
+    "ffnn": "3-layer FFN step (fwd + bwd), X 16384x8192, W1 8192^2, W2 8192x4096, W3 4096x1024, 2048^2 blocks, "
+            "relu / relu / softmax-CE; first activation split bf16 hi + lo (its extra Z2 products not counted "
+            "as FLOPs)",
+    "dag": "random DAG, %d ops, depth 8 (60%% matmul 128..2048, 15%% add, 15%% reduce 2-16, 10%% contraction "
+           "ijk,kl->ijl 32..256)"}
+
+
+def build_workload(workload, dtype, seed, n_ops=0, stream_kernel=0, **kw):
+    """A runtime holding one configuration's input blocks and command list."""
+    import torch
+    from bbts_b200 import runtime, workloads
+    rt = runtime.Runtime()
+    rt.set_dag_stream_kernel(stream_kernel)
+    if workload == "bmm":
+        info = workloads.bmm(rt, n=4096, split=4, dtype=dtype, seed=seed, host=False)
+    elif workload == "ffnn":
+        info = workloads.ffnn(rt, seed=seed, dtype=dtype, **kw)
+    else:
+        n_ops = n_ops or (5000 if workload == "learned" else 2000)
+        hi = 4096 if workload == "learned" else 2048
+        info = workloads.random_dag(rt, n_ops=n_ops, depth=8, seed=seed, dtype=dtype, hi=hi, **kw)
+    torch.cuda.synchronize()
+    return rt, info
+
+
+def dag_config(workload, args, hbm, bf16_peak, per_group=True):
+    """One DAG configuration (bmm = config 1, ffnn = config 3, dag = config 4):
+    the bf16 command list through the grouped graph path (autotuned tiles),
+    the same list on FP32 blocks through the plain per-op path (one launch per
+    command, reservation-station LIFO, one stream) and through the grouped
+    graph, each with its max relative error vs an FP64 re-evaluation.
+    Returns the summary dict."""
+    import numpy as np
+    from bbts_b200 import runtime
+    result = {}
+    tile = args.tile_n or runtime.AUTOTUNE
+    check = ffnn_accuracy if workload == "ffnn" else dag_accuracy
+    # the FFN's first activation is split hi + lo (matrix_relu_split): with it
+    # rounded to bf16, ReLU-mask flips put ~3 % of error into dW1 / dW2
+    sk = getattr(args, "stream_kernel", 0)
+    rt, info = build_workload(workload, "bf16", 7, args.n_ops, sk,
+                              **({"split_a1": True} if workload == "ffnn" else {}))
+    dag = rt.build_dag(runtime.HEURISTIC, tile_n=tile)
+    st = dag.stats()
+    for _ in range(args.warmup):
+        dag.launch()
+    ms = _time_on(rt.stream.value, dag.launch, args.steps)
+    flops = info["flops"]
+    groups = group_rooflines(dag.profile(), hbm, bf16_peak)
+    if not per_group:
+        groups.pop("per_group")
+    result["grouped_bf16"] = {"ms": round(ms, 3), "tflops": round(flops / ms / 1e9, 2), "dag": st,
+                              "groups": groups, "accuracy": check(rt, info, dag)}
+    dag.close()
+    rt.close()
+    if workload == "ffnn":
+        # the same step with the first activation rounded to bf16 (one Z2 product per block)
+        rt, info_r = build_workload(workload, "bf16", 7, 0, sk)
+        dag = rt.build_dag(runtime.HEURISTIC, tile_n=tile)
+        for _ in range(args.warmup):
+            dag.launch()
+        rms = _time_on(rt.stream.value, dag.launch, args.steps)
+        result["grouped_bf16_rounded_a1"] = {"ms": round(rms, 3), "tflops": round(flops / rms / 1e9, 2),
+                                             "accuracy": check(rt, info_r, dag)}
+        dag.close()
+        rt.close()
+    # plain FP32 per-op path: same DAG in f32 blocks on a fresh runtime,
+    # reservation-station LIFO, one launch per op; median of 3 runs after a warm-up
+    rt, info32 = build_workload(workload, "f32", 7, args.n_ops)
+    rt.run()
+    pms = float(np.median([_time_on(rt.stream.value, rt.run, 1) for _ in range(3)]))
+    result["plain_fp32_per_op"] = {"ms": round(pms, 3), "tflops": round(info32["flops"] / pms / 1e9, 3),
+                                   "accuracy": check(rt, info32)}
+    rt.close()
+    # the FP32 variant through the grouped graph path
+    rt, info32 = build_workload(workload, "f32", 7, args.n_ops, sk)
+    dag = rt.build_dag(runtime.HEURISTIC, tile_n=tile)
+    for _ in range(args.warmup):
+        dag.launch()
+    gms = _time_on(rt.stream.value, dag.launch, max(1, min(5, args.steps)))
+    result["grouped_fp32"] = {"ms": round(gms, 3), "tflops": round(info32["flops"] / gms / 1e9, 3),
+                              "accuracy": check(rt, info32, dag)}
+    dag.close()
+    rt.close()
+    name = DAG_NAMES[workload] % (args.n_ops or 2000) if workload == "dag" else DAG_NAMES[workload]
+    return {"workload": name, "flops_per_step": flops, "stream_kernel": "register" if sk else "bulk where aligned",
+            "value": round(flops / ms / 1e9, 2), "unit": "TFLOP/s",
+            "ms_per_step": round(ms, 3),
+            "makespan_ms": {"grouped_bf16_graph": round(ms, 3), "grouped_fp32_graph": round(gms, 3),
+                            "plain_fp32_per_op": round(pms, 3)},
+            "speedup_vs_plain_fp32": round(pms / ms, 2),
+            "max_rel_err_vs_fp64": {k: result[k]["accuracy"]["max_rel_err_vs_fp64"]
+                                    for k in ("grouped_bf16", "grouped_bf16_rounded_a1", "grouped_fp32",
+                                              "plain_fp32_per_op") if k in result},
+            "tensor_frac_of_bf16_burst": groups.get("tc_gemm", {}).get("frac_of_bf16_burst"),
+            "stream_frac_of_hbm": groups.get("stream", {}).get("frac_of_hbm"),
+            "detail": result,
+            "gpu_launches_per_step": st["tc_launches"] + st["stream_launches"] + st["other_launches"]}
+
+
 def run_dag_workload(args):
     """Whole-DAG configurations through the runtime: grouped graph path vs the
     plain FP32 per-op path, and learned vs heuristic scheduling."""
@@ -418,84 +492,17 @@ def run_dag_workload(args):
             "scaling": "weak", "vs_baseline": None, "data": "synthetic N(0,1), seeded Philox on the device"}
 
     def build(dtype, seed, **kw):
-        rt = runtime.Runtime()
-        if args.workload == "bmm":
-            info = workloads.bmm(rt, n=4096, split=4, dtype=dtype, seed=seed, host=False)
-        elif args.workload == "ffnn":
-            info = workloads.ffnn(rt, seed=seed, dtype=dtype, **kw)
-        else:
-            n_ops = args.n_ops or (5000 if args.workload == "learned" else 2000)
-            hi = 4096 if args.workload == "learned" else 2048
-            info = workloads.random_dag(rt, n_ops=n_ops, depth=8, seed=seed, dtype=dtype, hi=hi, **kw)
-        torch.cuda.synchronize()
-        return rt, info
+        return build_workload(args.workload, dtype, seed, args.n_ops, args.stream_kernel, **kw)
 
     with ClockSampler(0) as clk:
-        result = {}
         if args.workload in ("bmm", "dag", "ffnn"):
-            # fast path: bf16 blocks, grouped + graph, autotuned tiles, heuristic and learned-free policy
-            # the FFN's first activation is split hi + lo (matrix_relu_split): with it
-            # rounded to bf16, ReLU-mask flips put ~3 % of error into dW1 / dW2
-            rt, info = build("bf16", 7, **({"split_a1": True} if args.workload == "ffnn" else {}))
-            dag = rt.build_dag(runtime.HEURISTIC, tile_n=args.tile_n or -1)
-            st = dag.stats()
-            for _ in range(args.warmup):
-                dag.launch()
-            ms = _time_on(rt.stream.value, dag.launch, args.steps)
-            flops = info["flops"]
-            check = ffnn_accuracy if args.workload == "ffnn" else dag_accuracy
-            result["grouped_bf16"] = {"ms": round(ms, 3), "tflops": round(flops / ms / 1e9, 2), "dag": st,
-                                      "groups": group_rooflines(dag.profile(), hbm, bf16_peak),
-                                      "accuracy": check(rt, info, dag)}
-            dag.close()
-            rt.close()
-            if args.workload == "ffnn":
-                # the same step with the first activation rounded to bf16 (one Z2 product per block)
-                rt, info_r = build("bf16", 7)
-                dag = rt.build_dag(runtime.HEURISTIC, tile_n=args.tile_n or -1)
-                for _ in range(args.warmup):
-                    dag.launch()
-                rms = _time_on(rt.stream.value, dag.launch, args.steps)
-                result["grouped_bf16_rounded_a1"] = {"ms": round(rms, 3), "tflops": round(flops / rms / 1e9, 2),
-                                                     "accuracy": check(rt, info_r, dag)}
-                dag.close()
-                rt.close()
-            # plain FP32 per-op path: same DAG in f32 blocks on a fresh runtime,
-            # reservation-station LIFO, one launch per op; median of 3 runs after a warm-up
-            rt, info32 = build("f32", 7)
-            rt.run()
-            pms = float(np.median([_time_on(rt.stream.value, rt.run, 1) for _ in range(3)]))
-            result["plain_fp32_per_op"] = {"ms": round(pms, 3), "tflops": round(info32["flops"] / pms / 1e9, 3),
-                                           "accuracy": check(rt, info32)}
-            rt.close()
-            # the FP32 variant through the grouped graph path
-            rt, info32 = build("f32", 7)
-            dag = rt.build_dag(runtime.HEURISTIC, tile_n=args.tile_n or -1)
-            for _ in range(args.warmup):
-                dag.launch()
-            gms = _time_on(rt.stream.value, dag.launch, max(1, min(5, args.steps)))
-            result["grouped_fp32"] = {"ms": round(gms, 3), "tflops": round(info32["flops"] / gms / 1e9, 3),
-                                      "accuracy": check(rt, info32, dag)}
-            dag.close()
-            rt.close()
-            value = flops / ms / 1e9
-            name = {"bmm": "blocked matmul 4096^2 in 1024^2 blocks (64 matrix_mult + 16 4-input reduces)",
-                    "ffnn": "3-layer FFN step (fwd + bwd), X 16384x8192, W1 8192^2, W2 8192x4096, W3 4096x1024, "
-                            "2048^2 blocks, relu / relu / softmax-CE; first activation split bf16 hi + lo "
-                            "(its extra Z2 products not counted as FLOPs)",
-                    "dag": "random DAG, %d ops, depth 8 (60%% matmul 128..2048, 15%% add, 15%% reduce 2-16, "
-                           "10%% contraction ijk,kl->ijl 32..256)" % (args.n_ops or 2000)}[args.workload]
-            line.update({"metric": "block-op DAG TFLOP/s and makespan vs plain FP32 path", "value": round(value, 2),
-                         "unit": "TFLOP/s", "ms_per_step": round(ms, 3), "dtype": "bf16",
-                         "config": {"workload": name, "flops_per_step": flops},
-                         "makespan_ms": {"grouped_bf16_graph": round(ms, 3), "grouped_fp32_graph": round(gms, 3),
-                                         "plain_fp32_per_op": round(pms, 3)},
-                         "speedup_vs_plain_fp32": round(pms / ms, 2),
-                         "max_rel_err_vs_fp64": {k: result[k]["accuracy"]["max_rel_err_vs_fp64"]
-                                                 for k in ("grouped_bf16", "grouped_bf16_rounded_a1", "grouped_fp32",
-                                                           "plain_fp32_per_op") if k in result},
-                         "detail": result,
-                         "gpu_launches": st["tc_launches"] + st["stream_launches"] + st["other_launches"]})
+            sub = dag_config(args.workload, args, hbm, bf16_peak)
+            line.update({"metric": "block-op DAG TFLOP/s and makespan vs plain FP32 path", "value": sub["value"],
+                         "unit": "TFLOP/s", "ms_per_step": sub["ms_per_step"], "dtype": "bf16",
+                         "config": {"workload": sub["workload"], "flops_per_step": sub["flops_per_step"]},
+                         "makespan_ms": sub["makespan_ms"], "speedup_vs_plain_fp32": sub["speedup_vs_plain_fp32"],
+                         "max_rel_err_vs_fp64": sub["max_rel_err_vs_fp64"], "detail": sub["detail"],
+                         "gpu_launches": sub["gpu_launches_per_step"] * args.steps})
         elif args.workload == "spill":
             # per-op path (4 worker streams) with the whole DAG resident, then
             # under device budgets of a half and a quarter of its peak footprint
@@ -691,227 +698,345 @@ def run_dag_workload(args):
     print(json.dumps(line), flush=True)
 
 
-def main():
-    global GRID, FLOP_PER_STEP
-    args = parse()
-    GRID = args.grid
-    FLOP_PER_STEP = 2.0 * (GRID * BS) ** 2 * BS
-    if args.impl == "reference":
-        return run_reference(args)
-    if args.workload != "cpmm":
-        return run_dag_workload(args)
+def cpmm_block_inputs(seed_base):
+    """The cpmm input blocks on the host exactly as the device fill makes them:
+    U(-1,1) from Philox4x32-10 with the seeds of workloads.cpmm_seeds (A row
+    block i: seed + i, B column block j: seed + 1000 + j), rounded to bf16 and
+    widened to FP32 -- the same values the GPU arm multiplies."""
+    import numpy as np
+    import torch
+    import oracle
+    seeds_a = [seed_base + i for i in range(GRID)]
+    seeds_b = [seed_base + 1000 + j for j in range(GRID)]
+    widen = lambda x: torch.from_numpy(x).to(torch.bfloat16).float().numpy().reshape(BS, BS)
+    a = [widen(oracle.uniform(sd, BS * BS, -1.0, 1.0)) for sd in seeds_a]
+    b = [widen(oracle.uniform(sd, BS * BS, -1.0, 1.0)) for sd in seeds_b]
+    return a, b
+
+
+def run_reference(args):
+    """The reference's CPU block matmul (the oracle's restatement of
+    dense_matrix_mult_t::mult, an FP32 SGEMM on every host core) over the
+    cpmm step's block products, on the same inputs as the GPU arm. Each step
+    is a bounded sample of the step's 64 products (consecutive in row-major
+    block order, continuing where the last step stopped), sized from a timed
+    warm-up product so the whole run stays near REF_BUDGET_S; ms_per_step is
+    the measured duration of a sampled step and value its FLOPs over that."""
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return
+    import numpy as np
+    import oracle
+    threads = os.cpu_count() or 1
+    a, b = cpmm_block_inputs(CPMM_SEED)
+    flop1 = 2.0 * BS ** 3
+    t0 = time.perf_counter()
+    oracle.sgemm(a[0], b[0], threads=threads)  # warm-up product: page-in, thread start-up
+    t1 = time.perf_counter() - t0
+    per_step = int(max(1, min(GRID * GRID, REF_BUDGET_S / (max(1, args.steps + args.warmup) * t1))))
+    order = [(i, j) for i in range(GRID) for j in range(GRID)]
+    pos = 0
+
+    def step():
+        nonlocal pos
+        t = time.perf_counter()
+        for _ in range(per_step):
+            i, j = order[pos % len(order)]
+            oracle.sgemm(a[i], b[j], threads=threads)
+            pos += 1
+        return time.perf_counter() - t
+
+    for _ in range(args.warmup):
+        step()
+    ts = [step() for _ in range(args.steps)]
+    sec = float(np.mean(ts))
+    v = per_step * flop1 / sec / 1e12
+    sample = ("%d of the step's %d 4096^3 FP32 block products per step (row-major block order, continuing "
+              "across steps), oracle SGEMM on %d threads, same bf16-valued inputs as the GPU arm"
+              % (per_step, GRID * GRID, threads))
+    line = {"impl": "reference", "metric": "block-op DAG TFLOP/s (cross-product blocked matmul)",
+            "value": round(v, 5), "unit": "TFLOP/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1000 * sec, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic U(-1,1), seeded Philox (the GPU arm's generator, restated on the host)",
+            "config": {"workload": CPMM_NAME, "sample": sample, "flops_per_sampled_step": per_step * flop1,
+                       "warmup_product_s": round(t1, 3)},
+            "cpu_baseline": {"value": round(v, 5), "unit": "TFLOP/s", "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": round(v, 5), "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_cpmm(args):
+    """The headline: config 2 as a command list (64 matrix_mult APPLYs over
+    device-resident bf16 blocks) compiled by bbx_dag_build into one grouped
+    tcgen05 launch inside a captured CUDA graph, replayed by bbx_dag_launch."""
+    import numpy as np
     import torch
     import torch.distributed as dist
     import bbts_b200
-    from bbts_b200 import ops
+    from bbts_b200 import ops, runtime, workloads
 
     world, rank, local = dist_setup(args)
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     dev = torch.device("cuda", local)
-    stream = torch.cuda.current_stream()
-
-    # ---------------- inputs: 8 A blocks + 8 B blocks (BF16), 64 C blocks (FP32)
-    A = [torch.empty(BS, BS, dtype=torch.bfloat16, device=dev) for _ in range(GRID)]
-    B = [torch.empty(BS, BS, dtype=torch.bfloat16, device=dev) for _ in range(GRID)]
-    for i in range(GRID):
-        ops.fill_philox(A[i], seed=1000 + i + 100 * rank, dist=0, a=-1.0, b=1.0)
-        ops.fill_philox(B[i], seed=2000 + i + 100 * rank, dist=0, a=-1.0, b=1.0)
-    Cblk = [torch.empty(BS, BS, dtype=torch.float32, device=dev) for _ in range(GRID * GRID)]
-    probs = [ops.tc_problem(A[i], B[j], Cblk[i * GRID + j]) for i in range(GRID) for j in range(GRID)]
-    plan = ops.TcPlan(probs, tile_n=args.tile_n)
+    hbm, bf16_peak, bf16_sust, src = load_peaks()
 
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
 
-    # ---------------- device-resident timing of the grouped tensor-core path
+    # ---------------- the command list and its compiled DAG
+    rt = runtime.Runtime()
+    info = workloads.cpmm(rt, rows=GRID, cols=GRID, bs=BS, dtype="bf16", seed=CPMM_SEED + 100 * rank)
+    torch.cuda.synchronize()
+    tb = time.perf_counter()
+    dag = rt.build_dag(runtime.HEURISTIC, tile_n=args.tile_n or runtime.AUTOTUNE)
+    build_s = time.perf_counter() - tb
+    st = dag.stats()
+    tiles = [t for t in dag.group_tiles() if t]
+    launches_per_step = st["tc_launches"] + st["stream_launches"] + st["other_launches"]
+    stream = torch.cuda.ExternalStream(rt.stream.value)
+
+    # ---------------- device-resident timing: one graph replay per step
     for _ in range(args.warmup):
-        plan.launch()
+        dag.launch()
     barrier()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     with ClockSampler(local) as clk:
         ev[0].record(stream)
-        for s in range(args.steps):
-            plan.launch()
-            ev[s + 1].record(stream)
+        for s_ in range(args.steps):
+            dag.launch()
+            ev[s_ + 1].record(stream)
         barrier()
-    step_ms = [ev[s].elapsed_time(ev[s + 1]) for s in range(args.steps)]
-    total_ms = ev[0].elapsed_time(ev[-1])
+    step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
     rc = bbts_b200.lib.bbx_check_device_status(None, None)
     if rc != 0:
         raise RuntimeError(bbts_b200.last_error())
-    total_ms = max_over_ranks(total_ms, world, dev)
-    ms = total_ms / args.steps
+    ms = max_over_ranks(ev[0].elapsed_time(ev[-1]) / args.steps, world, dev)
     value = job_tflops(FLOP_PER_STEP, world, ms)
 
-    # ---------------- roofline of the dominant kernel (the grouped tcgen05 launch)
-    hbm, bf16_peak, bf16_sust, src = load_peaks()
-    kern_ms = sum(step_ms) / len(step_ms)
+    # ---------------- roofline of the dominant kernel: the graph holds one grouped
+    # tcgen05 launch, so a step's event interval is that kernel's duration
+    kern_ms = float(np.mean(step_ms))
     achieved = FLOP_PER_STEP / (kern_ms * 1e-3) / 1e12
-    # The timed region is args.steps back-to-back launches (hundreds of ms of
-    # dense tensor work under the 1 kW cap), so the denominator is the measured
-    # SUSTAINED bf16 peak; the burst fraction is reported beside it.
-    peak = bf16_sust or bf16_peak
-    roofline = {"bound": "tensor", "achieved": round(achieved, 1), "peak": peak,
-                "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
-                "traffic": TRAFFIC_BYTES_PER_LAUNCH.get(plan.tile_n) if GRID == 8 else None,
-                "peak_source": src + " bf16 sustained (of measured)", "frac_of_burst": round(achieved / bf16_peak, 4),
-                "kernel": plan.kernel_name, "launches_timed": args.steps}
+    tile = tiles[0] if tiles else 0
+    kname = ("tc_gemm2_kernel<0,1> (2-SM 256x256 pair, cta_group::2)" if tile == 512
+             else "tc_gemm_kernel<%d,0,1,0>" % tile)
+    traffic = TRAFFIC_BYTES_PER_LAUNCH.get(tile) if GRID == 8 else None
+    roofline = {"bound": "tensor", "achieved": round(achieved, 1), "peak": bf16_peak, "unit": "TFLOP/s",
+                "frac": round(achieved / bf16_peak, 4), "traffic": traffic,
+                "peak_source": "%s bf16 burst (of %s): the timed region is %d graph replays, %.0f ms at the "
+                               "clocks below" % (src, src, args.steps, kern_ms * args.steps),
+                "frac_of_sustained": round(achieved / (bf16_sust or bf16_peak), 4),
+                "traffic_source": TRAFFIC_SOURCE if traffic else None,
+                "algorithmic_bytes": ALG_BYTES_PER_STEP,
+                "kernel": kname, "tile": tile, "launches_timed": args.steps * launches_per_step}
 
-    # ---------------- accuracy: every output block against FP64 on the same (bf16) inputs
-    def block_errors(C):
+    # ---------------- accuracy: every output block against FP64 of the same (bf16) inputs
+    accuracy = {"definition": "per output block max|x - x64| / max|x64|, x64 = FP64 product of the same stored "
+                              "inputs (FP64 only in this check)"}
+    if not args.no_accuracy:
         errs = []
         for i in range(GRID):
-            a64 = A[i].double()
+            a64 = dev_block_f64(rt, info["A"][i])
             for j in range(GRID):
-                r = a64 @ B[j].double()
-                errs.append(float((C[i * GRID + j].double() - r).abs().max() / r.abs().max()))
-        return errs
+                r = a64 @ dev_block_f64(rt, info["B"][j])
+                errs.append(rel_err_f64(dev_block_f64(rt, info["C"][(i, j)], dag), r)[0])
+                del r
+            del a64
+        accuracy.update({"bf16_max": max(errs), "bf16_per_block": [float("%.3g" % e) for e in errs]})
+    c00 = dev_block_f64(rt, info["C"][(0, 0)], dag).float().cpu()
 
-    acc_bf16 = block_errors(Cblk) if not args.no_accuracy else [float("nan")]
-    accuracy = {"definition": "per output block max|x - x64| / max|x64|, x64 = FP64 product of the same inputs "
-                              "(FP64 only in this check)",
-                "bf16_max": max(acc_bf16), "bf16_per_block": [float("%.3g" % e) for e in acc_bf16]}
-
-    # ---------------- FP8-E4M3 variant: one absmax scale per 4096^2 block, same grouped launch shape
-    fp8 = None
-    if GRID == 8:
-        qA = [torch.empty(BS, BS, dtype=torch.float8_e4m3fn, device=dev) for _ in range(GRID)]
-        qB = [torch.empty(BS, BS, dtype=torch.float8_e4m3fn, device=dev) for _ in range(GRID)]
-        sA = torch.empty(GRID, device=dev)
-        sB = torch.empty(GRID, device=dev)
-
-        def quantize_all():
-            for i in range(GRID):
-                ops.quantize_e4m3(A[i], qA[i], sA[i:i + 1])
-                ops.quantize_e4m3(B[i], qB[i], sB[i:i + 1], transpose=True)  # K-major B for the fp8 MMA
-
-        quantize_all()
-        torch.cuda.synchronize()
-        hsA, hsB = sA.cpu().tolist(), sB.cpu().tolist()
-        plan8 = ops.TcPlan([ops.tc_problem(qA[i], qB[j], Cblk[i * GRID + j], trans_b=True, alpha=hsA[i] * hsB[j])
-                            for i in range(GRID) for j in range(GRID)], in_dtype=ops.E4M3)
-        for _ in range(args.warmup):
-            plan8.launch()
-        barrier()
-        q0, q1, q2 = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-        q0.record(stream)
-        for _ in range(args.steps):
-            plan8.launch()
-        q1.record(stream)
-        for _ in range(args.steps):
-            quantize_all()
-        q2.record(stream)
-        barrier()
-        ms8 = q0.elapsed_time(q1) / args.steps
-        msq = q1.elapsed_time(q2) / args.steps
-        acc8 = block_errors(Cblk) if not args.no_accuracy else [float("nan")]
-        fp8 = {"value": round(FLOP_PER_STEP / (ms8 * 1e-3) / 1e12, 2), "unit": "TFLOP/s", "ms_per_step": round(ms8, 3),
-               "quantize_ms_per_step": round(msq, 3), "kernel": plan8.kernel_name,
-               "max_rel_err": max(acc8), "per_block": [float("%.3g" % e) for e in acc8],
-               "note": "e4m3 keeps 3 mantissa bits: outside the 1e-2 budget, reported per block"}
-        plan8.close()
-        del qA, qB
-        plan.launch()  # the bf16 result back in C for the e2e / CPU comparisons
-
-    # ---------------- e2e through the C ABI with pinned host blocks
-    hA = [torch.empty(BS, BS, dtype=torch.bfloat16, pin_memory=True) for _ in range(GRID)]
-    hB = [torch.empty(BS, BS, dtype=torch.bfloat16, pin_memory=True) for _ in range(GRID)]
-    for i in range(GRID):
-        hA[i].copy_(A[i])
-        hB[i].copy_(B[i])
-    hC = [torch.empty(BS, BS, dtype=torch.float32, pin_memory=True) for _ in range(GRID * GRID)]
-    h2d = sum(x.numel() * x.element_size() for x in hA + hB)
-    d2h = sum(x.numel() * x.element_size() for x in hC)
+    # ---------------- e2e through the public API: pinned host blocks in, the DAG, host blocks out
+    in_tids = list(info["A"].values()) + list(info["B"].values())
+    out_tids = [info["C"][(i, j)] for i in range(GRID) for j in range(GRID)]
+    a_bytes = BS * BS * 2
+    c_bytes = BS * BS * 4
+    h_in = [torch.empty(BS * BS, dtype=torch.bfloat16, pin_memory=True) for _ in in_tids]
+    h_out = [torch.empty(BS * BS, dtype=torch.float32, pin_memory=True) for _ in out_tids]
+    for t, h in zip(in_tids, h_in):
+        dag.fetch(t, h.data_ptr(), a_bytes)  # the step's inputs, as a host caller would hold them
+    torch.cuda.synchronize()
 
     def e2e_step():
-        for i in range(GRID):
-            A[i].copy_(hA[i], non_blocking=True)
-            B[i].copy_(hB[i], non_blocking=True)
-        plan.launch()
-        for i in range(GRID * GRID):
-            hC[i].copy_(Cblk[i], non_blocking=True)
+        for t, h in zip(in_tids, h_in):
+            dag.write(t, h.data_ptr(), a_bytes)
+        dag.launch()
+        for t, h in zip(out_tids, h_out):
+            dag.fetch(t, h.data_ptr(), c_bytes)
 
-    e2e_steps = max(1, min(args.steps, 3))
     e2e_step()
     barrier()
+    e2e_steps = max(1, args.steps)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(e2e_steps):
         e2e_step()
     e1.record(stream)
     barrier()
-    e2e_ms = e0.elapsed_time(e1) / e2e_steps
-    e2e_ms = max_over_ranks(e2e_ms, world, dev)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, world, dev)
     e2e_val = job_tflops(FLOP_PER_STEP, world, e2e_ms)
+    e2e_ok = bool(torch.equal(h_out[0].view(BS, BS), c00))  # the host copy of C(0,0) is the DAG's result
+    h2d, d2h = a_bytes * len(in_tids), c_bytes * len(out_tids)
+    dag.close()
+    rt.close()
+    del h_in, h_out
 
-    c_block0 = Cblk[0].cpu()  # the bf16 path's block (0, 0), before the comparator reuses C
+    # ---------------- FP8-E4M3 variant: one absmax scale per 4096^2 block (library plan entry)
+    fp8 = None
+    if GRID == 8:
+        fp8 = fp8_leg(args, dev, barrier)
 
-    # ---------------- plain FP32 per-op path (the comparator): one SIMT launch per block op
+    # ---------------- plain FP32 per-op path: the same command list on FP32 blocks,
+    # reservation-station LIFO, one SIMT launch per command on one stream
     plain = None
     if not args.no_plain:
-        Af = [torch.empty(BS, BS, dtype=torch.float32, device=dev) for _ in range(GRID)]
-        Bf = [torch.empty(BS, BS, dtype=torch.float32, device=dev) for _ in range(GRID)]
-        for i in range(GRID):
-            ops.cast(A[i], Af[i])
-            ops.cast(B[i], Bf[i])
-
-        def plain_step():
-            for i in range(GRID):
-                for j in range(GRID):
-                    ops.matmul_f32(Af[i], Bf[j], Cblk[i * GRID + j])
-
-        plain_step()
-        barrier()
-        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        p0.record(stream)
-        plain_step()
-        p1.record(stream)
-        barrier()
-        pms = p0.elapsed_time(p1)
-        plain = {"value": round(world * FLOP_PER_STEP / (pms * 1e-3) / 1e12, 3), "unit": "TFLOP/s",
-                 "ms_per_step": round(pms, 2), "launches_per_step": GRID * GRID,
-                 "dtype": "f32", "speedup_of_value": round(value / (world * FLOP_PER_STEP / (pms * 1e-3) / 1e12), 2)}
-        del Af, Bf
+        rt = runtime.Runtime()
+        workloads.cpmm(rt, rows=GRID, cols=GRID, bs=BS, dtype="f32", seed=CPMM_SEED + 100 * rank)
+        torch.cuda.synchronize()
+        rt.run()
+        pms = max_over_ranks(_time_on(rt.stream.value, rt.run, 1), world, dev)
+        rt.close()
+        pv = job_tflops(FLOP_PER_STEP, world, pms)
+        plain = {"value": round(pv, 3), "unit": "TFLOP/s", "ms_per_step": round(pms, 2),
+                 "launches_per_step": GRID * GRID, "dtype": "f32", "path": "bbx_rt_run (per-op, LIFO, 1 stream)",
+                 "frac_of_fp32_simt_peak": round(pv / fp32_simt_peak_tflops(), 3),
+                 "speedup_of_value": round(value / pv, 2)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        # the step's 64 block products on the same bf16 inputs widened to FP32,
-        # within a 30 s budget; block (0, 0) doubles as the accuracy cross-check
-        a_host = [A[i].float().cpu().numpy() for i in range(GRID)]
-        b_host = [B[j].float().cpu().numpy() for j in range(GRID)]
+        # the step's 64 block products on the same bf16-valued inputs, within a 30 s
+        # budget; block (0, 0) doubles as the accuracy cross-check
+        a_host, b_host = cpmm_block_inputs(CPMM_SEED)
         v, done, dt, c0 = cpu_step_tflops(a_host, b_host, threads)
         del a_host, b_host
         r = torch.from_numpy(c0).double()
-        cpu_err = float((c_block0.double() - r).abs().max() / r.abs().max())
+        accuracy["vs_cpu_port_block0"] = float((c00.double() - r).abs().max() / r.abs().max())
         cpu = {"value": round(v, 5), "unit": "TFLOP/s", "cores": threads, "kind": "port",
                "sample": "%d of the step's %d 4096^3 FP32 block products (row-major block order, 30 s budget) "
                          "on the same inputs, oracle SGEMM, %.1f s" % (done, GRID * GRID, dt)}
-        accuracy["vs_cpu_port_block0"] = cpu_err
 
-    plan.close()
+    # ---------------- the other configurations, each through the runtime (sub-objects)
+    configs = {}
+    if world == 1 and GRID == 8:
+        for name in [c for c in args.configs.split(",") if c and c != "none"]:
+            configs[name] = dag_config(name, args, hbm, bf16_peak, per_group=False)
+            torch.cuda.empty_cache()
+
     if rank == 0:
         line = {"metric": "block-op DAG TFLOP/s (cross-product blocked matmul)", "value": round(value, 2),
                 "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "bf16",
                 "data": "synthetic U(-1,1) from a seeded Philox generator",
-                "config": {"workload": "cpmm 32768x4096 . 4096x32768 in 4096^2 blocks (64 matrix_mult ops), "
-                                       "bf16 in, f32 accumulate/out, one grouped launch per step",
+                "config": {"workload": CPMM_NAME,
+                           "path": "command list -> bbx_dag_build (autotuned tile) -> bbx_dag_launch graph replay",
                            "parallelism": "replicas" if world > 1 else "single-gpu",
-                           "l2": "inputs+outputs (4.5 GiB) larger than L2"},
+                           "l2": "inputs+outputs (4.5 GiB) larger than L2, no flush",
+                           "dag": st, "dag_build_s": round(build_s, 2)},
                 "e2e": {"value": round(e2e_val, 2), "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
-                        "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_ms, 2)},
+                        "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_ms, 2), "steps": e2e_steps,
+                        "path": "bbx_dag_write (16 pinned host blocks) + bbx_dag_launch + bbx_dag_fetch "
+                                "(64 pinned host blocks), one stream", "result_matches_device": e2e_ok},
                 "roofline": roofline, "plain_fp32": plain, "cpu_baseline": cpu,
-                "accuracy": accuracy, "fp8_e4m3": fp8,
-                "gpu_launches": args.steps, "clocks": clk.summary()}
+                "accuracy": accuracy, "fp8_e4m3": fp8, "configs": configs,
+                "gpu_launches": args.steps * launches_per_step, "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def fp8_leg(args, dev, barrier):
+    """cpmm with FP8-E4M3 blocks: per-block absmax quantisation of the same
+    bf16 inputs (A row-major, B transposed to K-major for the e4m3 MMA), then
+    one grouped e4m3 tcgen05 launch with the scale product as alpha."""
+    import torch
+    from bbts_b200 import ops
+    stream = torch.cuda.current_stream()
+    A = [torch.empty(BS, BS, dtype=torch.bfloat16, device=dev) for _ in range(GRID)]
+    B = [torch.empty(BS, BS, dtype=torch.bfloat16, device=dev) for _ in range(GRID)]
+    for i in range(GRID):
+        ops.fill_philox(A[i], seed=CPMM_SEED + i, dist=0, a=-1.0, b=1.0)
+        ops.fill_philox(B[i], seed=CPMM_SEED + 1000 + i, dist=0, a=-1.0, b=1.0)
+    C = [torch.empty(BS, BS, dtype=torch.float32, device=dev) for _ in range(GRID * GRID)]
+    qA = [torch.empty(BS, BS, dtype=torch.float8_e4m3fn, device=dev) for _ in range(GRID)]
+    qB = [torch.empty(BS, BS, dtype=torch.float8_e4m3fn, device=dev) for _ in range(GRID)]
+    sA = torch.empty(GRID, device=dev)
+    sB = torch.empty(GRID, device=dev)
+
+    def quantize_all():
+        for i in range(GRID):
+            ops.quantize_e4m3(A[i], qA[i], sA[i:i + 1])
+            ops.quantize_e4m3(B[i], qB[i], sB[i:i + 1], transpose=True)  # K-major B for the fp8 MMA
+
+    quantize_all()
+    torch.cuda.synchronize()
+    hsA, hsB = sA.cpu().tolist(), sB.cpu().tolist()
+    plan8 = ops.TcPlan([ops.tc_problem(qA[i], qB[j], C[i * GRID + j], trans_b=True, alpha=hsA[i] * hsB[j])
+                        for i in range(GRID) for j in range(GRID)], in_dtype=ops.E4M3)
+    for _ in range(args.warmup):
+        plan8.launch()
+        quantize_all()
+    barrier()
+    q0, q1, q2 = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    q0.record(stream)
+    for _ in range(args.steps):
+        plan8.launch()
+    q1.record(stream)
+    for _ in range(args.steps):
+        quantize_all()
+    q2.record(stream)
+    barrier()
+    ms8 = q0.elapsed_time(q1) / args.steps
+    msq = q1.elapsed_time(q2) / args.steps
+    errs = []
+    if not args.no_accuracy:
+        for i in range(GRID):
+            a64 = A[i].double()
+            for j in range(GRID):
+                r = a64 @ B[j].double()
+                errs.append(float((C[i * GRID + j].double() - r).abs().max() / r.abs().max()))
+    plan8.close()
+    qbytes = GRID * 2 * (BS * BS * 2 + BS * BS)  # bf16 read + e4m3 written per block (absmax fused)
+    return {"value": round(FLOP_PER_STEP / (ms8 * 1e-3) / 1e12, 2), "unit": "TFLOP/s", "ms_per_step": round(ms8, 3),
+            "quantize_ms_per_step": round(msq, 3),
+            "quantize_gbs": round(qbytes / (msq * 1e-3) / 1e9, 1),
+            "with_quantize_ms_per_step": round(ms8 + msq, 3),
+            "kernel": plan8.kernel_name, "path": "bbx_quantize_e4m3 x16 + bbx_tc_plan (library entry points)",
+            "max_rel_err": max(errs) if errs else None, "per_block": [float("%.3g" % e) for e in errs],
+            "note": "e4m3 keeps 3 mantissa bits: outside the 1e-2 budget, reported per block"}
+
+
+def fp32_simt_peak_tflops():
+    """FP32 SIMT peak of the device: SMs x 128 FP32 lanes x 2 FLOP (FMA) x max SM clock."""
+    import torch
+    try:
+        import pynvml as nv
+        nv.nvmlInit()
+        mhz = nv.nvmlDeviceGetMaxClockInfo(nv.nvmlDeviceGetHandleByIndex(torch.cuda.current_device()),
+                                           nv.NVML_CLOCK_SM)
+    except Exception:
+        mhz = 1965
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    return sms * 128 * 2 * mhz * 1e6 / 1e12
+
+
+def main():
+    global GRID, FLOP_PER_STEP, ALG_BYTES_PER_STEP
+    args = parse()
+    GRID = args.grid
+    FLOP_PER_STEP = 2.0 * (GRID * BS) ** 2 * BS
+    ALG_BYTES_PER_STEP = 2 * GRID * BS * BS * 2 + GRID * GRID * BS * BS * 4
+    if args.impl == "reference":
+        return run_reference(args)
+    if args.workload != "cpmm":
+        return run_dag_workload(args)
+    return run_cpmm(args)
 
 
 if __name__ == "__main__":

@@ -177,9 +177,12 @@ int bbx_quantize_e4m3(int src_dtype, const void* in, void* out, int rows, int co
  * device pointers, scales_out a device array of `count` floats) and calls no
  * cudaMalloc / cudaFree: its absmax scratch is a fixed 4 KiB __device__ array
  * of the library, so count is at most 1024 per call (larger counts fail with
- * BBX_ERR_INVALID). The first call on a device looks the array up
- * (cudaGetSymbolAddress), so make it before any stream capture. All calls on
- * a device share that array: calls that overlap on the GPU race. */
+ * BBX_ERR_INVALID; count 0 is a no-op). The first call on a device looks the
+ * array up (cudaGetSymbolAddress) and caches its address for the process, so
+ * make it before any stream capture, and do not call the function after
+ * cudaDeviceReset on that device (the cached address belongs to the old
+ * context). All calls on a device share that array: calls that overlap on the
+ * GPU race. */
 int bbx_quantize_e4m3_batched_noalloc(int src_dtype, const void* const* in, void* const* out, int count,
                                       int rows, int cols, int transpose, float* scales_out, void* stream);
 
@@ -223,6 +226,14 @@ typedef struct bbx_stream_plan bbx_stream_plan_t;
 int bbx_stream_plan_create(const bbx_stream_op_t* ops, int count, bbx_stream_plan_t** out);
 int bbx_stream_plan_launch(bbx_stream_plan_t* plan, void* stream);
 int bbx_stream_plan_destroy(bbx_stream_plan_t* plan);
+/* Kernel choice of a plan: AUTO runs the bulk-staged kernel when every
+ * pointer is 16-byte aligned (fastest alone, but its 196 KB of shared memory
+ * leaves no room on an SM for a tensor-core CTA), REGISTER always runs the
+ * register kernel (no shared memory: it shares SMs with a concurrent
+ * tensor-core launch). */
+#define BBX_STREAM_KERNEL_AUTO 0
+#define BBX_STREAM_KERNEL_REGISTER 1
+int bbx_stream_plan_create_kernel(const bbx_stream_op_t* ops, int count, int kernel, bbx_stream_plan_t** out);
 /* 1 when the plan runs the bulk-staged kernel (every pointer of every op
  * 16-byte aligned: inputs staged in shared memory by cp.async.bulk), 0 for
  * the register kernel, negative on error. */
@@ -378,6 +389,26 @@ int bbx_dag_profile(bbx_dag_t* dag, void* stream, int cap, int* kinds, int* wave
 int bbx_dag_tensor(bbx_dag_t* dag, int tid, void** ptr, void* meta_out);
 /* copies up to `cap` payload bytes of a DAG tensor to host memory (synchronous) */
 int bbx_dag_read(bbx_dag_t* dag, int tid, void* host_dst, size_t cap);
+/* Kernel of the grouped streaming launches of DAGs built afterwards on this
+ * runtime (BBX_STREAM_KERNEL_AUTO, the default: the bulk-staged kernel where
+ * aligned; BBX_STREAM_KERNEL_REGISTER: the register kernel, which can share
+ * SMs with the wave's tensor-core launch on the other stream). */
+int bbx_rt_set_dag_stream_kernel(bbx_rt_t* rt, int kernel);
+/* Stream-ordered host <-> block copies around bbx_dag_launch, the DAG's
+ * counterpart of the reference's per-command storage transactions
+ * (src/commands/command_runner.cc:86-172 reads inputs / writes outputs through
+ * the storage). bbx_dag_write overwrites `bytes` of an input block that the
+ * DAG reads in place (a registered tensor no command of the DAG writes;
+ * anything else is BBX_ERR_INVALID); bbx_dag_fetch copies up to `cap` bytes
+ * of any DAG tensor out. Both only enqueue a cudaMemcpyAsync on `stream`:
+ * with pinned host memory they overlap other work; the caller synchronises
+ * before reading `dst` or reusing `src`. */
+int bbx_dag_write(bbx_dag_t* dag, int tid, const void* src, size_t bytes, int src_on_device, void* stream);
+int bbx_dag_fetch(bbx_dag_t* dag, int tid, void* dst, size_t cap, int dst_on_device, void* stream);
+/* Tile of each launch group in profile order: 128 / 256 (1-SM tcgen05 width),
+ * 512 (the 2-SM 256 x 256 pair) for tensor-core groups, 0 for the others.
+ * Writes min(cap, groups) values; *n_out = the group count. */
+int bbx_dag_group_tiles(bbx_dag_t* dag, int cap, int* tiles, int* n_out);
 
 /* ------------------------------------------------------------------ learned cost model
  * MLP 12 -> 128 -> 128 -> 128 -> 1 (ReLU, FP32) predicting log latency from op

@@ -70,3 +70,48 @@ def test_cpu_step_sample():
     assert np.array_equal(c00, oracle.sgemm(a[0], b[0], threads=1))
     tf, done, dt, c00 = bench.cpu_step_tflops(a, b, threads=2, budget_s=0.0)
     assert done == 1 and c00 is not None
+
+
+def test_reference_arm_line(capsys):
+    """The reference arm on a tiny cpmm (2x2 grid of 64^2 blocks): a measured
+    warm-up product, a bounded sample per step, one JSON line whose
+    ms_per_step is a measured step (steps x ms_per_step fits the run) and
+    whose cpu_baseline / e2e restate the line's value."""
+    import json
+    import time
+    import types
+    sys.path.insert(0, ROOT)
+    import bench
+    saved = bench.GRID, bench.BS, bench.REF_BUDGET_S
+    bench.GRID, bench.BS, bench.REF_BUDGET_S = 2, 64, 0.05
+    try:
+        args = types.SimpleNamespace(gpus=1, steps=3, warmup=1)
+        t0 = time.perf_counter()
+        bench.run_reference(args)
+        wall = time.perf_counter() - t0
+    finally:
+        bench.GRID, bench.BS, bench.REF_BUDGET_S = saved
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["unit"] == "TFLOP/s" and line["value"] > 0
+    assert line["steps"] * line["ms_per_step"] * 1e-3 <= wall
+    assert line["cpu_baseline"]["value"] == line["value"] == line["e2e"]["value"]
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["kind"] == "port"
+
+
+def test_reference_inputs_are_the_device_fill_values():
+    """The reference arm's inputs restate the device fill: Philox uniform in
+    [-1, 1), rounded to bf16 (so exactly representable in bf16)."""
+    import numpy as np
+    import torch
+    sys.path.insert(0, ROOT)
+    import bench
+    saved = bench.GRID, bench.BS
+    bench.GRID, bench.BS = 2, 32
+    try:
+        a, b = bench.cpmm_block_inputs(bench.CPMM_SEED)
+    finally:
+        bench.GRID, bench.BS = saved
+    assert len(a) == 2 and a[0].shape == (32, 32)
+    x = torch.from_numpy(a[1])
+    assert torch.equal(x.to(torch.bfloat16).float(), x)
+    assert float(x.abs().max()) <= 1.0 and not np.array_equal(a[0], a[1])

@@ -1,4 +1,6 @@
 """Parity of the CUDA block kernels (through the C ABI) against the CPU oracle."""
+import zlib
+
 import numpy as np
 import pytest
 
@@ -324,13 +326,14 @@ def test_matmul_f32_integer_exact(T):
         assert np.array_equal(host(c), cref)
 
 
-def test_matmul_f32_epilogue_and_batch(T):
+@pytest.mark.parametrize("n", [90, 96])  # 90: element-wise kernel; 96: the 16-byte-load kernel, float4 epilogue
+def test_matmul_f32_epilogue_and_batch(T, n):
     torch, ops = T
     rng = np.random.default_rng(8)
     a = rng.standard_normal((3, 100, 64)).astype(np.float32)
-    b = rng.standard_normal((3, 64, 90)).astype(np.float32)
-    c0 = rng.standard_normal((3, 100, 90)).astype(np.float32)
-    bias = rng.standard_normal(90).astype(np.float32)
+    b = rng.standard_normal((3, 64, n)).astype(np.float32)
+    c0 = rng.standard_normal((3, 100, n)).astype(np.float32)
+    bias = rng.standard_normal(n).astype(np.float32)
     c = dev(torch, c0)
     ops.matmul_f32(dev(torch, a), dev(torch, b), c, alpha=0.5, beta=2.0, bias=dev(torch, bias), relu=True)
     ref = np.stack([oracle.matmul_f64(a[i], b[i]) for i in range(3)]) * 0.5 + 2.0 * c0 + bias
@@ -451,6 +454,47 @@ def test_matmul_fp8_per_block_scale(T):
     deq_a = qa.float().cpu().numpy() * host(sa)[0]
     deq_b = qb.float().cpu().numpy().T * host(sb)[0]
     assert rel_err(host(c), oracle.matmul_f64(np.ascontiguousarray(deq_a), np.ascontiguousarray(deq_b))) <= 1e-5
+
+
+def _quantize_ref(x, transpose):
+    """Host restatement of the e4m3 quantisation: s = 448 / absmax (f32
+    division), q = e4m3(x * s) rounded to nearest even with saturation at
+    +-448 (torch's cast does not saturate, so the clamp comes first; values
+    in (448, 464) round to 448 either way)."""
+    import torch
+    x = torch.as_tensor(x, dtype=torch.float32)
+    amax = float(x.abs().max())
+    s = np.float32(448.0) / np.float32(amax) if amax > 0 else np.float32(1.0)
+    q = (x * torch.tensor(s, dtype=torch.float32)).clamp(-448.0, 448.0).to(torch.float8_e4m3fn)
+    if transpose:
+        q = q.t().contiguous()
+    return q.view(torch.uint8), np.float32(amax) / np.float32(448.0) if amax > 0 else np.float32(1.0)
+
+
+@pytest.mark.parametrize("shape,dtype,transpose,offset", [
+    ((384, 640), "bf16", False, 0), ((384, 640), "bf16", True, 0),      # vector and tiled-transpose paths
+    ((384, 640), "f32", False, 0), ((384, 640), "f32", True, 0),
+    ((80, 264), "bf16", True, 0), ((4096, 4096), "bf16", True, 0),      # partial tiles; a full block
+    ((37, 53), "bf16", False, 0), ((37, 53), "f32", True, 0),           # element-wise fallback
+    ((64, 64), "f32", True, 1)])                                        # unaligned input -> fallback
+def test_quantize_e4m3_paths(T, shape, dtype, transpose, offset):
+    """Every dispatch path of the FP8 quantiser gives the host restatement's
+    bytes and scale exactly."""
+    torch, ops = T
+    rng = np.random.default_rng(zlib.crc32(repr((shape, dtype, transpose, offset)).encode()))
+    x = (rng.standard_normal(shape) * 3).astype(np.float32)
+    tdt = torch.bfloat16 if dtype == "bf16" else torch.float32
+    flat = torch.empty(x.size + offset, dtype=tdt, device="cuda")
+    xd = flat[offset:].view(shape)
+    xd.copy_(torch.from_numpy(x))
+    out_shape = (shape[1], shape[0]) if transpose else shape
+    q = torch.empty(out_shape, dtype=torch.float8_e4m3fn, device="cuda")
+    scale = torch.empty(1, device="cuda")
+    ops.quantize_e4m3(xd, q, scale, transpose=transpose)
+    torch.cuda.synchronize()
+    want, want_scale = _quantize_ref(xd.float().cpu(), transpose)
+    assert torch.equal(q.view(torch.uint8).cpu(), want)
+    assert float(scale.cpu()[0]) == float(want_scale)
 
 
 # ----------------------------------------------------------------- contraction
