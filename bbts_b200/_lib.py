@@ -104,6 +104,7 @@ SIGNATURES = {
     "bbx_dag_read": (i32, [vp, i32, vp, sz]),
     "bbx_stream_plan_create_kernel": (i32, [vp, i32, i32, C.POINTER(vp)]),
     "bbx_rt_set_dag_stream_kernel": (i32, [vp, i32]),
+    "bbx_dag_register_waves": (i32, [vp]),
     "bbx_dag_write": (i32, [vp, i32, vp, sz, i32, vp]),
     "bbx_dag_fetch": (i32, [vp, i32, vp, sz, i32, vp]),
     "bbx_dag_group_tiles": (i32, [vp, i32, vp, C.POINTER(i32)]),

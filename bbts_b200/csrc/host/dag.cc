@@ -39,6 +39,10 @@
 #include "contraction.h"
 #include "runtime.h"
 
+namespace bbx {
+int pick_tile_n(const bbx_tc_problem_t* probs, int count, int in_dtype);  // abi_kernels.cu
+}
+
 namespace bbts {
 
 namespace {
@@ -334,6 +338,25 @@ int learned_tile_n(const runtime_t& rt, int dtype, bool ta, bool tb, const std::
   for (size_t i = 1; i < cand.size() && i < t.size(); ++i)
     if (t[i] < t[best]) best = i;
   return cand[best];
+}
+
+// Bytes per microsecond of the bulk streaming kernel alone on DAG levels
+// (4.7 TB/s measured on the 2000-op DAG's levels).
+constexpr double kBulkStreamBytesPerUs = 4.7e6;
+
+// Predicted duration (us) of a grouped tensor-core launch with tile `tn`: the
+// tile model's prediction when one is installed, else its FLOPs at 1 PFLOP/s
+// (about the grouped kernel's rate on the DAG's matmul groups).
+double predicted_tc_us(const runtime_t& rt, int dtype, bool ta, bool tb, const std::vector<bbx_tc_problem_t>& ps,
+                       int tn) {
+  if (rt.tile_predictor) {
+    if (tn == 0) {
+      std::vector<bbx_tc_problem_t> v(ps);
+      tn = bbx::pick_tile_n(v.data(), (int)v.size(), dtype == ELEM_E4M3 ? BBX_E4M3 : BBX_BF16);
+    }
+    return rt.tile_predictor({tile_features(dtype, ta, tb, ps, tn)})[0];
+  }
+  return tc_group_flops(ps) / 1e15 * 1e6;
 }
 
 // Contraction params: rank_l, rank_r, rank_o, modes_l..., modes_r..., modes_o..., alpha.
@@ -728,10 +751,37 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
       d->groups.push_back(std::move(gpre));
       d->stats.stream_launches++;
     }
+    // tiles of the wave's tensor groups first: the per-wave streaming kernel
+    // choice weighs the wave's predicted tensor time
+    std::map<int, int> tc_tile;
+    double tc_us = 0.0;
+    for (auto& kv : tc_groups) {
+      const int dt = (kv.first & 0xff) / 4;
+      // tile_n -1: autotune per group; -2: the learned tile model (the size
+      // heuristic without one); 0: size heuristic; 128 / 256 / 512: forced
+      const bool ta = (kv.first & 2) != 0, tb = (kv.first & 1) != 0;
+      int tn = tile_n;
+      if (tile_n == -2) tn = rt->tile_predictor ? learned_tile_n(*rt, dt, ta, tb, kv.second) : 0;
+      else if (tile_n < 0) tn = autotune_tile_n(dt, ta, tb, kv.second);
+      tc_tile[kv.first] = tn;
+      if (rt->dag_stream_kernel == BBX_STREAM_KERNEL_PER_WAVE)
+        tc_us += predicted_tc_us(*rt, dt, ta, tb, kv.second, tn);
+    }
+    int stream_kernel = rt->dag_stream_kernel;
+    if (stream_kernel == BBX_STREAM_KERNEL_PER_WAVE) {
+      double st_bytes = 0.0;
+      for (auto& ph : phases) st_bytes += stream_group_bytes(ph);
+      // the register kernel shares SMs with the tensor launch but streams
+      // slower than the bulk kernel alone: worth it when the wave's tensor work
+      // is long enough to hide the streaming work under it
+      const double st_us = st_bytes / kBulkStreamBytesPerUs;
+      stream_kernel = (st_bytes > 0 && tc_us >= st_us) ? BBX_STREAM_KERNEL_REGISTER : BBX_STREAM_KERNEL_AUTO;
+      if (stream_kernel == BBX_STREAM_KERNEL_REGISTER && st_bytes > 0) d->stats.register_waves++;
+    }
     for (size_t ph = 0; ph < phases.size(); ++ph) {
       if (phases[ph].empty()) continue;
       group_t g{G_STREAM, w};
-      dag_bbx(bbx_stream_plan_create_kernel(phases[ph].data(), (int)phases[ph].size(), rt->dag_stream_kernel,
+      dag_bbx(bbx_stream_plan_create_kernel(phases[ph].data(), (int)phases[ph].size(), stream_kernel,
                                             &g.stream_plan));
       g.bytes = stream_group_bytes(phases[ph]);
       g.reads = phase_rw[ph].first;
@@ -746,12 +796,7 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
     for (auto& kv : tc_groups) {
       group_t g{G_TC, w};
       const int dt = (kv.first & 0xff) / 4;
-      // tile_n -1: autotune per group; -2: the learned tile model (the size
-      // heuristic without one); 0: size heuristic; 128 / 256 / 512: forced
-      const bool ta = (kv.first & 2) != 0, tb = (kv.first & 1) != 0;
-      int tn = tile_n;
-      if (tile_n == -2) tn = rt->tile_predictor ? learned_tile_n(*rt, dt, ta, tb, kv.second) : 0;
-      else if (tile_n < 0) tn = autotune_tile_n(dt, ta, tb, kv.second);
+      const int tn = tc_tile.at(kv.first);
       dag_bbx(bbx_tc_plan_create(dt == ELEM_E4M3 ? BBX_E4M3 : BBX_BF16, kv.second.data(), (int)kv.second.size(), tn,
                                  &g.tc_plan));
       g.flops = tc_group_flops(kv.second);

@@ -435,10 +435,15 @@ int bbx_dag_read(bbx_dag_t* dag, int tid, void* host_dst, size_t cap) {
 
 int bbx_rt_set_dag_stream_kernel(bbx_rt_t* rt, int kernel) {
   if (!rt) return bbx::set_error(BBX_ERR_INVALID, "null runtime");
-  if (kernel != BBX_STREAM_KERNEL_AUTO && kernel != BBX_STREAM_KERNEL_REGISTER)
+  if (kernel != BBX_STREAM_KERNEL_AUTO && kernel != BBX_STREAM_KERNEL_REGISTER && kernel != BBX_STREAM_KERNEL_PER_WAVE)
     return bbx::set_error(BBX_ERR_INVALID, "dag stream kernel %d", kernel);
   rt->rt.dag_stream_kernel = kernel;
   return BBX_OK;
+}
+
+int bbx_dag_register_waves(bbx_dag_t* dag) {
+  if (!dag) return bbx::set_error(BBX_ERR_INVALID, "null dag");
+  return dag_stats(dag->d).register_waves;
 }
 
 int bbx_dag_write(bbx_dag_t* dag, int tid, const void* src, size_t bytes, int src_on_device, void* stream) {

@@ -219,6 +219,7 @@ void dag_launch(dag_t* d, cudaStream_t st);
 void dag_destroy(dag_t* d);
 struct dag_stats_t {
   int waves, tc_launches, stream_launches, opaque_launches, nodes;
+  int register_waves;  // waves whose streaming launches run the register kernel (per-wave choice)
   double flops, bytes;
   size_t arena_bytes;
 };

@@ -251,7 +251,7 @@ class Runtime:
     def set_dag_stream_kernel(self, kernel):
         """Streaming kernel of DAGs built afterwards: 0 = bulk-staged where
         aligned (default), 1 = the register kernel (shares SMs with tensor-core
-        launches)."""
+        launches), 2 = chosen per wave from predicted tensor / streaming times."""
         check(lib.bbx_rt_set_dag_stream_kernel(self.h, int(kernel)))
 
     def build_dag(self, policy=HEURISTIC, tile_n=0):
@@ -345,6 +345,13 @@ class Dag:
         """Enqueues a copy of up to `cap` payload bytes of `tid` to `dst_ptr`."""
         check(lib.bbx_dag_fetch(self.h, tid, C.c_void_p(dst_ptr), cap, int(on_device),
                                 stream if stream is not None else self.rt.stream))
+
+    def register_waves(self):
+        """Waves whose streaming launches run the register kernel."""
+        n = lib.bbx_dag_register_waves(self.h)
+        if n < 0:
+            check(n)
+        return n
 
     def group_tiles(self):
         """Tile of each launch group, in profile order (0 for non-tensor-core groups)."""

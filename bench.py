@@ -67,9 +67,9 @@ def parse():
     p.add_argument("--configs", default="bmm,ffnn,dag",
                    help="cpmm line: other configurations run through the runtime as sub-objects "
                         "(comma list of bmm, ffnn, dag; none to skip)")
-    p.add_argument("--stream-kernel", type=int, default=0, choices=[0, 1],
+    p.add_argument("--stream-kernel", type=int, default=0, choices=[0, 1, 2],
                    help="DAG streaming launches: 0 = bulk-staged kernel where aligned, 1 = register kernel "
-                        "(shares SMs with the wave's tensor-core launch)")
+                        "(shares SMs with the wave's tensor-core launch), 2 = chosen per wave from predicted times")
     p.add_argument("--n-ops", type=int, default=0, help="DAG size override (dag: 2000, learned: 5000)")
     p.add_argument("--train-dags", type=int, default=100, help="learned: DAGs recorded for the training set")
     p.add_argument("--tile-dags", type=int, default=16,
@@ -464,7 +464,7 @@ def dag_config(workload, args, hbm, bf16_peak, per_group=True):
     dag.close()
     rt.close()
     name = DAG_NAMES[workload] % (args.n_ops or 2000) if workload == "dag" else DAG_NAMES[workload]
-    return {"workload": name, "flops_per_step": flops, "stream_kernel": "register" if sk else "bulk where aligned",
+    return {"workload": name, "flops_per_step": flops, "stream_kernel": ["bulk where aligned", "register", "per wave"][sk],
             "value": round(flops / ms / 1e9, 2), "unit": "TFLOP/s",
             "ms_per_step": round(ms, 3),
             "makespan_ms": {"grouped_bf16_graph": round(ms, 3), "grouped_fp32_graph": round(gms, 3),

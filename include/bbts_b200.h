@@ -233,6 +233,12 @@ int bbx_stream_plan_destroy(bbx_stream_plan_t* plan);
  * tensor-core launch). */
 #define BBX_STREAM_KERNEL_AUTO 0
 #define BBX_STREAM_KERNEL_REGISTER 1
+/* DAG builds only (bbx_rt_set_dag_stream_kernel): per wave, the register
+ * kernel when the wave's predicted tensor-core time is at least its predicted
+ * bulk streaming time (the streaming work then hides under the tensor work),
+ * else AUTO. Tensor time comes from the runtime's tile model when one is
+ * installed (bbx_rt_set_tile_predictor), else from the group's FLOPs. */
+#define BBX_STREAM_KERNEL_PER_WAVE 2
 int bbx_stream_plan_create_kernel(const bbx_stream_op_t* ops, int count, int kernel, bbx_stream_plan_t** out);
 /* 1 when the plan runs the bulk-staged kernel (every pointer of every op
  * 16-byte aligned: inputs staged in shared memory by cp.async.bulk), 0 for
@@ -392,8 +398,11 @@ int bbx_dag_read(bbx_dag_t* dag, int tid, void* host_dst, size_t cap);
 /* Kernel of the grouped streaming launches of DAGs built afterwards on this
  * runtime (BBX_STREAM_KERNEL_AUTO, the default: the bulk-staged kernel where
  * aligned; BBX_STREAM_KERNEL_REGISTER: the register kernel, which can share
- * SMs with the wave's tensor-core launch on the other stream). */
+ * SMs with the wave's tensor-core launch on the other stream;
+ * BBX_STREAM_KERNEL_PER_WAVE: chosen per wave from predicted times). */
 int bbx_rt_set_dag_stream_kernel(bbx_rt_t* rt, int kernel);
+/* Waves of the DAG whose streaming launches run the register kernel. */
+int bbx_dag_register_waves(bbx_dag_t* dag);
 /* Stream-ordered host <-> block copies around bbx_dag_launch, the DAG's
  * counterpart of the reference's per-command storage transactions
  * (src/commands/command_runner.cc:86-172 reads inputs / writes outputs through

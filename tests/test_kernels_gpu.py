@@ -316,6 +316,30 @@ def test_matmul_f32_vs_f64(T, m, n, k, ta, tb):
     assert rel_err(host(c), ref) <= 1e-5
 
 
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+def test_matmul_vs_cpu_port_of_reference_sgemm(T, ta, tb):
+    """The GPU block matmuls against the oracle's CPU port of the reference's
+    block matmul (dense_matrix_mult.cc:78-82, cblas_sgemm RowMajor with the
+    transpose flags) on the same seeded inputs: the FP32 SIMT path within
+    1e-5 of the port's FP32 result, and the bf16 tensor-core path, on the
+    bf16-rounded inputs, within 1e-5 of the port run on those inputs."""
+    torch, ops = T
+    rng = np.random.default_rng(100 + 2 * ta + tb)
+    m, n, k = 512, 384, 640
+    a = rng.uniform(-1, 1, (k, m) if ta else (m, k)).astype(np.float32)
+    b = rng.uniform(-1, 1, (n, k) if tb else (k, n)).astype(np.float32)
+    port = oracle.sgemm(a, b, bool(ta), bool(tb), threads=4)
+    c = torch.empty(m, n, device="cuda")
+    ops.matmul_f32(dev(torch, a), dev(torch, b), c, bool(ta), bool(tb))
+    assert rel_err(host(c), port) <= 1e-5
+    ab, bb = bf16_round(a), bf16_round(b)
+    port16 = oracle.sgemm(ab, bb, bool(ta), bool(tb), threads=4)
+    c16 = torch.empty(m, n, device="cuda")
+    ops.matmul_tc([ops.tc_problem(dev(torch, ab, torch.bfloat16), dev(torch, bb, torch.bfloat16), c16,
+                                  trans_a=bool(ta), trans_b=bool(tb))])
+    assert rel_err(host(c16), port16) <= 1e-5
+
+
 def test_matmul_f32_integer_exact(T):
     torch, ops = T
     g = golden("matmul_int.npz")
