@@ -1,5 +1,7 @@
 """The native runtime on the GPU: ud registry + per-op path + grouped DAG path +
 learned cost model, checked against the CPU oracle."""
+import struct
+
 import numpy as np
 import pytest
 
@@ -625,6 +627,37 @@ def test_random_bf16_dag_with_contractions_matches_per_op(R, policy):
             a = rt1.get_bytes(t)
             b = dag.read_bytes(t, a.nbytes)
             assert np.array_equal(a, b), t
+
+
+@pytest.mark.parametrize("stream_kernel", [1, 2])
+def test_dag_streaming_kernel_choice_keeps_results(R, stream_kernel):
+    """The register streaming kernel (1) and the per-wave choice (2) give the
+    same bytes as the default bulk kernel: both kernels fold the inputs in the
+    same order; the per-wave choice picks the register kernel for at least one
+    wave of a DAG whose waves carry tensor work."""
+    runtime, workloads = R
+    mk = lambda rt: workloads.random_dag(rt, n_ops=120, depth=5, seed=23, dtype="bf16", lo=256, hi=1024, step=64,
+                                         contraction_dims=(16, 72), mix=(0.55, 0.2, 0.2, 0.05))
+    rt1 = runtime.Runtime()
+    info = mk(rt1)
+    dag1 = rt1.build_dag(runtime.HEURISTIC, tile_n=256)
+    dag1.launch()
+    rt2 = runtime.Runtime()
+    mk(rt2)
+    rt2.set_dag_stream_kernel(stream_kernel)
+    dag2 = rt2.build_dag(runtime.HEURISTIC, tile_n=256)
+    if stream_kernel == 2:
+        assert 1 <= dag2.register_waves() <= dag2.stats()["waves"]
+    dag2.launch()
+    checked = 0
+    for t in info["finals"]:
+        _, meta = dag1.tensor(t)
+        if struct.unpack_from("<i", meta, 0)[0] == rt1.fmt("cutensor"):
+            continue
+        assert np.array_equal(read_dense(rt1, t, dag1), read_dense(rt2, t, dag2)), t
+        checked += 1
+    assert checked > 0
+    dag1.close(); dag2.close(); rt1.close(); rt2.close()
 
 
 # ------------------------------------------------------------------ multi-stream per-op executor
