@@ -41,13 +41,20 @@ struct tensor_meta_t {
   tfid_t fmt_id;
   char _blob[MAX_META_SIZE];
 
-  // The payload address this library set, or nullptr when the slot is not
-  // tagged (a meta this library did not place).
-  void* payload() const {
+  // True when this library set the payload slot (the tag matches).
+  bool payload_tagged() const {
     uint64_t p, tag;
     std::memcpy(&p, _blob + PAYLOAD_SLOT, sizeof(p));
     std::memcpy(&tag, _blob + PAYLOAD_TAG, sizeof(tag));
-    return (tag ^ p) == kPayloadMagic ? (void*)p : nullptr;
+    return (tag ^ p) == kPayloadMagic;
+  }
+  // The payload address this library set (nullptr for a block with no
+  // resident payload), or nullptr when the slot is not tagged.
+  void* payload() const {
+    if (!payload_tagged()) return nullptr;
+    uint64_t p;
+    std::memcpy(&p, _blob + PAYLOAD_SLOT, sizeof(p));
+    return (void*)p;
   }
   void set_payload(void* p) {
     const uint64_t v = (uint64_t)p, tag = v ^ kPayloadMagic;
@@ -64,11 +71,11 @@ struct tensor_t {
   template <class T>
   T& as() const { return *((T*)this); }
 
-  // The payload: the tagged slot's address, else the bytes after the header
-  // (the reference's layout).
+  // The payload: the tagged slot's address (nullptr for a block with no
+  // resident payload), else the bytes after the header (the reference's layout).
   void* payload() const {
-    void* p = _meta.payload();
-    return p ? p : (void*)((const char*)this + sizeof(tensor_meta_t));
+    if (_meta.payload_tagged()) return _meta.payload();
+    return (void*)((const char*)this + sizeof(tensor_meta_t));
   }
 
   tensor_meta_t _meta;

@@ -59,6 +59,27 @@ static void test_dense_format() {
   auto& t = tf.init_tensor((tensor_t*)mem.data(), m).as<dense_tensor_t>();
   EXPECT((char*)t.data() == mem.data() + sizeof(tensor_meta_t));
   EXPECT(t.meta().m().num_rows == 100 && t.meta().m().num_cols == 200);
+  // payload slot: tagged by this library; an untagged header (a tensor the
+  // reference initialised, zeroed or garbage blob) has its payload inline
+  {
+    std::vector<char> raw(sizeof(tensor_meta_t) + 16, 0);
+    tensor_t* u = (tensor_t*)raw.data();
+    u->_meta.fmt_id = id;
+    EXPECT(!u->_meta.payload_tagged() && u->_meta.payload() == nullptr);
+    EXPECT((char*)u->payload() == raw.data() + sizeof(tensor_meta_t));
+    for (size_t i = 0; i < tensor_meta_t::MAX_META_SIZE; ++i) u->_meta._blob[i] = (char)(i * 37 + 11);
+    EXPECT(!u->_meta.payload_tagged() && (char*)u->payload() == raw.data() + sizeof(tensor_meta_t));
+    int dev_word = 0;
+    u->_meta.set_payload(&dev_word);  // a device address placed by this library
+    EXPECT(u->_meta.payload_tagged() && u->payload() == &dev_word);
+    u->_meta.set_payload(nullptr);    // a block with no resident payload (zero bytes, or spilled)
+    EXPECT(u->_meta.payload_tagged() && u->payload() == nullptr);
+    tensor_meta_t copy = u->_meta;    // the tag travels with the meta
+    copy.set_payload(&dev_word);
+    EXPECT(copy.payload() == &dev_word);
+    copy._blob[tensor_meta_t::PAYLOAD_SLOT] ^= 1;  // a slot changed behind the tag is not trusted
+    EXPECT(!copy.payload_tagged());
+  }
   // register_fmt returns the new id, and the first one on re-registration
   tfid_t f2 = tf.register_fmt("ffnn_dense", ffnn_dense_creation_fs());
   EXPECT(f2 == tf.get_tensor_ftm("ffnn_dense"));
