@@ -636,8 +636,10 @@ def test_dag_streaming_kernel_choice_keeps_results(R, stream_kernel):
     same order; the per-wave choice picks the register kernel for at least one
     wave of a DAG whose waves carry tensor work."""
     runtime, workloads = R
-    mk = lambda rt: workloads.random_dag(rt, n_ops=120, depth=5, seed=23, dtype="bf16", lo=256, hi=1024, step=64,
-                                         contraction_dims=(16, 72), mix=(0.55, 0.2, 0.2, 0.05))
+    # tensor-heavy waves (80 % matmuls of 512..1024): the FLOP estimate puts
+    # the register kernel on most waves
+    mk = lambda rt: workloads.random_dag(rt, n_ops=120, depth=5, seed=23, dtype="bf16", lo=512, hi=1024, step=64,
+                                         mix=(0.8, 0.1, 0.1, 0.0))
     rt1 = runtime.Runtime()
     info = mk(rt1)
     dag1 = rt1.build_dag(runtime.HEURISTIC, tile_n=256)
