@@ -42,3 +42,23 @@ def test_ffnn_program_round_trip(tmp_path):
     assert all("fill" in v or v["data"] is not None for v in inputs.values())
     programs.write_bbts(str(tmp_path / "again.bbts"), cmds)
     assert open(str(tmp_path / "again.bbts"), "rb").read() == open(path, "rb").read()
+
+
+def test_cpmm_seed_formula_is_shared():
+    """bench.py restates the cpmm input seeds on the host (its reference arm
+    must not load the library); they must equal workloads.cpmm_seeds and the
+    seeds cpmm_bbts writes into its uniform APPLYs."""
+    import os
+    import sys
+    import tempfile
+    from bbts_b200 import workloads
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    sa, sb = workloads.cpmm_seeds(bench.CPMM_SEED, bench.GRID, bench.GRID)
+    assert sa == [bench.CPMM_SEED + i for i in range(bench.GRID)]
+    assert sb == [bench.CPMM_SEED + 1000 + j for j in range(bench.GRID)]
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "c.bbts")
+        programs.cpmm_bbts(path, rows=bench.GRID, cols=bench.GRID, bs=64, seed=bench.CPMM_SEED)
+        seeds = [c["params"][4] for c in programs.read_bbts(path) if c["ud"] == "uniform"]
+    assert seeds == sa + sb
