@@ -51,6 +51,7 @@ SIGNATURES = {
     "bbx_cast": (i32, [i32, pf, i32, pf, i64, vp]),
     "bbx_relu_split": (i32, [pf, vp, vp, i64, vp]),
     "bbx_quantize_e4m3": (i32, [i32, pf, pf, i32, i32, i32, pf, vp]),
+    "bbx_quantize_e4m3_batched": (i32, [i32, C.POINTER(vp), C.POINTER(vp), i32, i32, i32, i32, pf, vp]),
     "bbx_quantize_e4m3_batched_noalloc": (i32, [i32, C.POINTER(vp), C.POINTER(vp), i32, i32, i32, i32, pf, vp]),
     "bbx_fill_philox": (i32, [i32, pf, i64, u64, i32, f32, f32, vp]),
     "bbx_softmax_ce_f32": (i32, [pf, pf, pf, pf, i32, i32, i64, f32, vp]),

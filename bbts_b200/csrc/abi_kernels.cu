@@ -626,13 +626,43 @@ int bbx_quantize_e4m3(int src_dtype, const void* in, void* out, int rows, int co
   unsigned int* amax = nullptr;
   BBX_CUDA(cudaMallocAsync((void**)&amax, 4, st));
   BBX_CUDA(cudaMemsetAsync(amax, 0, 4, st));
-  cudaError_t le = src_dtype == BBX_F32
-                       ? launch_quantize_block((const float*)in, (uint8_t*)out, rows, cols, transpose, amax,
-                                               scale_out, d->sms, st)
-                       : launch_quantize_block((const __nv_bfloat16*)in, (uint8_t*)out, rows, cols, transpose,
-                                               amax, scale_out, d->sms, st);
+  uint8_t* o = (uint8_t*)out;
+  cudaError_t le;
+  if (src_dtype == BBX_F32) {
+    const float* i = (const float*)in;
+    le = launch_quantize_batch(&i, &o, 1, rows, cols, transpose, amax, scale_out, d->sms, st);
+  } else {
+    const __nv_bfloat16* i = (const __nv_bfloat16*)in;
+    le = launch_quantize_batch(&i, &o, 1, rows, cols, transpose, amax, scale_out, d->sms, st);
+  }
   cudaFreeAsync(amax, st);
   if (le != cudaSuccess) return set_error(BBX_ERR_CUDA, "quantize_e4m3: %s", cudaGetErrorString(le));
+  return BBX_OK;
+}
+
+int bbx_quantize_e4m3_batched(int src_dtype, const void* const* in, void* const* out, int count, int rows, int cols,
+                              int transpose, float* scales_out, void* stream) {
+  if (count == 0) return BBX_OK;
+  if (!in || !out || !scales_out || rows <= 0 || cols <= 0 || count < 0)
+    return set_error(BBX_ERR_INVALID, "bad batched quantize arguments");
+  if (src_dtype != BBX_F32 && src_dtype != BBX_BF16) return set_error(BBX_ERR_UNSUPPORTED, "quantize source dtype");
+  for (int i = 0; i < count; ++i)
+    if (!in[i] || !out[i]) return set_error(BBX_ERR_INVALID, "null block pointer %d", i);
+  DeviceState* d;
+  int rc = device_state(&d);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  // one absmax word per block, stream-ordered scratch of this call
+  unsigned int* amax = nullptr;
+  BBX_CUDA(cudaMallocAsync((void**)&amax, sizeof(unsigned int) * count, st));
+  BBX_CUDA(cudaMemsetAsync(amax, 0, sizeof(unsigned int) * count, st));
+  cudaError_t le = src_dtype == BBX_F32
+                       ? launch_quantize_batch((const float* const*)in, (uint8_t* const*)out, count, rows, cols,
+                                               transpose, amax, scales_out, d->sms, st)
+                       : launch_quantize_batch((const __nv_bfloat16* const*)in, (uint8_t* const*)out, count, rows,
+                                               cols, transpose, amax, scales_out, d->sms, st);
+  cudaFreeAsync(amax, st);
+  if (le != cudaSuccess) return set_error(BBX_ERR_CUDA, "quantize_e4m3_batched: %s", cudaGetErrorString(le));
   return BBX_OK;
 }
 

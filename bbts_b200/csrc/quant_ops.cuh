@@ -97,9 +97,21 @@ __device__ __forceinline__ uint32_t q2(float a, float b, float s) {
 
 constexpr int kQuantThreads = 256;
 
+// A batch of blocks quantised by one launch of each pass: block y of the grid
+// (blockIdx.y) works on in[y] / out[y] / scale[y] with absmax word amax[y].
+constexpr int kQuantBatchMax = 64;
 template <typename T>
-__global__ void __launch_bounds__(kQuantThreads) k_absmax_v(const T* __restrict__ in, long long n8,
-                                                            unsigned int* amax) {
+struct QuantBatch {
+  const T* in[kQuantBatchMax];
+  uint8_t* out[kQuantBatchMax];
+  float* scale[kQuantBatchMax];
+  unsigned int* amax;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kQuantThreads) k_absmax_v(const __grid_constant__ QuantBatch<T> b, long long n8) {
+  const T* __restrict__ in = b.in[blockIdx.y];
+  unsigned int* amax = b.amax + blockIdx.y;
   float m = 0.f;
   const long long stride = (long long)gridDim.x * blockDim.x;
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -132,9 +144,11 @@ __global__ void __launch_bounds__(kQuantThreads) k_absmax_v(const T* __restrict_
 
 // Row-major output: 8 elements in, 8 packed bytes out per step.
 template <typename T>
-__global__ void __launch_bounds__(kQuantThreads) k_quant_e4m3_v(const T* __restrict__ in, uint8_t* out,
-                                                                long long n8, const unsigned int* amax,
-                                                                float* scale_out) {
+__global__ void __launch_bounds__(kQuantThreads) k_quant_e4m3_v(const __grid_constant__ QuantBatch<T> b, long long n8) {
+  const T* __restrict__ in = b.in[blockIdx.y];
+  uint8_t* out = b.out[blockIdx.y];
+  const unsigned int* amax = b.amax + blockIdx.y;
+  float* scale_out = b.scale[blockIdx.y];
   const float s = quant_scale(amax);
   write_scale(amax, scale_out);
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -171,9 +185,12 @@ __global__ void __launch_bounds__(kQuantThreads) k_quant_e4m3_v(const T* __restr
 constexpr int kQtR = 64, kQtC = 128, kQtWords = 18;
 
 template <typename T>
-__global__ void __launch_bounds__(kQuantThreads) k_quant_e4m3_t(const T* __restrict__ in, uint8_t* out, int rows,
-                                                                int cols, const unsigned int* amax,
-                                                                float* scale_out) {
+__global__ void __launch_bounds__(kQuantThreads) k_quant_e4m3_t(const __grid_constant__ QuantBatch<T> b, int rows,
+                                                                int cols) {
+  const T* __restrict__ in = b.in[blockIdx.y];
+  uint8_t* out = b.out[blockIdx.y];
+  const unsigned int* amax = b.amax + blockIdx.y;
+  float* scale_out = b.scale[blockIdx.y];
   __shared__ __align__(16) uint32_t tile[kQtC * kQtWords];
   const float s = quant_scale(amax);
   write_scale(amax, scale_out);
@@ -215,37 +232,62 @@ __global__ void __launch_bounds__(kQuantThreads) k_quant_e4m3_t(const T* __restr
   }
 }
 
-// Enqueues the absmax and quantisation passes of one block on `st`; amax must
-// hold 0 when the first pass runs. Returns the launch error, if any.
+// Enqueues the absmax and quantisation passes of `count` blocks (each rows x
+// cols) on `st`: block i reads in[i], writes out[i] and scales[i], with absmax
+// word amax[i], which must hold 0 when the first pass runs. When every block
+// qualifies for the vector kernels, each pass is one launch per 64 blocks
+// (grid.y = block); otherwise each block takes the element-wise kernels.
+// Returns the launch error, if any.
 template <typename T>
-inline cudaError_t launch_quantize_block(const T* in, uint8_t* out, int rows, int cols, int transpose,
-                                         unsigned int* amax, float* scale_out, int sms, cudaStream_t st) {
+inline cudaError_t launch_quantize_batch(const T* const* in, uint8_t* const* out, int count, int rows, int cols,
+                                         int transpose, unsigned int* amax, float* scales, int sms, cudaStream_t st) {
   const long long n = (long long)rows * cols;
-  const bool a16 = ((uintptr_t)in & 15) == 0, o16 = ((uintptr_t)out & 15) == 0;
   const long long cap = (long long)sms * 8;
-  if (a16 && n % 8 == 0) {
-    const long long n8 = n / 8;
-    long long g = (n8 + kQuantThreads * 4 - 1) / (kQuantThreads * 4);
-    g = g < 1 ? 1 : g > cap ? cap : g;
-    k_absmax_v<T><<<(int)g, kQuantThreads, 0, st>>>(in, n8, amax);
-  } else {
-    long long g = (n + 255) / 256;
-    g = g < 1 ? 1 : g > cap ? cap : g;
-    k_absmax<T><<<(int)g, 256, 0, st>>>(in, n, amax);
+  bool a16 = n % 8 == 0, o16 = true, o8 = true;
+  for (int i = 0; i < count; ++i) {
+    a16 = a16 && ((uintptr_t)in[i] & 15) == 0;
+    o16 = o16 && ((uintptr_t)out[i] & 15) == 0;
+    o8 = o8 && ((uintptr_t)out[i] & 7) == 0;
   }
-  if (!transpose && a16 && ((uintptr_t)out & 7) == 0 && n % 8 == 0) {
-    const long long n8 = n / 8;
-    long long g = (n8 + kQuantThreads * 2 - 1) / (kQuantThreads * 2);
-    g = g < 1 ? 1 : g > cap ? cap : g;
-    k_quant_e4m3_v<T><<<(int)g, kQuantThreads, 0, st>>>(in, out, n8, amax, scale_out);
-  } else if (transpose && a16 && o16 && rows % 16 == 0 && cols % 8 == 0) {
-    long long tiles = (long long)((cols + kQtC - 1) / kQtC) * ((rows + kQtR - 1) / kQtR);
-    long long g = tiles < cap ? tiles : cap;
-    k_quant_e4m3_t<T><<<(int)g, kQuantThreads, 0, st>>>(in, out, rows, cols, amax, scale_out);
-  } else {
-    long long g = (n + 255) / 256;
-    g = g < 1 ? 1 : g > cap ? cap : g;
-    k_quant_e4m3<T><<<(int)g, 256, 0, st>>>(in, (__nv_fp8_e4m3*)out, rows, cols, amax, scale_out, transpose);
+  const bool vec_abs = a16;
+  const bool vec_q = !transpose && a16 && o8;
+  const bool vec_t = transpose && a16 && o16 && rows % 16 == 0 && cols % 8 == 0;
+  for (int b0 = 0; b0 < count; b0 += kQuantBatchMax) {
+    const int cnt = count - b0 < kQuantBatchMax ? count - b0 : kQuantBatchMax;
+    QuantBatch<T> qb;
+    for (int i = 0; i < cnt; ++i) {
+      qb.in[i] = in[b0 + i];
+      qb.out[i] = out[b0 + i];
+      qb.scale[i] = scales + b0 + i;
+    }
+    qb.amax = amax + b0;
+    const long long per = cap / cnt > 1 ? cap / cnt : 1;  // CTAs per block: about 8 per SM in all
+    if (vec_abs) {
+      const long long n8 = n / 8;
+      long long g = (n8 + kQuantThreads * 4 - 1) / (kQuantThreads * 4);
+      g = g < 1 ? 1 : g > per ? per : g;
+      k_absmax_v<T><<<dim3((unsigned)g, (unsigned)cnt), kQuantThreads, 0, st>>>(qb, n8);
+    } else {
+      long long g = (n + 255) / 256;
+      g = g < 1 ? 1 : g > cap ? cap : g;
+      for (int i = 0; i < cnt; ++i) k_absmax<T><<<(int)g, 256, 0, st>>>(qb.in[i], n, qb.amax + i);
+    }
+    if (vec_q) {
+      const long long n8 = n / 8;
+      long long g = (n8 + kQuantThreads * 2 - 1) / (kQuantThreads * 2);
+      g = g < 1 ? 1 : g > per ? per : g;
+      k_quant_e4m3_v<T><<<dim3((unsigned)g, (unsigned)cnt), kQuantThreads, 0, st>>>(qb, n8);
+    } else if (vec_t) {
+      const long long tiles = (long long)((cols + kQtC - 1) / kQtC) * ((rows + kQtR - 1) / kQtR);
+      const long long g = tiles < per ? tiles : per;
+      k_quant_e4m3_t<T><<<dim3((unsigned)g, (unsigned)cnt), kQuantThreads, 0, st>>>(qb, rows, cols);
+    } else {
+      long long g = (n + 255) / 256;
+      g = g < 1 ? 1 : g > cap ? cap : g;
+      for (int i = 0; i < cnt; ++i)
+        k_quant_e4m3<T><<<(int)g, 256, 0, st>>>(qb.in[i], (__nv_fp8_e4m3*)qb.out[i], rows, cols, qb.amax + i,
+                                                qb.scale[i], transpose);
+    }
   }
   return cudaGetLastError();
 }

@@ -85,14 +85,12 @@ extern "C" int bbx_quantize_e4m3_batched_noalloc(int src_dtype, const void* cons
   // the array keeps the previous call's words: clear the ones this call uses
   cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(unsigned int) * count, st);
   if (e != cudaSuccess) return set_error(BBX_ERR_CUDA, "cudaMemsetAsync(no-alloc scratch): %s", cudaGetErrorString(e));
-  for (int i = 0; i < count; ++i) {
-    e = src_dtype == BBX_F32
-            ? launch_quantize_block((const float*)in[i], (uint8_t*)out[i], rows, cols, transpose, scratch + i,
-                                    scales_out + i, sms, st)
-            : launch_quantize_block((const __nv_bfloat16*)in[i], (uint8_t*)out[i], rows, cols, transpose,
-                                    scratch + i, scales_out + i, sms, st);
-    if (e != cudaSuccess) return set_error(BBX_ERR_CUDA, "no-alloc quantize launch: %s", cudaGetErrorString(e));
-  }
+  e = src_dtype == BBX_F32
+          ? launch_quantize_batch((const float* const*)in, (uint8_t* const*)out, count, rows, cols, transpose, scratch,
+                                  scales_out, sms, st)
+          : launch_quantize_batch((const __nv_bfloat16* const*)in, (uint8_t* const*)out, count, rows, cols, transpose,
+                                  scratch, scales_out, sms, st);
+  if (e != cudaSuccess) return set_error(BBX_ERR_CUDA, "no-alloc quantize launch: %s", cudaGetErrorString(e));
   e = cudaGetLastError();
   if (e != cudaSuccess) return set_error(BBX_ERR_CUDA, "no-alloc quantize launch: %s", cudaGetErrorString(e));
   return BBX_OK;

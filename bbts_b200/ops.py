@@ -209,6 +209,17 @@ def quantize_e4m3(x, out, scale_out, transpose=False):
     return out
 
 
+def quantize_e4m3_batched(xs, outs, scales_out, transpose=False):
+    """quantize_e4m3 over a list of equally shaped blocks in one call;
+    scales_out: a device tensor of len(xs) floats."""
+    rows, cols = xs[0].shape
+    arr_in = (C.c_void_p * len(xs))(*[x.data_ptr() for x in xs])
+    arr_out = (C.c_void_p * len(outs))(*[o.data_ptr() for o in outs])
+    check(lib.bbx_quantize_e4m3_batched(_dtype_code(xs[0]), arr_in, arr_out, len(xs), rows, cols, int(transpose),
+                                        _p(scales_out), _stream()))
+    return outs
+
+
 def fill_philox(out, seed, dist=0, a=0.0, b=1.0):
     check(lib.bbx_fill_philox(_dtype_code(out), _p(out), out.numel(), seed, dist, a, b, _stream()))
     return out

@@ -1027,9 +1027,8 @@ def fp8_leg(args, dev, barrier):
     sB = torch.empty(GRID, device=dev)
 
     def quantize_all():
-        for i in range(GRID):
-            ops.quantize_e4m3(A[i], qA[i], sA[i:i + 1])
-            ops.quantize_e4m3(B[i], qB[i], sB[i:i + 1], transpose=True)  # K-major B for the fp8 MMA
+        ops.quantize_e4m3_batched(A, qA, sA)
+        ops.quantize_e4m3_batched(B, qB, sB, transpose=True)  # K-major B for the fp8 MMA
 
     quantize_all()
     torch.cuda.synchronize()
@@ -1059,7 +1058,7 @@ def fp8_leg(args, dev, barrier):
                 r = a64 @ B[j].double()
                 errs.append(float((C[i * GRID + j].double() - r).abs().max() / r.abs().max()))
     plan8.close()
-    qbytes = GRID * 2 * (BS * BS * 2 + BS * BS)  # bf16 read + e4m3 written per block (absmax fused)
+    qbytes = GRID * 2 * (BS * BS * 2 + BS * BS)  # bf16 read once + e4m3 written, per block
     return {"value": round(FLOP_PER_STEP / (ms8 * 1e-3) / 1e12, 2), "unit": "TFLOP/s", "ms_per_step": round(ms8, 3),
             "quantize_ms_per_step": round(msq, 3),
             "quantize_gbs": round(qbytes / (msq * 1e-3) / 1e9, 1),

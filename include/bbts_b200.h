@@ -169,6 +169,13 @@ int bbx_relu_split(const float* z, void* hi, void* lo, long long n, void* stream
 int bbx_quantize_e4m3(int src_dtype, const void* in, void* out, int rows, int cols, int transpose,
                       float* scale_out, void* stream);
 
+/* bbx_quantize_e4m3 over `count` blocks of rows x cols (in / out HOST arrays
+ * of device pointers, scales_out a device array of `count` floats): the same
+ * bytes per block, with each pass one launch per 64 blocks. Takes a
+ * stream-ordered scratch of one word per block. */
+int bbx_quantize_e4m3_batched(int src_dtype, const void* const* in, void* const* out, int count, int rows, int cols,
+                              int transpose, float* scales_out, void* stream);
+
 /* Allocation-free batched variant of bbx_quantize_e4m3 (no counterpart in the
  * reference). For callers that must not allocate device memory while they
  * run -- code under a memory manager that owns all of the GPU, latency paths

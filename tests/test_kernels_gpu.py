@@ -521,6 +521,40 @@ def test_quantize_e4m3_paths(T, shape, dtype, transpose, offset):
     assert float(scale.cpu()[0]) == float(want_scale)
 
 
+@pytest.mark.parametrize("transpose", [False, True])
+@pytest.mark.parametrize("count,unaligned", [(5, False), (70, False), (3, True)])
+def test_quantize_e4m3_batched_matches_per_block(T, transpose, count, unaligned):
+    """The batched entry point (one launch per pass per 64 blocks; 70 blocks
+    take two) gives each block the bytes and scale of the per-block entry
+    point; a batch with an unaligned block takes the element-wise kernels."""
+    torch, ops = T
+    rng = np.random.default_rng(count + 2 * int(transpose) + 4 * int(unaligned))
+    rows, cols = 64, 96
+    xs = []
+    for i in range(count):
+        x = torch.from_numpy((rng.standard_normal((rows, cols)) * 10 ** rng.uniform(-2, 2)).astype(np.float32))
+        if unaligned and i == 1:
+            flat = torch.empty(rows * cols + 1, device="cuda")
+            d = flat[1:].view(rows, cols)
+            d.copy_(x)
+            xs.append(d)
+        else:
+            xs.append(x.cuda().to(torch.bfloat16))
+    if unaligned:  # one element type per batch
+        xs = [x.float() if x.dtype != torch.float32 else x for x in xs]
+    shape = (cols, rows) if transpose else (rows, cols)
+    outs = [torch.empty(shape, dtype=torch.float8_e4m3fn, device="cuda") for _ in range(count)]
+    scales = torch.empty(count, device="cuda")
+    ops.quantize_e4m3_batched(xs, outs, scales, transpose=transpose)
+    for i in range(count):
+        ref = torch.empty(shape, dtype=torch.float8_e4m3fn, device="cuda")
+        ref_scale = torch.empty(1, device="cuda")
+        ops.quantize_e4m3(xs[i], ref, ref_scale, transpose=transpose)
+        torch.cuda.synchronize()
+        assert torch.equal(outs[i].view(torch.uint8), ref.view(torch.uint8)), i
+        assert torch.equal(scales[i:i + 1], ref_scale), i
+
+
 # ----------------------------------------------------------------- contraction
 @pytest.mark.parametrize("precision", [0, 1])
 def test_contraction_golden(T, precision):
