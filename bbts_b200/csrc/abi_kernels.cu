@@ -516,7 +516,7 @@ int bbx_binary_f32(int op, const float* a, const float* b, float* c, long long n
 }
 
 int bbx_unary_f32(int op, const float* in, float* out, long long n, float param, void* stream) {
-  if (op < 0 || op > U_SCALE) return set_error(BBX_ERR_INVALID, "unknown unary op %d", op);
+  if (op < 0 || op > U_RELU_LO) return set_error(BBX_ERR_INVALID, "unknown unary op %d", op);
   if (n == 0) return BBX_OK;
   if (!in || !out || n < 0) return set_error(BBX_ERR_INVALID, "bad unary arguments");
   DeviceState* d;

@@ -5,7 +5,8 @@
 //   PRE     one grouped gather launch: the operand gathers of the wave's
 //           tensor-core contractions (Lc / Rc staging blocks)
 //   STREAM  grouped streaming launches: every add / n-ary reduce / elementwise
-//           node of the wave (more than 16 reduce inputs chain extra phases)
+//           node of the wave, and the split first activation as two
+//           element-wise ops (more than 16 reduce inputs chain extra phases)
 //   OTHER   direct calls of the remaining impls (FP32 SIMT matmul, FP32
 //           contraction, FNN ops, softmax, uniform)
 //   TC      one grouped tcgen05 launch per operand-layout class: the wave's
@@ -730,6 +731,23 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
           phase_rw[0].first.insert(phase_rw[0].first.end(), n.ins.begin(), n.ins.end());
           phase_rw[0].second.push_back(n.outs[0]);
         }
+      } else if (n.kind == NK_OPAQUE && !c.is_reduce() && n.impl->impl_name == "b200_dense_split_relu") {
+        // the split first activation as two element-wise ops of the wave's
+        // streaming launch: hi = bf16(relu(z)), lo = bf16(relu(z) - hi), the
+        // bytes of its impl (bbx_relu_split)
+        const auto& mz = d->tensors.at(n.ins[0]).meta.as<dense_tensor_meta_t>().m();
+        for (int j = 0; j < 2; ++j) {
+          bbx_stream_op_t s{};
+          s.kind = BBX_S_UNARY;
+          s.op = j == 0 ? BBX_U_RELU : BBX_U_RELU_LO;
+          s.in_dtype = BBX_F32; s.out_dtype = BBX_BF16; s.n_in = 1; s.kahan = 0;
+          s.n = (long long)mz.num_rows * mz.num_cols;
+          s.in[0] = d->tensors.at(n.ins[0]).payload;
+          s.out = d->tensors.at(n.outs[j]).payload;
+          phases[0].push_back(s);
+          phase_rw[0].second.push_back(n.outs[j]);
+        }
+        phase_rw[0].first.push_back(n.ins[0]);
       } else {
         opaque_t o;
         o.impl = n.impl;

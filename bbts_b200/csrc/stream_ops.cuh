@@ -25,6 +25,7 @@ enum UnaryOp : int {
   U_SQRT = 6,
   U_ADD_SCALAR = 7,  // v + param
   U_SCALE = 8,       // v * param
+  U_RELU_LO = 9,     // relu(v) - bf16(relu(v)): the low part of a split activation (exact in f32)
 };
 
 enum BinaryOp : int {
@@ -55,6 +56,10 @@ __device__ __forceinline__ float apply_unary(int op, float v, float p) {
     case U_SQRT: return sqrtf(v);
     case U_ADD_SCALAR: return __fadd_rn(v, p);
     case U_SCALE: return __fmul_rn(v, p);
+    case U_RELU_LO: {
+      const float r = v > 0.f ? v : 0.f;
+      return __fsub_rn(r, __bfloat162float(__float2bfloat16_rn(r)));
+    }
   }
   return v;
 }
@@ -87,6 +92,12 @@ __device__ __forceinline__ void with_unary(int op, float p, Body&& body) {
     case U_SQRT: body([](float v) { return sqrtf(v); }); break;
     case U_ADD_SCALAR: body([p](float v) { return __fadd_rn(v, p); }); break;
     case U_SCALE: body([p](float v) { return __fmul_rn(v, p); }); break;
+    case U_RELU_LO:
+      body([](float v) {
+        const float r = v > 0.f ? v : 0.f;
+        return __fsub_rn(r, __bfloat162float(__float2bfloat16_rn(r)));
+      });
+      break;
     default: body([](float v) { return v; }); break;
   }
 }

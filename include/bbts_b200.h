@@ -53,6 +53,10 @@ extern "C" {
 #define BBX_U_SQRT 6
 #define BBX_U_ADD_SCALAR 7
 #define BBX_U_SCALE 8
+/* relu(v) - bf16(relu(v)), exact in f32: with an f32 -> bf16 output it is the
+ * low part lo of bbx_relu_split, so a grouped launch can write hi (BBX_U_RELU
+ * to bf16) and lo as two element-wise ops */
+#define BBX_U_RELU_LO 9
 
 /* binary ops (bbx_binary_f32) */
 #define BBX_B_ADD 0         /* dense_matrix_add.cc:67-73 */
