@@ -279,15 +279,15 @@ static int build_problem(int in_dtype, const bbx_tc_problem_t& q, int bn_code, T
     return BBX_OK;
   }
   // C through TMA stores when its base, pitch and row length meet the 16-byte
-  // rules and the epilogue does not read C: 32-row boxes of 128 bytes (32 f32 /
-  // 64 bf16). A TMA store clips the box at the tensor's edge in whole 16-byte
+  // rules and the epilogue does not read C: 32-row boxes of 64 bytes (16 f32 /
+  // 32 bf16), unswizzled, two per epilogue warp in turn. A TMA store clips the box at the tensor's edge in whole 16-byte
   // pieces of a row (measured: with m = 1031 f32 rows stored column-major,
   // element 1031 of a 16-byte piece holding 1028..1031 was written), so a row
   // length that is not a multiple of 16 bytes would write into the pitch
   // padding: such C goes through the staged stores.
   if (!(out->flags & EPI_BETA) && (((uintptr_t)q.c) & 15) == 0 && ((q.ldc * c_esz) & 15) == 0 &&
       ((q.n * c_esz) & 15) == 0) {
-    rc = make_map(&out->tmap_c, q.c, c_bf16 ? BBX_BF16 : BBX_F32, q.m, q.n, q.ldc, 128 / c_esz, 32);
+    rc = make_map(&out->tmap_c, q.c, c_bf16 ? BBX_BF16 : BBX_F32, q.m, q.n, q.ldc, 64 / c_esz, 32, false);
     if (rc) return rc;
     out->flags |= EPI_TMA_STORE;
   }

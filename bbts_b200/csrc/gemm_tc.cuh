@@ -42,7 +42,8 @@ enum : int {
 struct alignas(64) TcProblem {
   CUtensorMap tmap_a;  // 128 B
   CUtensorMap tmap_b;  // 128 B
-  CUtensorMap tmap_c;  // 128 B, valid with EPI_TMA_STORE: 32-row x 128-byte boxes, 128-byte swizzle
+  CUtensorMap tmap_c;  // 128 B, valid with EPI_TMA_STORE: 32-row x 64-byte boxes (row-major C) or
+                       // 32 x 32-element boxes (column-major C), no swizzle
   void* c;
   const float* bias;
   long long ldc;       // elements
@@ -69,10 +70,10 @@ struct TcArgs {
 // is an on-chip binary search instead of a chain of dependent global loads.
 constexpr int kTcMetaMax = 512;
 constexpr int kTcMetaBytes = kTcMetaMax * 16;
-// Epilogue slots, one per epilogue warp, 1024-byte aligned: either a 32 x 36
-// float staging buffer (the 144-byte pitch keeps 16-byte accesses conflict-free
-// in both directions) or a 32-row x 128-byte box for a TMA store, laid out with
-// the 128-byte swizzle.
+// Epilogue slots, one per epilogue warp, 1024-byte aligned: a 32 x 36 float
+// staging buffer (the 144-byte pitch keeps 16-byte accesses conflict-free in
+// both directions), or two alternating 32-row x 64-byte boxes for TMA stores of
+// row-major C, or one 32 x 32-element box for column-major C.
 constexpr int kTcEpiPitch = 36;
 constexpr int kTcEpiSlot = 5120;
 constexpr int kTcEpiBytes = 4 * kTcEpiSlot;
@@ -305,20 +306,24 @@ __device__ __forceinline__ void tc_epi_rows(const TcProblem* pr, uint32_t t_row,
 }
 
 // Accumulator drain through TMA stores (problems with EPI_TMA_STORE: C's base
-// and pitch meet the 16-byte rules, no beta * C). Per 128 bytes of each of the
-// warp's 32 rows (32 f32 or 64 bf16 columns): the lane of row r loads its
-// values from TMEM, applies alpha, bias and ReLU, converts, and writes its 128
-// bytes into the warp's box with the 128-byte swizzle (16-byte chunk j of row r
-// at chunk j ^ (r & 7): conflict-free); one lane then issues the TMA store of
-// the 32 x 128-byte box, which clips rows >= m and columns >= n (the host
-// takes this path only when a row of C is a whole number of 16-byte pieces,
-// the granularity of the clip). The box is rewritten only after the previous
-// store has read it. With EPI_C_TRANS (column-major C) the box is 32 columns x
-// the warp's 32 rows, unswizzled, and m is the dimension a whole number of
-// 16-byte pieces.
+// and pitch meet the 16-byte rules, no beta * C). Row-major C: per 64 bytes of
+// each of the warp's 32 rows (16 f32 or 32 bf16 columns), the lane of row r
+// loads its values from TMEM, applies alpha, bias and ReLU, converts, and
+// writes its 64 bytes into one of the warp's two alternating 32 x 64-byte
+// boxes; one lane then issues the TMA store of the box, which clips rows >= m
+// and columns >= n (the host takes this path only when a row of C is a whole
+// number of 16-byte pieces, the granularity of the clip). A box is rewritten
+// once the store issued from it has read it (cp.async.bulk.wait_group.read 1),
+// so filling one box overlaps the store of the other; with a single box each
+// 4 KB chunk waited for the previous store, which held the 2-SM headline
+// kernel at 0.87 of the burst peak (0.92 with two boxes, same box). `box_sel`
+// (per warp, kept across tiles) names the box to fill next; 2 means the last
+// store read the whole 4 KB slot (column-major C). With EPI_C_TRANS
+// (column-major C) the box is 32 columns x the warp's 32 rows, unswizzled, and
+// m is the dimension a whole number of 16-byte pieces.
 template <int BN>
 __device__ __forceinline__ void tc_epi_rows_tma(const TcProblem* pr, uint32_t t_row, int row0, int lane,
-                                                uint8_t* box, int col_base) {
+                                                uint8_t* box, int col_base, int& box_sel) {
   const int flags = pr->flags;
   const float alpha = pr->alpha;
   const int n = pr->n;
@@ -326,9 +331,9 @@ __device__ __forceinline__ void tc_epi_rows_tma(const TcProblem* pr, uint32_t t_
   const bool relu = (flags & EPI_RELU) != 0;
   const bool bf16 = (flags & EPI_OUT_BF16) != 0;
   const int step = bf16 ? 64 : 32;  // columns per 128-byte row of the box
-  uint8_t* myrow = box + lane * 128;
   if (row0 >= pr->m) return;  // warp-uniform: this warp's rows are all past the matrix, no box to store
   if (flags & EPI_C_TRANS) {
+    box_sel = 2;  // its 4 KB box spans both 2 KB row-major boxes
     // column-major C: per 32 columns, the box holds column c's 32 rows (this
     // warp's) contiguously; lane l writes element l of every box row
 #pragma unroll 1
@@ -372,45 +377,27 @@ __device__ __forceinline__ void tc_epi_rows_tma(const TcProblem* pr, uint32_t t_
     }
     return;
   }
+  // row-major C: per 64 bytes of the warp's 32 rows (16 f32 / 32 bf16
+  // columns) each lane writes its row's 64 bytes into one of two alternating
+  // 32 x 64-byte boxes, and one lane stores the box with TMA; a box is
+  // rewritten once the store issued from it has read it (wait_group.read 1:
+  // the other box's store may still be reading)
+  (void)step;
+  const int half = bf16 ? 32 : 16;
+  if (box_sel == 2) {  // the last store read the whole 4 KB box (column-major C): let it finish
+    if (lane == 0) bulk_wait_read_all();
+    box_sel = 0;
+  }
 #pragma unroll 1
-  for (int c0 = 0; c0 < BN; c0 += step) {
+  for (int c0 = 0; c0 < BN; c0 += half) {
     const int col = col_base + c0;
     if (col >= n) break;  // warp-uniform
-    uint32_t r0[16], r1[16], r2[16], r3[16];
+    uint32_t r0[16], r1[16];
     tmem_ld16_nowait(t_row + c0, r0);
-    tmem_ld16_nowait(t_row + c0 + 16, r1);
-    if (bf16) {
-      tmem_ld16_nowait(t_row + c0 + 32, r2);
-      tmem_ld16_nowait(t_row + c0 + 48, r3);
-    }
+    if (bf16) tmem_ld16_nowait(t_row + c0 + 16, r1);
     tmem_ld_wait();
-    uint4 q[8];
+    uint4 q[4];
     if (bf16) {
-      float v[64];
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        v[i] = __uint_as_float(r0[i]) * alpha;
-        v[16 + i] = __uint_as_float(r1[i]) * alpha;
-        v[32 + i] = __uint_as_float(r2[i]) * alpha;
-        v[48 + i] = __uint_as_float(r3[i]) * alpha;
-      }
-      if (has_bias) {
-#pragma unroll
-        for (int i = 0; i < 64; ++i)
-          if (col + i < n) v[i] += pr->bias[col + i];
-      }
-      if (relu) {
-#pragma unroll
-        for (int i = 0; i < 64; ++i) v[i] = fmaxf(v[i], 0.f);
-      }
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        __nv_bfloat162 h[4];
-#pragma unroll
-        for (int t = 0; t < 4; ++t) h[t] = __floats2bfloat162_rn(v[8 * j + 2 * t], v[8 * j + 2 * t + 1]);
-        q[j] = make_uint4(*(uint32_t*)&h[0], *(uint32_t*)&h[1], *(uint32_t*)&h[2], *(uint32_t*)&h[3]);
-      }
-    } else {
       float v[32];
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
@@ -427,20 +414,42 @@ __device__ __forceinline__ void tc_epi_rows_tma(const TcProblem* pr, uint32_t t_
         for (int i = 0; i < 32; ++i) v[i] = fmaxf(v[i], 0.f);
       }
 #pragma unroll
-      for (int j = 0; j < 8; ++j)
+      for (int j = 0; j < 4; ++j) {
+        __nv_bfloat162 h[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) h[t] = __floats2bfloat162_rn(v[8 * j + 2 * t], v[8 * j + 2 * t + 1]);
+        q[j] = make_uint4(*(uint32_t*)&h[0], *(uint32_t*)&h[1], *(uint32_t*)&h[2], *(uint32_t*)&h[3]);
+      }
+    } else {
+      float v[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r0[i]) * alpha;
+      if (has_bias) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+          if (col + i < n) v[i] += pr->bias[col + i];
+      }
+      if (relu) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i], 0.f);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
         q[j] = make_uint4(__float_as_uint(v[4 * j]), __float_as_uint(v[4 * j + 1]), __float_as_uint(v[4 * j + 2]),
                           __float_as_uint(v[4 * j + 3]));
     }
-    if (lane == 0) bulk_wait_read_all();  // the previous store has read the box
+    uint8_t* hb = box + box_sel * 2048;
+    if (lane == 0) bulk_wait_read_1();
     __syncwarp();
 #pragma unroll
-    for (int j = 0; j < 8; ++j) *(uint4*)(myrow + ((j ^ (lane & 7)) << 4)) = q[j];
+    for (int j = 0; j < 4; ++j) *(uint4*)(hb + lane * 64 + j * 16) = q[j];
     fence_proxy_async_smem();
     __syncwarp();
     if (lane == 0) {
-      tma_store_2d(&pr->tmap_c, box, col, row0);
+      tma_store_2d(&pr->tmap_c, hb, col, row0);
       bulk_commit();
     }
+    box_sel ^= 1;
   }
 }
 
@@ -595,6 +604,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     int acc = 0;
     uint32_t acc_ph = 0;
     int last_p = -1;
+    int box_sel = 0;
     for (int t = blockIdx.x; t < args.total_tiles; t += gridDim.x) {
       int p, tm, tn, kdim;
       tc_locate(args, meta, t, p, tm, tn, kdim);
@@ -608,7 +618,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       if (!__all_sync(0xffffffffu, got)) break;
       tc_fence_after();
       const uint32_t t_row = tmem_base + acc * BN + ((uint32_t)lane_base << 16);
-      if (pr->flags & EPI_TMA_STORE) tc_epi_rows_tma<BN>(pr, t_row, tm * C::BM + lane_base, lane, epi_buf, tn * BN);
+      if (pr->flags & EPI_TMA_STORE) tc_epi_rows_tma<BN>(pr, t_row, tm * C::BM + lane_base, lane, epi_buf, tn * BN, box_sel);
       else tc_epi_rows<BN>(pr, t_row, tm * C::BM + lane_base, lane, epi_stage, tn * BN);
       tc_fence_before();
       mbar_arrive(&tempty_bar[acc]);
@@ -804,6 +814,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
     int acc = 0;
     uint32_t acc_ph = 0;
     int last_p = -1;
+    int box_sel = 0;
     for (int t = pair; t < args.total_tiles; t += num_pairs) {
       int p, tm, tn, kdim;
       tc_locate(args, meta, t, p, tm, tn, kdim);
@@ -817,7 +828,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
       tc_fence_after();
       const uint32_t t_row = tmem_base + acc * C::BN + ((uint32_t)lane_base << 16);
       const int row0 = tm * C::BM + (int)rank * 128 + lane_base;
-      if (pr->flags & EPI_TMA_STORE) tc_epi_rows_tma<C::BN>(pr, t_row, row0, lane, epi_buf, tn * C::BN);
+      if (pr->flags & EPI_TMA_STORE) tc_epi_rows_tma<C::BN>(pr, t_row, row0, lane, epi_buf, tn * C::BN, box_sel);
       else tc_epi_rows<C::BN>(pr, t_row, row0, lane, epi_stage, tn * C::BN);
       tc_fence_before();
       mbar_arrive_cluster(acc == 0 ? tempty_leader0 : tempty_leader1);

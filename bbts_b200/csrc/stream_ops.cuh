@@ -858,8 +858,6 @@ __device__ __forceinline__ void bulk_store(void* gdst, const void* smem_src, uin
                "r"(bytes)
                : "memory");
 }
-// at most one committed bulk-store group still reading shared memory
-__device__ __forceinline__ void bulk_wait_read_1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
 __device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kBulkConsumers) : "memory"); }
 // Barrier over the consumer threads that also ANDs their flags: every consumer
 // takes the same branch after a bounded wait, so none is left at a barrier.
