@@ -639,14 +639,15 @@ def run_dag_workload(args):
                     dag.launch()
                 tiles[nm] = _time_on(rt.stream.value, dag.launch, args.steps)
                 dag.close()
-            # the whole learned path: learned schedule, tile model, and the streaming kernel
-            # chosen per wave from the tile model's predicted tensor time
+            # the per-wave streaming-kernel choice on top (register kernel where the tile
+            # model's predicted tensor time hides the streaming work): reported beside the
+            # learned path, not part of it (measured slower than the bulk kernel throughout)
             rt.set_dag_stream_kernel(2)
             dag = rt.build_dag(runtime.LEARNED, tile_n=runtime.LEARNED_TILES)
             reg_waves = dag.register_waves()
             for _ in range(args.warmup):
                 dag.launch()
-            full_learned = _time_on(rt.stream.value, dag.launch, args.steps)
+            per_wave_ms = _time_on(rt.stream.value, dag.launch, args.steps)
             dag.close()
             rt.set_dag_stream_kernel(0)
             rt.set_tile_predictor(None)
@@ -664,7 +665,8 @@ def run_dag_workload(args):
             one_stream = float(np.median([_time_on(rt.stream.value, lambda: rt.run(runtime.HEURISTIC), 1)
                                           for _ in range(3)]))
             flops = info["flops"]
-            # the learned path: learned schedule, learned tiles, per-wave streaming kernel
+            # the learned path: learned schedule and the tile model's tiles
+            full_learned = tiles["learned"]
             value = flops / full_learned / 1e9
             r3 = lambda v: round(v, 3)
             line.update({"metric": "block-op DAG makespan, learned vs heuristic schedule", "value": round(value, 2),
@@ -681,12 +683,13 @@ def run_dag_workload(args):
                                          "per_op_1_stream_lifo": r3(one_stream),
                                          "grouped_learned_autotuned_tiles": r3(tiles["autotuned"]),
                                          "grouped_learned_learned_tiles": r3(tiles["learned"]),
-                                         "grouped_learned_tiles_per_wave_stream": r3(full_learned)},
+                                         "grouped_learned_tiles_per_wave_stream": r3(per_wave_ms)},
                          "learned_path": {"heuristic": "ASAP waves, LIFO problem order, size-rule tiles, bulk "
                                                        "streaming kernel",
-                                          "learned": "MLP wave balancing and problem order, tile model, streaming "
-                                                     "kernel per wave from the tile model's predicted tensor time",
-                                          "register_stream_waves": reg_waves,
+                                          "learned": "MLP wave balancing and problem order, tile model, bulk "
+                                                     "streaming kernel",
+                                          "per_wave_stream_ms": r3(per_wave_ms),
+                                          "per_wave_register_stream_waves": reg_waves,
                                           "makespan_gain_vs_heuristic": round(make["heuristic"] / full_learned, 4)},
                          "waves": waves,
                          "tile_model": {"samples": int(len(ty)), "holdout_mse_log_time": round(tile_mse, 4),
