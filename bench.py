@@ -40,10 +40,14 @@ CPMM_NAME = ("cpmm 32768x4096 . 4096x32768 in 4096^2 blocks (64 matrix_mult ops)
              "one grouped launch per step")
 REF_BUDGET_S = 150.0  # the reference arm's whole run (warm-up + timed steps)
 # DRAM bytes (read + write) of one full grouped launch per tile: ncu's
-# dram__bytes_read.sum + dram__bytes_write.sum of one launch of the 4x4-block
-# case (16 problems) scaled by the 64/16 problems of the full launch.
-TRAFFIC_BYTES_PER_LAUNCH = {256: 8.77e9, 512: 10.03e9}
-TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum, 2x2-block capture scaled x16"
+# dram__bytes_read.sum + dram__bytes_write.sum of one launch of a smaller grid,
+# scaled to the full launch by its problem count (traffic grows with the
+# problems: each one reads its own A and B panels). 512 (the 2-SM pair): one
+# launch of the 4x4-block case (16 problems), 2727.9 MB, x4; 256: the 2x2-block
+# case (4 problems), 548 MB, x16.
+TRAFFIC_BYTES_PER_LAUNCH = {512: 10.91e9, 256: 8.77e9}
+TRAFFIC_SOURCE = {512: "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 16-problem launch (--grid 4), x4",
+                  256: "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 4-problem launch (--grid 2), x16"}
 
 
 def parse():
@@ -852,7 +856,7 @@ def run_cpmm(args):
                 "peak_source": "%s bf16 burst (of %s): the timed region is %d graph replays, %.0f ms at the "
                                "clocks below" % (src, src, args.steps, kern_ms * args.steps),
                 "frac_of_sustained": round(achieved / (bf16_sust or bf16_peak), 4),
-                "traffic_source": TRAFFIC_SOURCE if traffic else None,
+                "traffic_source": TRAFFIC_SOURCE.get(tile) if traffic else None,
                 "algorithmic_bytes": ALG_BYTES_PER_STEP,
                 "kernel": kname, "tile": tile, "launches_timed": args.steps * launches_per_step}
 
