@@ -406,8 +406,10 @@ def test_bbts_program_cpmm(R, tmp_path):
             dag = rt.build_dag(runtime.HEURISTIC, tile_n=runtime.AUTOTUNE)
             dag.launch()
             get = lambda t: dag.read_bytes(t, bs * bs * 4).view(np.float32).reshape(bs, bs)
-        a = {key: read_dense(rt, t) for key, t in A.items()}
-        b = {key: read_dense(rt, t) for key, t in B.items()}
+        # the uniform APPLYs produce A and B: in storage per-op, inside the graph as a DAG
+        src = None if mode == "per_op" else dag
+        a = {key: read_dense(rt, t, src) for key, t in A.items()}
+        b = {key: read_dense(rt, t, src) for key, t in B.items()}
         # U(-1, 1) rounded to bf16: a value within half a bf16 step of 1 becomes 1.0
         assert a[(0, 0)].min() >= -1.0 and a[(0, 0)].max() <= 1.0 and not np.array_equal(a[(0, 0)], a[(1, 0)])
         for (i, j), t in C.items():
