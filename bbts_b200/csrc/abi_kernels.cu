@@ -57,11 +57,25 @@ struct DeviceState {
 static std::mutex g_dev_mu;
 static DeviceState g_dev[64];
 
-template <int BN, bool AMN, bool BMN, bool FP8>
+template <int BN, bool AMN, bool BMN, bool FP8, bool EP8 = false>
 static int set_tc_attr() {
-  BBX_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<BN, AMN, BMN, FP8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                TcCfg<BN, AMN, BMN, FP8>::SMEM_BYTES));
+  BBX_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<BN, AMN, BMN, FP8, EP8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                TcCfg<BN, AMN, BMN, FP8, EP8>::SMEM_BYTES));
   return BBX_OK;
+}
+
+template <bool EP8>
+static int set_tc_attrs() {
+  int rc = 0;
+  rc |= set_tc_attr<256, false, false, false, EP8>(); rc |= set_tc_attr<256, false, true, false, EP8>();
+  rc |= set_tc_attr<256, true, false, false, EP8>();  rc |= set_tc_attr<256, true, true, false, EP8>();
+  rc |= set_tc_attr<128, false, false, false, EP8>(); rc |= set_tc_attr<128, false, true, false, EP8>();
+  rc |= set_tc_attr<128, true, false, false, EP8>();  rc |= set_tc_attr<128, true, true, false, EP8>();
+  rc |= set_tc_attr<256, false, false, true, EP8>();  rc |= set_tc_attr<256, false, true, true, EP8>();
+  rc |= set_tc_attr<256, true, false, true, EP8>();   rc |= set_tc_attr<256, true, true, true, EP8>();
+  rc |= set_tc_attr<128, false, false, true, EP8>();  rc |= set_tc_attr<128, false, true, true, EP8>();
+  rc |= set_tc_attr<128, true, false, true, EP8>();   rc |= set_tc_attr<128, true, true, true, EP8>();
+  return rc;
 }
 
 template <bool AMN, bool BMN>
@@ -86,14 +100,8 @@ static int launch_tc2(bool amn, bool bmn, const TcArgs& args, int grid, cudaStre
 
 static int init_tc_attributes() {
   int rc = 0;
-  rc |= set_tc_attr<256, false, false, false>(); rc |= set_tc_attr<256, false, true, false>();
-  rc |= set_tc_attr<256, true, false, false>();  rc |= set_tc_attr<256, true, true, false>();
-  rc |= set_tc_attr<128, false, false, false>(); rc |= set_tc_attr<128, false, true, false>();
-  rc |= set_tc_attr<128, true, false, false>();  rc |= set_tc_attr<128, true, true, false>();
-  rc |= set_tc_attr<256, false, false, true>();  rc |= set_tc_attr<256, false, true, true>();
-  rc |= set_tc_attr<256, true, false, true>();   rc |= set_tc_attr<256, true, true, true>();
-  rc |= set_tc_attr<128, false, false, true>();  rc |= set_tc_attr<128, false, true, true>();
-  rc |= set_tc_attr<128, true, false, true>();   rc |= set_tc_attr<128, true, true, true>();
+  rc |= set_tc_attrs<false>();
+  rc |= set_tc_attrs<true>();
   rc |= set_tc2_attr<false, false>(); rc |= set_tc2_attr<false, true>();
   rc |= set_tc2_attr<true, false>();  rc |= set_tc2_attr<true, true>();
   for (auto f : {(const void*)k_stream_bulk<false>, (const void*)k_stream_bulk<true>,
@@ -117,7 +125,7 @@ int device_state(DeviceState** out) {
     // inside a stream capture.
     int rc = init_tc_attributes();
     if (rc) return rc;
-    d.attr_done = 0xFFFFu;
+    d.attr_done = 0xFFFFFFFFu;
     d.ready = true;
   }
   *out = &d;
@@ -180,11 +188,11 @@ static int make_map(CUtensorMap* map, const void* base, int dtype, long long row
 }
 
 // ------------------------------------------------------------------ tcgen05 dispatch
-template <int BN, bool AMN, bool BMN, bool FP8>
+template <int BN, bool AMN, bool BMN, bool FP8, bool EP8>
 static int launch_tc_variant(const TcArgs& args, int grid, cudaStream_t st, DeviceState* d,
                              int bit) {
-  using C = TcCfg<BN, AMN, BMN, FP8>;
-  auto kern = tc_gemm_kernel<BN, AMN, BMN, FP8>;
+  using C = TcCfg<BN, AMN, BMN, FP8, EP8>;
+  auto kern = tc_gemm_kernel<BN, AMN, BMN, FP8, EP8>;
   if (!(d->attr_done & (1u << bit))) {
     BBX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM_BYTES));
     d->attr_done |= (1u << bit);
@@ -194,12 +202,13 @@ static int launch_tc_variant(const TcArgs& args, int grid, cudaStream_t st, Devi
   return BBX_OK;
 }
 
-static int launch_tc(int bn, bool amn, bool bmn, bool fp8, const TcArgs& args, int grid,
+static int launch_tc(int bn, bool amn, bool bmn, bool fp8, bool ep8, const TcArgs& args, int grid,
                      cudaStream_t st, DeviceState* d) {
-  const int bit = (bn == 256 ? 8 : 0) | (amn ? 4 : 0) | (bmn ? 2 : 0) | (fp8 ? 1 : 0);
-#define TC_CASE(BN_, A_, B_, F_)                                                         \
-  if (bn == BN_ && amn == A_ && bmn == B_ && fp8 == F_)                                  \
-    return launch_tc_variant<BN_, A_, B_, F_>(args, grid, st, d, bit);
+  const int bit = (ep8 ? 16 : 0) | (bn == 256 ? 8 : 0) | (amn ? 4 : 0) | (bmn ? 2 : 0) | (fp8 ? 1 : 0);
+#define TC_CASE(BN_, A_, B_, F_)                                                                   \
+  if (bn == BN_ && amn == A_ && bmn == B_ && fp8 == F_)                                            \
+    return ep8 ? launch_tc_variant<BN_, A_, B_, F_, true>(args, grid, st, d, bit)                  \
+               : launch_tc_variant<BN_, A_, B_, F_, false>(args, grid, st, d, bit);
   TC_CASE(256, false, false, false) TC_CASE(256, false, true, false)
   TC_CASE(256, true, false, false) TC_CASE(256, true, true, false)
   TC_CASE(128, false, false, false) TC_CASE(128, false, true, false)
@@ -329,6 +338,7 @@ using namespace bbx;
 struct bbx_tc_plan {
   int dtype = BBX_BF16;
   int bn = 256;
+  bool ep8 = false;  // 1-SM tiles: eight epilogue warps (every problem's K <= kTcEp8MaxK)
   bool amn = false, bmn = true;
   int count = 0;
   int total_tiles = 0;
@@ -437,6 +447,9 @@ int bbx_tc_plan_create(int in_dtype, const bbx_tc_problem_t* problems, int count
     tiles += p->host[i].tiles_m * p->host[i].tiles_n;
   }
   p->total_tiles = tiles;
+  int max_k = 0;
+  for (int i = 0; i < count; ++i) max_k = std::max(max_k, problems[i].k);
+  p->ep8 = tile_n != 512 && max_k <= kTcEp8MaxK;
   if (count > kTcMaxInline) {
     cudaError_t e = cudaMalloc(&p->d_table, sizeof(TcProblem) * count);
     if (e != cudaSuccess) { delete p; return set_error(BBX_ERR_CUDA, "cudaMalloc(plan table): %s", cudaGetErrorString(e)); }
@@ -466,7 +479,7 @@ int bbx_tc_plan_launch(bbx_tc_plan_t* p, void* stream) {
     return launch_tc2(p->amn, p->bmn, args, grid, (cudaStream_t)stream);
   }
   const int grid = std::min(p->total_tiles, d->sms);
-  return launch_tc(p->bn, p->amn, p->bmn, p->dtype == BBX_E4M3, args, grid,
+  return launch_tc(p->bn, p->amn, p->bmn, p->dtype == BBX_E4M3, p->ep8, args, grid,
                    (cudaStream_t)stream, d);
 }
 

@@ -14,10 +14,11 @@
 // dimension is contiguous ("MN-major") are both read directly by TMA with the
 // 128-byte swizzle; no transpose pass is needed.
 //
-// Roles inside a 192-thread CTA:
+// Roles inside a 192-thread CTA (320 with EP8):
 //   warp 0      TMA producer (one elected lane) feeding a STAGES-deep smem ring
 //   warp 1      TMEM allocator + MMA issuer (one elected lane)
-//   warps 2..5  epilogue: tcgen05.ld from TMEM -> registers -> global
+//   warps 2..5  epilogue: tcgen05.ld from TMEM -> registers -> global (2..9 with
+//               EP8: two warps per TMEM lane quarter, half the columns each)
 // The accumulator is double buffered in TMEM (2 x BN f32 columns), so the
 // epilogue of tile t overlaps the main loop of tile t+1.
 #pragma once
@@ -79,7 +80,15 @@ constexpr int kTcEpiSlot = 5120;
 constexpr int kTcEpiBytes = 4 * kTcEpiSlot;
 static_assert(32 * kTcEpiPitch * 4 <= kTcEpiSlot && 32 * 128 <= kTcEpiSlot && kTcEpiSlot % 1024 == 0, "epilogue slot");
 
-template <int BN, bool A_MN, bool B_MN, bool FP8>
+// EP8: eight epilogue warps (two per TMEM lane quarter, each draining half of
+// the tile's columns) and one shared-memory stage fewer. For groups of short
+// main loops (K <= kTcEp8MaxK) the tile rate is set by the epilogue: measured
+// on the contraction-only DAG, 4.08 -> 3.46 ms for its tensor groups; with
+// long K the missing stage costs more than the extra warps give (the FP8 4096^3
+// blocks: 2609 -> 2453 TFLOP/s), so the host picks it only for short K.
+constexpr int kTcEp8MaxK = 512;
+
+template <int BN, bool A_MN, bool B_MN, bool FP8, bool EP8 = false>
 struct TcCfg {
   static constexpr int BM = 128;
   static constexpr int BK_BYTES = 128;                // one 128-byte swizzle row of K
@@ -89,11 +98,13 @@ struct TcCfg {
   static constexpr int A_BYTES = BM * BK_BYTES;       // 16 KiB
   static constexpr int B_BYTES = BN * BK_BYTES;       // 32 or 16 KiB
   static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-  static constexpr int STAGES = (BN == 256) ? 4 : 6;
+  static constexpr int STAGES = EP8 ? ((BN == 256) ? 3 : 5) : ((BN == 256) ? 4 : 6);
   static constexpr int TMEM_COLS = 2 * BN;            // double-buffered accumulator
+  static constexpr int EPI_WARPS = EP8 ? 8 : 4;
+  static constexpr int EPI_COLS = EP8 ? BN / 2 : BN;  // accumulator columns one epilogue warp drains
   static constexpr int SMEM_BYTES =
-      STAGES * STAGE_BYTES + 1024 /*align slack*/ + kTcEpiBytes + 256 /*bars*/ + kTcMetaBytes;
-  static constexpr int THREADS = 192;
+      STAGES * STAGE_BYTES + 1024 /*align slack*/ + EPI_WARPS * kTcEpiSlot + 256 /*bars*/ + kTcMetaBytes;
+  static constexpr int THREADS = 64 + 32 * EPI_WARPS;
   static constexpr int MN_BOX = 128 / ELEM;           // MN-major TMA box width (elements)
 };
 
@@ -111,8 +122,10 @@ __device__ __forceinline__ void tc_stage_meta(const TcArgs& args, int4* meta) {
 }
 
 // Map a global tile index to (problem, tile_m, tile_n) and the problem's k.
-// Tiles inside a problem are visited in groups of 8 tile-rows so concurrently
-// running CTAs share operand tiles in L2.
+// Tiles inside a problem are visited in bands of 16 tile-rows so concurrently
+// running CTAs share operand tiles in L2: a 4096^2 block's B panels are then
+// read from DRAM once per problem (with bands of 8, twice; the pair kernel ran
+// 1358 -> 1440 TFLOP/s on the 64 x 4096^3 step, same box and clock).
 __device__ __forceinline__ void tc_locate(const TcArgs& args, const int4* meta, int t, int& p, int& tm, int& tn,
                                           int& k) {
   int lo = 0, hi = args.num_problems - 1;
@@ -134,7 +147,7 @@ __device__ __forceinline__ void tc_locate(const TcArgs& args, const int4* meta, 
   p = lo;
   k = e.w;
   const int lt = t - e.x;
-  constexpr int G = 8;
+  constexpr int G = 16;
   const int per_group = G * e.z;
   const int group = lt / per_group;
   const int first_m = group * G;
@@ -453,15 +466,15 @@ __device__ __forceinline__ void tc_epi_rows_tma(const TcProblem* pr, uint32_t t_
   }
 }
 
-template <int BN, bool A_MN, bool B_MN, bool FP8>
-__global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__ TcArgs args) {
-  using C = TcCfg<BN, A_MN, B_MN, FP8>;
+template <int BN, bool A_MN, bool B_MN, bool FP8, bool EP8>
+__global__ void __launch_bounds__(EP8 ? 320 : 192, 1) tc_gemm_kernel(const __grid_constant__ TcArgs args) {
+  using C = TcCfg<BN, A_MN, B_MN, FP8, EP8>;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   // 1024-byte alignment for the 128B-swizzle atoms.
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t* stage_base = smem;
   uint8_t* epi_base = smem + C::STAGES * C::STAGE_BYTES;  // 4 epilogue slots, 1024-byte aligned
-  uint64_t* bars = (uint64_t*)(epi_base + kTcEpiBytes);
+  uint64_t* bars = (uint64_t*)(epi_base + C::EPI_WARPS * kTcEpiSlot);
   uint64_t* full_bar = bars;                       // [STAGES]
   uint64_t* empty_bar = bars + C::STAGES;          // [STAGES]
   uint64_t* tfull_bar = bars + 2 * C::STAGES;      // [2]
@@ -483,7 +496,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&tfull_bar[b], 1);
-      mbar_init(&tempty_bar[b], 128);
+      mbar_init(&tempty_bar[b], 32 * C::EPI_WARPS);
     }
     fence_mbar_init();
   }
@@ -617,9 +630,12 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       const bool got = mbar_wait(&tfull_bar[acc], acc_ph, status, DEV_TIMEOUT_TMEM_FULL);
       if (!__all_sync(0xffffffffu, got)) break;
       tc_fence_after();
-      const uint32_t t_row = tmem_base + acc * BN + ((uint32_t)lane_base << 16);
-      if (pr->flags & EPI_TMA_STORE) tc_epi_rows_tma<BN>(pr, t_row, tm * C::BM + lane_base, lane, epi_buf, tn * BN, box_sel);
-      else tc_epi_rows<BN>(pr, t_row, tm * C::BM + lane_base, lane, epi_stage, tn * BN);
+      // with EP8 warps 2..5 and 6..9 drain the left and right halves of the columns
+      const int col0 = EP8 ? ((warp - 2) >> 2) * C::EPI_COLS : 0;
+      const uint32_t t_row = tmem_base + acc * BN + col0 + ((uint32_t)lane_base << 16);
+      if (pr->flags & EPI_TMA_STORE)
+        tc_epi_rows_tma<C::EPI_COLS>(pr, t_row, tm * C::BM + lane_base, lane, epi_buf, tn * BN + col0, box_sel);
+      else tc_epi_rows<C::EPI_COLS>(pr, t_row, tm * C::BM + lane_base, lane, epi_stage, tn * BN + col0);
       tc_fence_before();
       mbar_arrive(&tempty_bar[acc]);
       if (++acc == 2) { acc = 0; acc_ph ^= 1; }

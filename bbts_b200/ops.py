@@ -62,6 +62,11 @@ def matmul_tc(problems, in_dtype=BF16, tile_n=0):
     check(lib.bbx_matmul_tc(in_dtype, arr, len(problems), tile_n, _stream()))
 
 
+# Groups whose largest K is at most this run the 1-SM kernel with eight epilogue warps
+# (the variant the plan picks; `kTcEp8MaxK` in csrc/gemm_tc.cuh).
+TC_EP8_MAX_K = 512
+
+
 class TcPlan:
     """A prepared grouped tensor-core matmul (tensor maps built once)."""
 
@@ -70,6 +75,7 @@ class TcPlan:
         self.h = C.c_void_p()
         self.in_dtype = in_dtype
         self.trans = (bool(problems[0].trans_a), bool(problems[0].trans_b))
+        self.max_k = max(int(p.k) for p in problems)
         check(lib.bbx_tc_plan_create(in_dtype, arr, len(problems), tile_n, C.byref(self.h)))
 
     def launch(self, stream=None):
@@ -87,7 +93,8 @@ class TcPlan:
         b = "K-major B" if self.trans[1] else "MN-major B"
         if tn == 512:
             return "tc_gemm2_kernel<%s,%s> (2-SM 256x256 pair, cta_group::2)" % (a, b)
-        return "tc_gemm_kernel<%d,%s,%s,%s>" % (tn, a, b, "e4m3" if self.in_dtype == E4M3 else "bf16")
+        epi = "8 epilogue warps" if self.max_k <= TC_EP8_MAX_K else "4 epilogue warps"
+        return "tc_gemm_kernel<%d,%s,%s,%s,%s>" % (tn, a, b, "e4m3" if self.in_dtype == E4M3 else "bf16", epi)
 
     def close(self):
         if self.h:
