@@ -80,8 +80,8 @@ constexpr int kTcEpiSlot = 5120;
 constexpr int kTcEpiBytes = 4 * kTcEpiSlot;
 static_assert(32 * kTcEpiPitch * 4 <= kTcEpiSlot && 32 * 128 <= kTcEpiSlot && kTcEpiSlot % 1024 == 0, "epilogue slot");
 
-// EP8: eight epilogue warps (two per TMEM lane quarter, each draining half of
-// the tile's columns) and one shared-memory stage fewer. For groups of short
+// EP8: eight epilogue warps (two per TMEM lane quarter, taking alternate
+// column chunks of the tile) and one shared-memory stage fewer. For groups of short
 // main loops (K <= kTcEp8MaxK) the tile rate is set by the epilogue: measured
 // on the contraction-only DAG, 4.08 -> 3.46 ms for its tensor groups; with
 // long K the missing stage costs more than the extra warps give (the FP8 4096^3
@@ -101,7 +101,7 @@ struct TcCfg {
   static constexpr int STAGES = EP8 ? ((BN == 256) ? 3 : 5) : ((BN == 256) ? 4 : 6);
   static constexpr int TMEM_COLS = 2 * BN;            // double-buffered accumulator
   static constexpr int EPI_WARPS = EP8 ? 8 : 4;
-  static constexpr int EPI_COLS = EP8 ? BN / 2 : BN;  // accumulator columns one epilogue warp drains
+  static constexpr int EPI_PARTS = EP8 ? 2 : 1;       // epilogue warps per TMEM lane quarter
   static constexpr int SMEM_BYTES =
       STAGES * STAGE_BYTES + 1024 /*align slack*/ + EPI_WARPS * kTcEpiSlot + 256 /*bars*/ + kTcMetaBytes;
   static constexpr int THREADS = 64 + 32 * EPI_WARPS;
@@ -168,9 +168,9 @@ __device__ __forceinline__ void tc_locate(const TcArgs& args, const int4* meta, 
 // half-sector writes per instruction); these write whole sectors. Warp-
 // collective: every lane runs it; rows at or past m and columns at or past n
 // are not written.
-template <int BN>
+template <int BN, int PARTS = 1>
 __device__ __forceinline__ void tc_epi_rows(const TcProblem* pr, uint32_t t_row, int row0, int lane, float* stage,
-                                            int col_base) {
+                                            int col_base, int part = 0) {
   const int flags = pr->flags;
   const float alpha = pr->alpha, beta = pr->beta;
   const long long ldc = pr->ldc;
@@ -184,7 +184,7 @@ __device__ __forceinline__ void tc_epi_rows(const TcProblem* pr, uint32_t t_row,
     const bool bf16 = (flags & EPI_OUT_BF16) != 0;
     const int row = row0 + lane;
 #pragma unroll 1
-    for (int c0 = 0; c0 < BN; c0 += 32) {
+    for (int c0 = 32 * part; c0 < BN; c0 += 32 * PARTS) {
       const int col = col_base + c0;
       if (col >= n || row0 >= m) break;  // warp-uniform
       uint32_t r0[16], r1[16];
@@ -224,7 +224,7 @@ __device__ __forceinline__ void tc_epi_rows(const TcProblem* pr, uint32_t t_row,
   if (lane == 0) bulk_wait_read_all();
   __syncwarp();
 #pragma unroll 1
-  for (int c = 0; c < BN / 16; c += 2) {
+  for (int c = 2 * part; c < BN / 16; c += 2 * PARTS) {
     const int col0 = col_base + c * 16;
     if (col0 >= n) break;  // warp-uniform
     uint32_t r0[16], r1[16];
@@ -334,9 +334,9 @@ __device__ __forceinline__ void tc_epi_rows(const TcProblem* pr, uint32_t t_row,
 // store read the whole 4 KB slot (column-major C). With EPI_C_TRANS
 // (column-major C) the box is 32 columns x the warp's 32 rows, unswizzled, and
 // m is the dimension a whole number of 16-byte pieces.
-template <int BN>
+template <int BN, int PARTS = 1>
 __device__ __forceinline__ void tc_epi_rows_tma(const TcProblem* pr, uint32_t t_row, int row0, int lane,
-                                                uint8_t* box, int col_base, int& box_sel) {
+                                                uint8_t* box, int col_base, int& box_sel, int part = 0) {
   const int flags = pr->flags;
   const float alpha = pr->alpha;
   const int n = pr->n;
@@ -350,7 +350,7 @@ __device__ __forceinline__ void tc_epi_rows_tma(const TcProblem* pr, uint32_t t_
     // column-major C: per 32 columns, the box holds column c's 32 rows (this
     // warp's) contiguously; lane l writes element l of every box row
 #pragma unroll 1
-    for (int c0 = 0; c0 < BN; c0 += 32) {
+    for (int c0 = 32 * part; c0 < BN; c0 += 32 * PARTS) {
       const int col = col_base + c0;
       if (col >= n) break;  // warp-uniform
       uint32_t r0[16], r1[16];
@@ -402,7 +402,7 @@ __device__ __forceinline__ void tc_epi_rows_tma(const TcProblem* pr, uint32_t t_
     box_sel = 0;
   }
 #pragma unroll 1
-  for (int c0 = 0; c0 < BN; c0 += half) {
+  for (int c0 = half * part; c0 < BN; c0 += half * PARTS) {
     const int col = col_base + c0;
     if (col >= n) break;  // warp-uniform
     uint32_t r0[16], r1[16];
@@ -630,12 +630,13 @@ __global__ void __launch_bounds__(EP8 ? 320 : 192, 1) tc_gemm_kernel(const __gri
       const bool got = mbar_wait(&tfull_bar[acc], acc_ph, status, DEV_TIMEOUT_TMEM_FULL);
       if (!__all_sync(0xffffffffu, got)) break;
       tc_fence_after();
-      // with EP8 warps 2..5 and 6..9 drain the left and right halves of the columns
-      const int col0 = EP8 ? ((warp - 2) >> 2) * C::EPI_COLS : 0;
-      const uint32_t t_row = tmem_base + acc * BN + col0 + ((uint32_t)lane_base << 16);
+      // with EP8 warps 2..5 and 6..9 take alternate column chunks of the tile (even
+      // and odd), so a problem whose n ends inside the tile splits its chunks evenly
+      const int part = EP8 ? (warp - 2) >> 2 : 0;
+      const uint32_t t_row = tmem_base + acc * BN + ((uint32_t)lane_base << 16);
       if (pr->flags & EPI_TMA_STORE)
-        tc_epi_rows_tma<C::EPI_COLS>(pr, t_row, tm * C::BM + lane_base, lane, epi_buf, tn * BN + col0, box_sel);
-      else tc_epi_rows<C::EPI_COLS>(pr, t_row, tm * C::BM + lane_base, lane, epi_stage, tn * BN + col0);
+        tc_epi_rows_tma<BN, C::EPI_PARTS>(pr, t_row, tm * C::BM + lane_base, lane, epi_buf, tn * BN, box_sel, part);
+      else tc_epi_rows<BN, C::EPI_PARTS>(pr, t_row, tm * C::BM + lane_base, lane, epi_stage, tn * BN, part);
       tc_fence_before();
       mbar_arrive(&tempty_bar[acc]);
       if (++acc == 2) { acc = 0; acc_ph ^= 1; }
