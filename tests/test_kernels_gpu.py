@@ -803,3 +803,65 @@ def test_matmul_tc_padded_pitch_untouched(T):
     cf = torch.empty(40, 77, device="cuda")
     with pytest.raises(BbxError, match="beta"):
         ops.matmul_tc([ops.tc_problem(A, B, cf, beta=1.0, c_colmajor=True)])
+
+
+@pytest.mark.parametrize("tile_n", [128, 256])
+@pytest.mark.parametrize("kmax", [192, 1024])
+def test_matmul_tc_colmajor_mixed_group(T, tile_n, kmax):
+    """One grouped launch mixing column-major C whose m is a whole number of
+    16-byte pieces (TMA boxes), column-major C of any m and any element-aligned
+    base (the 1-SM kernel's cooperative 128-row column runs) and row-major C,
+    with bias / relu and f32 or bf16 outputs. Integer-valued inputs make every
+    product exact: each C equals its int64 product and nothing around it
+    changes. kmax 192 runs the eight-epilogue-warp kernel, 1024 the four-warp
+    one."""
+    torch, ops = T
+    rng = np.random.default_rng(71 + tile_n + kmax)
+    probs, checks, keep = [], [], []
+    for i in range(48):
+        kind = i % 4  # 0 column-major TMA, 1 column-major ragged m, 2 column-major offset base, 3 row-major
+        odt = torch.bfloat16 if (i // 4) % 2 else torch.float32
+        q = 8 if odt == torch.bfloat16 else 4  # elements per 16-byte piece
+        m = int(rng.integers(1, 48)) * q if kind == 0 else int(rng.integers(1, 700))
+        if kind == 1 and m % q == 0:
+            m += 1
+        n = int(rng.integers(1, 300))
+        k = kmax if i == 0 else int(rng.choice([32, 64, 96, 160, kmax]))
+        a = rng.integers(-3, 4, (m, k)).astype(np.float32)
+        b = rng.integers(-3, 4, (k, n)).astype(np.float32)
+        bias = rng.integers(-8, 9, n).astype(np.float32) if i % 3 == 0 else None
+        relu = i % 5 == 1
+        A = dev(torch, a, torch.bfloat16)
+        B = torch.zeros(k, (n + 7) // 8 * 8, dtype=torch.bfloat16, device="cuda")  # pitch: 16-byte multiple
+        B[:, :n] = dev(torch, b, torch.bfloat16)
+        B = B[:, :n]
+        bt = dev(torch, bias) if bias is not None else None
+        off = int(rng.integers(1, q)) if kind == 2 else 0
+        if kind == 3:
+            ld = n + int(rng.integers(0, 9))
+            flat = torch.full((off + m * ld + 5,), float("nan"), dtype=odt, device="cuda")
+            c = flat[off:off + m * ld].view(m, ld)[:, :n]
+        else:
+            ld = m + (int(rng.integers(0, 3)) * q if kind == 0 else int(rng.integers(0, 9)))
+            flat = torch.full((off + n * ld + 5,), float("nan"), dtype=odt, device="cuda")
+            c = flat[off:off + n * ld].view(n, ld)[:, :m]
+        probs.append(ops.tc_problem(A, B, c, bias=bt, relu=relu, c_colmajor=kind != 3))
+        r = a.astype(np.int64) @ b.astype(np.int64)
+        if bias is not None:
+            r = r + bias.astype(np.int64)[None, :]
+        if relu:
+            r = np.maximum(r, 0)
+        want = bf16_round(r.astype(np.float32)) if odt == torch.bfloat16 else r.astype(np.float64)
+        keep += [A, B, bt, flat, c]
+        checks.append((flat, off, ld, m, n, kind, want))
+    plan = ops.TcPlan(probs, tile_n=tile_n)
+    for _ in range(2):
+        plan.launch()
+        for i, (flat, off, ld, m, n, kind, want) in enumerate(checks):
+            got = host(flat)
+            rows, cols = (m, n) if kind == 3 else (n, m)
+            body = got[off:off + rows * ld].reshape(rows, ld)
+            assert np.array_equal(body[:, :cols], want if kind == 3 else want.T), (i, kind, m, n, off)
+            assert np.all(np.isnan(body[:, cols:])) and np.all(np.isnan(got[:off])), (i, kind, m, n, off)
+            assert np.all(np.isnan(got[off + rows * ld:])), (i, kind, m, n, off)
+    plan.close()
