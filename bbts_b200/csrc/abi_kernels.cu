@@ -106,7 +106,7 @@ static int init_tc_attributes() {
   rc |= set_tc2_attr<true, false>();  rc |= set_tc2_attr<true, true>();
   for (auto f : {(const void*)k_stream_bulk<false>, (const void*)k_stream_bulk<true>,
                  (const void*)k_stream_bulk_inline<false>, (const void*)k_stream_bulk_inline<true>})
-    rc |= cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kBulkSmem) != cudaSuccess;
+    rc |= cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kBulkSmemMax) != cudaSuccess;
   return rc ? BBX_ERR_CUDA : BBX_OK;
 }
 
@@ -865,7 +865,7 @@ int bbx_stream_plan_launch(bbx_stream_plan_t* p, void* stream) {
   if (rc) return rc;
   if (p->bulk) {
     const long long grid = std::min<long long>(p->total_chunks, (long long)d->sms);
-    k_stream_bulk<kBulkStoreTS><<<(int)grid, kBulkThreads, kBulkSmem, (cudaStream_t)stream>>>(
+    k_stream_bulk<kBulkStoreTS><<<(int)grid, kBulkThreads, bulk_smem_bytes(p->count), (cudaStream_t)stream>>>(
         p->d_table, p->count, p->total_chunks, d->status, kBulkPiece);
     BBX_CHECK_LAUNCH("k_stream_bulk");
     return BBX_OK;
@@ -907,7 +907,7 @@ int bbx_stream_group(const bbx_stream_op_t* ops, int count, void* stream) {
     for (int j = 0; j < c; ++j) args.ops[j] = table[j];
     if (bulk) {
       const long long grid = std::min<long long>(total, (long long)d->sms);
-      k_stream_bulk_inline<kBulkStoreTS><<<(int)grid, kBulkThreads, kBulkSmem, (cudaStream_t)stream>>>(
+      k_stream_bulk_inline<kBulkStoreTS><<<(int)grid, kBulkThreads, bulk_smem_bytes(c), (cudaStream_t)stream>>>(
           args, c, total, d->status, kBulkPiece);
       BBX_CHECK_LAUNCH("k_stream_bulk_inline");
       continue;

@@ -744,7 +744,22 @@ constexpr int kBulkSlot = 65536;     // bytes per stage: input tiles + output ti
 constexpr int kBulkConsumerWarps = 8;
 constexpr int kBulkConsumers = kBulkConsumerWarps * 32;
 constexpr int kBulkThreads = kBulkConsumers + 32;
-constexpr int kBulkSmem = kBulkStages * kBulkSlot + kBulkStages * 16 + kBulkStages * 4;
+// Shared memory after the stages: the full / empty barriers, each stage's op
+// descriptor (a copy of its StreamOp, which the consumers read instead of the
+// table in global memory) and, for plans of at most kBulkMaxStagedOps ops,
+// every op's chunk_start, where the producer finds the op of an item. The
+// binary search through the global table this replaces was a chain of
+// dependent L2 reads per item, with the table evicted from L1 by the stages:
+// measured on 2000-op random DAGs' streaming levels, adds 5.33 -> 6.49 TB/s,
+// 2-16-input reduces 4.90 -> 5.73 TB/s.
+constexpr int kBulkDescBytes = (int)sizeof(StreamOp);
+static_assert(kBulkDescBytes % 16 == 0, "stage descriptors are copied in 16-byte pieces");
+constexpr int kBulkSmem = kBulkStages * kBulkSlot + kBulkStages * 16 + kBulkStages * kBulkDescBytes;
+constexpr int kBulkMaxStagedOps = 4096;
+constexpr int kBulkSmemMax = kBulkSmem + 8 * kBulkMaxStagedOps;
+__host__ __device__ inline int bulk_smem_bytes(int count) {
+  return kBulkSmem + (count <= kBulkMaxStagedOps ? 8 * count : 0);
+}
 constexpr bool kBulkStoreTS = false;   // output tiles by consumer stores (see stream_bulk_body)
 constexpr uint32_t kBulkPiece = 65536;  // bytes per bulk load (one copy per input tile: splitting measured slower)
 
@@ -884,7 +899,9 @@ __device__ __forceinline__ void stream_bulk_body(const TableT* table, int count,
   extern __shared__ __align__(128) uint8_t bulk_smem[];
   uint64_t* full = (uint64_t*)(bulk_smem + kBulkStages * kBulkSlot);
   uint64_t* empty = full + kBulkStages;
-  int* stage_op = (int*)(empty + kBulkStages);
+  StreamOp* desc = (StreamOp*)(empty + kBulkStages);       // [kBulkStages]: the op of the stage's item
+  long long* starts = (long long*)(desc + kBulkStages);    // [count] when staged: every op's chunk_start
+  const bool staged = count <= kBulkMaxStagedOps;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < kBulkStages; ++s) {
@@ -893,10 +910,18 @@ __device__ __forceinline__ void stream_bulk_body(const TableT* table, int count,
     }
     fence_mbar_init();
   }
+  if (staged)
+    for (int i = threadIdx.x; i < count; i += blockDim.x) starts[i] = table[i].chunk_start;
   __syncthreads();
   volatile uint32_t* st = status;
   if (warp == kBulkConsumerWarps) {
-    // producer warp: lane 0 owns the barriers, lane j issues input j's copies
+    // producer warp: lane 0 owns the barriers and the stage descriptors, lane j
+    // issues input j's copies. A CTA's items come in increasing order, so the
+    // op index only moves forward; lane 0 keeps the current op in registers and
+    // reads the table only when the op changes.
+    constexpr int kDescPieces = kBulkDescBytes / 16;
+    uint4 cur[kDescPieces];
+    int oi = -1;
     int k = 0;
     for (long long it = blockIdx.x; it < total_items; it += gridDim.x, ++k) {
       const int s = k % kBulkStages;
@@ -904,15 +929,40 @@ __device__ __forceinline__ void stream_bulk_body(const TableT* table, int count,
       bool ok = true;
       if (lane == 0) ok = mbar_wait(&empty[s], ph ^ 1u, st, DEV_TIMEOUT_EMPTY);
       if (!__shfl_sync(0xffffffffu, ok, 0)) break;
-      const int oi = stream_find_op(table, count, it);
-      const auto& o = table[oi];
+      int noi;
+      if (!staged) {
+        noi = stream_find_op(table, count, it);
+      } else if (oi < 0) {
+        int lo = 0, hi = count - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (starts[mid] <= it) lo = mid; else hi = mid - 1;
+        }
+        noi = lo;
+      } else {
+        noi = oi;
+        while (noi + 1 < count && starts[noi + 1] <= it) ++noi;
+      }
+      if (lane == 0) {
+        if (noi != oi) {
+          const uint4* src = (const uint4*)&table[noi];
+#pragma unroll
+          for (int q = 0; q < kDescPieces; ++q) cur[q] = src[q];
+        }
+        uint4* dst = (uint4*)&desc[s];
+#pragma unroll
+        for (int q = 0; q < kDescPieces; ++q) dst[q] = cur[q];
+      }
+      oi = noi;
+      __syncwarp();
+      const StreamOp& o = desc[s];
       const int esz = o.in_dtype == 1 ? 2 : 4;
       const long long e0 = (it - o.chunk_start) * (long long)o.tile;
       const long long e1 = min(e0 + (long long)o.tile, o.n);
       const uint32_t nb = (uint32_t)((e1 - e0) & ~7LL) * esz;  // a multiple of 8 elements: 16-byte multiples
       uint8_t* slot = bulk_smem + s * kBulkSlot;
       if (lane == 0) {
-        stage_op[s] = oi;  // published by the arrive below (release)
+        // the descriptor is published by this arrive (release)
         if (nb) mbar_arrive_expect_tx(&full[s], nb * (uint32_t)o.n_in);
         else mbar_arrive(&full[s]);
       }
@@ -938,7 +988,7 @@ __device__ __forceinline__ void stream_bulk_body(const TableT* table, int count,
     const int s = k % kBulkStages;
     const uint32_t ph = (uint32_t)(k / kBulkStages) & 1u;
     if (!consumers_all(mbar_wait(&full[s], ph, st, DEV_TIMEOUT_FULL))) break;
-    const auto& o = table[stage_op[s]];
+    const StreamOp& o = desc[s];
     const int esz = o.in_dtype == 1 ? 2 : 4, osz = o.out_dtype == 1 ? 2 : 4;
     const long long e0 = (it - o.chunk_start) * (long long)o.tile;
     const long long e1 = min(e0 + (long long)o.tile, o.n);
