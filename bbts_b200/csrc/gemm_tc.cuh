@@ -466,6 +466,17 @@ __device__ __forceinline__ void tc_epi_rows_tma(const TcProblem* pr, uint32_t t_
   }
 }
 
+// Tile of CTA blockIdx.x in round `round` (t0 = round * grid + blockIdx.x):
+// snake order, so in odd rounds CTA b takes the round's tile grid - 1 - b and a
+// CTA that drew a costly tile early in the list draws a cheap one next (the
+// plan sorts problems by descending tile cost). A partial last round keeps the
+// plain order. The producer, MMA and epilogue warps all walk this sequence.
+__device__ __forceinline__ int snake_tile(int t0, int round, int total) {
+  const int base = t0 - (int)blockIdx.x;
+  if ((round & 1) && base + (int)gridDim.x <= total) return base + (int)gridDim.x - 1 - (int)blockIdx.x;
+  return t0;
+}
+
 template <int BN, bool A_MN, bool B_MN, bool FP8, bool EP8>
 __global__ void __launch_bounds__(EP8 ? 320 : 192, 1) tc_gemm_kernel(const __grid_constant__ TcArgs args) {
   using C = TcCfg<BN, A_MN, B_MN, FP8, EP8>;
@@ -514,7 +525,8 @@ __global__ void __launch_bounds__(EP8 ? 320 : 192, 1) tc_gemm_kernel(const __gri
       uint32_t ph = 0;
       bool ok = true;
       int last_p = -1;
-      for (int t = blockIdx.x; t < args.total_tiles && ok; t += gridDim.x) {
+      for (int t0 = blockIdx.x, rr = 0; t0 < args.total_tiles && ok; t0 += gridDim.x, ++rr) {
+        const int t = snake_tile(t0, rr, args.total_tiles);
         int p, tm, tn, kdim;
         tc_locate(args, meta, t, p, tm, tn, kdim);
         const TcProblem* pr = tc_problem(args, p);
@@ -580,7 +592,8 @@ __global__ void __launch_bounds__(EP8 ? 320 : 192, 1) tc_gemm_kernel(const __gri
       int acc = 0;
       uint32_t acc_ph = 0;
       bool ok = true;
-      for (int t = blockIdx.x; t < args.total_tiles && ok; t += gridDim.x) {
+      for (int t0 = blockIdx.x, rr = 0; t0 < args.total_tiles && ok; t0 += gridDim.x, ++rr) {
+        const int t = snake_tile(t0, rr, args.total_tiles);
         int p, tm, tn, kdim;
         tc_locate(args, meta, t, p, tm, tn, kdim);
         const int kb_n = (kdim + C::BK - 1) / C::BK;
@@ -618,7 +631,8 @@ __global__ void __launch_bounds__(EP8 ? 320 : 192, 1) tc_gemm_kernel(const __gri
     uint32_t acc_ph = 0;
     int last_p = -1;
     int box_sel = 0;
-    for (int t = blockIdx.x; t < args.total_tiles; t += gridDim.x) {
+    for (int t0 = blockIdx.x, rr = 0; t0 < args.total_tiles; t0 += gridDim.x, ++rr) {
+      const int t = snake_tile(t0, rr, args.total_tiles);
       int p, tm, tn, kdim;
       tc_locate(args, meta, t, p, tm, tn, kdim);
       const TcProblem* pr = tc_problem(args, p);
