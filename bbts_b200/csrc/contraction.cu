@@ -195,12 +195,20 @@ __global__ void k_gather_rows1(const __grid_constant__ GatherRec r, long long ch
 
 // Many gathers in one launch: chunk c belongs to the record whose
 // [chunk_start, next chunk_start) range holds it.
+// A CTA's chunks come in increasing order, so after a binary search for the
+// first one the record index only moves forward.
 __global__ void k_gather_group(const GatherRec* __restrict__ recs, int count, long long total_chunks) {
+  int lo = -1;
   for (long long c = blockIdx.x; c < total_chunks; c += gridDim.x) {
-    int lo = 0, hi = count - 1;
-    while (lo < hi) {
-      int mid = (lo + hi + 1) >> 1;
-      if (recs[mid].chunk_start <= c) lo = mid; else hi = mid - 1;
+    if (lo < 0) {
+      int hi = count - 1;
+      lo = 0;
+      while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (recs[mid].chunk_start <= c) lo = mid; else hi = mid - 1;
+      }
+    } else {
+      while (lo + 1 < count && recs[lo + 1].chunk_start <= c) ++lo;
     }
     const GatherRec& r = recs[lo];
     if (r.row_mode) {
