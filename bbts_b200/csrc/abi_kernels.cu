@@ -78,22 +78,31 @@ static int set_tc_attrs() {
   return rc;
 }
 
-template <bool AMN, bool BMN>
+template <bool AMN, bool BMN, bool EP8>
 static int set_tc2_attr() {
-  BBX_CUDA(cudaFuncSetAttribute(tc_gemm2_kernel<AMN, BMN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                Tc2Cfg<AMN, BMN>::SMEM_BYTES));
+  BBX_CUDA(cudaFuncSetAttribute(tc_gemm2_kernel<AMN, BMN, EP8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                Tc2Cfg<AMN, BMN, EP8>::SMEM_BYTES));
   return BBX_OK;
 }
 
-static int launch_tc2(bool amn, bool bmn, const TcArgs& args, int grid, cudaStream_t st) {
+template <bool EP8>
+static int set_tc2_attrs() {
+  int rc = 0;
+  rc |= set_tc2_attr<false, false, EP8>(); rc |= set_tc2_attr<false, true, EP8>();
+  rc |= set_tc2_attr<true, false, EP8>();  rc |= set_tc2_attr<true, true, EP8>();
+  return rc;
+}
+
+static int launch_tc2(bool amn, bool bmn, bool ep8, const TcArgs& args, int grid, cudaStream_t st) {
   if (grid < 2) grid = 2;
-#define TC2_CASE(A_, B_)                                                                     \
-  if (amn == A_ && bmn == B_) {                                                              \
-    tc_gemm2_kernel<A_, B_><<<grid, Tc2Cfg<A_, B_>::THREADS, Tc2Cfg<A_, B_>::SMEM_BYTES, st>>>(args); \
-    BBX_CHECK_LAUNCH("tc_gemm2_kernel");                                                     \
-    return BBX_OK;                                                                           \
+#define TC2_CASE(A_, B_, E_)                                                                  \
+  if (amn == A_ && bmn == B_ && ep8 == E_) {                                                  \
+    tc_gemm2_kernel<A_, B_, E_><<<grid, Tc2Cfg<A_, B_, E_>::THREADS, Tc2Cfg<A_, B_, E_>::SMEM_BYTES, st>>>(args); \
+    BBX_CHECK_LAUNCH("tc_gemm2_kernel");                                                      \
+    return BBX_OK;                                                                            \
   }
-  TC2_CASE(false, false) TC2_CASE(false, true) TC2_CASE(true, false) TC2_CASE(true, true)
+  TC2_CASE(false, false, false) TC2_CASE(false, true, false) TC2_CASE(true, false, false) TC2_CASE(true, true, false)
+  TC2_CASE(false, false, true) TC2_CASE(false, true, true) TC2_CASE(true, false, true) TC2_CASE(true, true, true)
 #undef TC2_CASE
   return set_error(BBX_ERR_UNSUPPORTED, "no 2-SM variant");
 }
@@ -102,8 +111,8 @@ static int init_tc_attributes() {
   int rc = 0;
   rc |= set_tc_attrs<false>();
   rc |= set_tc_attrs<true>();
-  rc |= set_tc2_attr<false, false>(); rc |= set_tc2_attr<false, true>();
-  rc |= set_tc2_attr<true, false>();  rc |= set_tc2_attr<true, true>();
+  rc |= set_tc2_attrs<false>();
+  rc |= set_tc2_attrs<true>();
   for (auto f : {(const void*)k_stream_bulk<false>, (const void*)k_stream_bulk<true>,
                  (const void*)k_stream_bulk_inline<false>, (const void*)k_stream_bulk_inline<true>})
     rc |= cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kBulkSmemMax) != cudaSuccess;
@@ -338,7 +347,7 @@ using namespace bbx;
 struct bbx_tc_plan {
   int dtype = BBX_BF16;
   int bn = 256;
-  bool ep8 = false;  // 1-SM tiles: eight epilogue warps (every problem's K <= kTcEp8MaxK)
+  bool ep8 = false;  // eight epilogue warps (every problem's K <= kTcEp8MaxK, kTc2Ep8MaxK for the pair)
   bool amn = false, bmn = true;
   int count = 0;
   int total_tiles = 0;
@@ -458,7 +467,7 @@ int bbx_tc_plan_create(int in_dtype, const bbx_tc_problem_t* problems, int count
   p->total_tiles = tiles;
   int max_k = 0;
   for (int i = 0; i < count; ++i) max_k = std::max(max_k, problems[i].k);
-  p->ep8 = tile_n != 512 && max_k <= kTcEp8MaxK;
+  p->ep8 = max_k <= (tile_n == 512 ? kTc2Ep8MaxK : kTcEp8MaxK);
   if (count > kTcMaxInline) {
     cudaError_t e = cudaMalloc(&p->d_table, sizeof(TcProblem) * count);
     if (e != cudaSuccess) { delete p; return set_error(BBX_ERR_CUDA, "cudaMalloc(plan table): %s", cudaGetErrorString(e)); }
@@ -485,7 +494,7 @@ int bbx_tc_plan_launch(bbx_tc_plan_t* p, void* stream) {
   if (p->bn == 512) {
     // one CTA pair (cluster of 2) per 256 x 256 tile, persistent over the tile list
     const int grid = 2 * std::min(p->total_tiles, d->sms / 2);
-    return launch_tc2(p->amn, p->bmn, args, grid, (cudaStream_t)stream);
+    return launch_tc2(p->amn, p->bmn, p->ep8, args, grid, (cudaStream_t)stream);
   }
   const int grid = std::min(p->total_tiles, d->sms);
   return launch_tc(p->bn, p->amn, p->bmn, p->dtype == BBX_E4M3, p->ep8, args, grid,

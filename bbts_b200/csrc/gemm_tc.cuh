@@ -87,6 +87,11 @@ static_assert(32 * kTcEpiPitch * 4 <= kTcEpiSlot && 32 * 128 <= kTcEpiSlot && kT
 // long K the missing stage costs more than the extra warps give (the FP8 4096^3
 // blocks: 2609 -> 2453 TFLOP/s), so the host picks it only for short K.
 constexpr int kTcEp8MaxK = 512;
+// The same for the 2-SM pair kernel's 256 x 256 tiles: config 1's 64 x 1024^3
+// products 0.143 -> 0.128 ms. Not for longer K: with groups of K up to 2048 the
+// 2000-op DAG's tensor groups ran 10 % faster alone but its makespan 2-4 %
+// slower, and the FFN step (K = 2048) 3 % slower.
+constexpr int kTc2Ep8MaxK = 1024;
 
 template <int BN, bool A_MN, bool B_MN, bool FP8, bool EP8 = false>
 struct TcCfg {
@@ -679,7 +684,7 @@ __global__ void __launch_bounds__(EP8 ? 320 : 192, 1) tc_gemm_kernel(const __gri
 // barriers; both epilogues release the accumulator on the leader's tempty.
 // bf16 only.
 // ============================================================================
-template <bool A_MN, bool B_MN>
+template <bool A_MN, bool B_MN, bool EP8 = false>
 struct Tc2Cfg {
   static constexpr int BM = 256;  // rows per pair (128 per CTA)
   static constexpr int BN = 256;  // columns per pair (128 B rows per CTA)
@@ -688,21 +693,25 @@ struct Tc2Cfg {
   static constexpr int A_BYTES = 128 * 128;  // 128 rows x 128 B
   static constexpr int B_BYTES = 128 * 128;
   static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-  static constexpr int STAGES = 6;
+  // EP8: eight epilogue warps per CTA (two per TMEM lane quarter, alternate
+  // 32-column chunks) and one stage fewer, as in the 1-SM kernel
+  static constexpr int STAGES = EP8 ? 5 : 6;
   static constexpr int TMEM_COLS = 512;
-  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256 + kTcMetaBytes + kTcEpiBytes;
-  static constexpr int THREADS = 192;
+  static constexpr int EPI_WARPS = EP8 ? 8 : 4;
+  static constexpr int EPI_PARTS = EP8 ? 2 : 1;
+  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256 + kTcMetaBytes + EPI_WARPS * kTcEpiSlot;
+  static constexpr int THREADS = 64 + 32 * EPI_WARPS;
 };
 
-template <bool A_MN, bool B_MN>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
+template <bool A_MN, bool B_MN, bool EP8>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(EP8 ? 320 : 192, 1)
     tc_gemm2_kernel(const __grid_constant__ TcArgs args) {
-  using C = Tc2Cfg<A_MN, B_MN>;
+  using C = Tc2Cfg<A_MN, B_MN, EP8>;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t* stage_base = smem;
-  uint8_t* epi_base = smem + C::STAGES * C::STAGE_BYTES;  // 4 epilogue slots, 1024-byte aligned
-  uint64_t* bars = (uint64_t*)(epi_base + kTcEpiBytes);
+  uint8_t* epi_base = smem + C::STAGES * C::STAGE_BYTES;  // EPI_WARPS epilogue slots, 1024-byte aligned
+  uint64_t* bars = (uint64_t*)(epi_base + C::EPI_WARPS * kTcEpiSlot);
   uint64_t* full_bar = bars;
   uint64_t* empty_bar = bars + C::STAGES;
   uint64_t* tfull_bar = bars + 2 * C::STAGES;
@@ -727,7 +736,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&tfull_bar[b], 1);
-      mbar_init(&tempty_bar[b], 256);  // both CTAs' epilogue threads
+      mbar_init(&tempty_bar[b], 2 * 32 * C::EPI_WARPS);  // both CTAs' epilogue threads
     }
     fence_mbar_init();
   }
@@ -859,8 +868,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
       tc_fence_after();
       const uint32_t t_row = tmem_base + acc * C::BN + ((uint32_t)lane_base << 16);
       const int row0 = tm * C::BM + (int)rank * 128 + lane_base;
-      if (pr->flags & EPI_TMA_STORE) tc_epi_rows_tma<C::BN>(pr, t_row, row0, lane, epi_buf, tn * C::BN, box_sel);
-      else tc_epi_rows<C::BN>(pr, t_row, row0, lane, epi_stage, tn * C::BN);
+      const int part = EP8 ? (warp - 2) >> 2 : 0;
+      if (pr->flags & EPI_TMA_STORE)
+        tc_epi_rows_tma<C::BN, C::EPI_PARTS>(pr, t_row, row0, lane, epi_buf, tn * C::BN, box_sel, part);
+      else tc_epi_rows<C::BN, C::EPI_PARTS>(pr, t_row, row0, lane, epi_stage, tn * C::BN, part);
       tc_fence_before();
       mbar_arrive_cluster(acc == 0 ? tempty_leader0 : tempty_leader1);
       if (++acc == 2) { acc = 0; acc_ph ^= 1; }

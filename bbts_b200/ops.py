@@ -62,9 +62,10 @@ def matmul_tc(problems, in_dtype=BF16, tile_n=0):
     check(lib.bbx_matmul_tc(in_dtype, arr, len(problems), tile_n, _stream()))
 
 
-# Groups whose largest K is at most this run the 1-SM kernel with eight epilogue warps
-# (the variant the plan picks; `kTcEp8MaxK` in csrc/gemm_tc.cuh).
+# Groups whose largest K is at most this run with eight epilogue warps (the variant the
+# plan picks; `kTcEp8MaxK` / `kTc2Ep8MaxK` in csrc/gemm_tc.cuh): 1-SM tiles, the 2-SM pair.
 TC_EP8_MAX_K = 512
+TC2_EP8_MAX_K = 1024
 
 
 class TcPlan:
@@ -92,7 +93,8 @@ class TcPlan:
         a = "MN-major A" if self.trans[0] else "K-major A"
         b = "K-major B" if self.trans[1] else "MN-major B"
         if tn == 512:
-            return "tc_gemm2_kernel<%s,%s> (2-SM 256x256 pair, cta_group::2)" % (a, b)
+            epi = "8 epilogue warps" if self.max_k <= TC2_EP8_MAX_K else "4 epilogue warps"
+            return "tc_gemm2_kernel<%s,%s,%s> (2-SM 256x256 pair, cta_group::2)" % (a, b, epi)
         epi = "8 epilogue warps" if self.max_k <= TC_EP8_MAX_K else "4 epilogue warps"
         return "tc_gemm_kernel<%d,%s,%s,%s,%s>" % (tn, a, b, "e4m3" if self.in_dtype == E4M3 else "bf16", epi)
 

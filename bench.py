@@ -848,7 +848,7 @@ def run_cpmm(args):
     kern_ms = float(np.mean(step_ms))
     achieved = FLOP_PER_STEP / (kern_ms * 1e-3) / 1e12
     tile = tiles[0] if tiles else 0
-    kname = ("tc_gemm2_kernel<0,1> (2-SM 256x256 pair, cta_group::2)" if tile == 512
+    kname = ("tc_gemm2_kernel<0,1,0> (2-SM 256x256 pair, cta_group::2)" if tile == 512
              else "tc_gemm_kernel<%d,0,1,0,0>" % tile)
     traffic = TRAFFIC_BYTES_PER_LAUNCH.get(tile) if GRID == 8 else None
     roofline = {"bound": "tensor", "achieved": round(achieved, 1), "peak": bf16_peak, "unit": "TFLOP/s",
