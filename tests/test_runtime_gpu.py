@@ -324,7 +324,10 @@ def test_learned_tile_choice(R):
     try:
         for seed in range(5):
             rt = runtime.Runtime()
-            _tile_dag(workloads, rt, 300 + seed)
+            # sizes to 2048: group times spread over an order of magnitude (with
+            # sizes to 1024 most groups take a few tens of microseconds, launch-bound)
+            workloads.random_dag(rt, n_ops=240, depth=6, seed=300 + seed, dtype="bf16", lo=128, hi=2048, step=64,
+                                 contraction_dims=(16, 64))
             dag = rt.build_dag(runtime.HEURISTIC, tile_n=runtime.AUTOTUNE)
             dag.close()
             rt.close()
