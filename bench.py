@@ -45,7 +45,7 @@ REF_BUDGET_S = 150.0  # the reference arm's whole run (warm-up + timed steps)
 # problems: each one reads its own A and B panels). 512 (the 2-SM pair): one
 # launch of the 4x4-block case (16 problems), 2727.9 MB, x4; 256: the 2x2-block
 # case (4 problems), 548 MB, x16.
-TRAFFIC_BYTES_PER_LAUNCH = {512: 10.91e9, 256: 8.77e9}
+TRAFFIC_BYTES_PER_LAUNCH = {512: 10.12e9, 256: 8.77e9}
 TRAFFIC_SOURCE = {512: "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 16-problem launch (--grid 4), x4",
                   256: "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 4-problem launch (--grid 2), x16"}
 
