@@ -422,9 +422,49 @@ def test_matmul_tc_grouped_epilogues(T):
         ref = 0.5 * oracle.matmul_f64(a, b) + 1.5 * c0 + bias
         refs.append(np.maximum(ref, 0) if relu else ref)
         outs.append(Cd)
-    ops.matmul_tc(probs)  # 6 problems -> device problem table path
+    ops.matmul_tc(probs)  # 6 problems: carried in the kernel parameters
     for o, r in zip(outs, refs):
         assert rel_err(host(o), r) <= 1e-5
+
+
+@pytest.mark.parametrize("tile_n", [128, 256, 512])
+def test_matmul_tc_params_and_table_paths(T, tile_n):
+    """Plans of up to 72 problems carry them (tensor maps included) in the
+    kernel parameters, larger ones in a device table whose maps each CTA
+    acquires before use: 72 and 73 problems of integer-valued blocks, ragged
+    shapes, row- and column-major C and bias / relu epilogues, give every
+    problem's exact int64 product, over three replays."""
+    torch, ops = T
+    rng = np.random.default_rng(91 + tile_n)
+    for count in (72, 73):
+        probs, checks, keep = [], [], []
+        for i in range(count):
+            m, n = int(rng.integers(1, 9)) * 64, int(rng.integers(1, 9)) * 64
+            k = int(rng.choice([64, 128, 192]))
+            a = rng.integers(-3, 4, (m, k)).astype(np.float32)
+            b = rng.integers(-3, 4, (k, n)).astype(np.float32)
+            bias = rng.integers(-8, 9, n).astype(np.float32) if i % 3 == 0 else None
+            relu = i % 4 == 1
+            colmajor = i % 5 == 2
+            A, B = dev(torch, a, torch.bfloat16), dev(torch, b, torch.bfloat16)
+            bt = dev(torch, bias) if bias is not None else None
+            c = torch.full((n, m) if colmajor else (m, n), float("nan"), device="cuda")
+            probs.append(ops.tc_problem(A, B, c, bias=bt, relu=relu, c_colmajor=colmajor))
+            r = a.astype(np.int64) @ b.astype(np.int64)
+            if bias is not None:
+                r = r + bias.astype(np.int64)[None, :]
+            if relu:
+                r = np.maximum(r, 0)
+            keep += [A, B, bt, c]
+            checks.append((c, r.T if colmajor else r))
+        plan = ops.TcPlan(probs, tile_n=tile_n)
+        for _ in range(3):
+            for c, _r in checks:
+                c.fill_(float("nan"))
+            plan.launch()
+            for i, (c, want) in enumerate(checks):
+                assert np.array_equal(host(c), want.astype(np.float64)), (count, i)
+        plan.close()
 
 
 def test_matmul_tc_bf16_output(T):
