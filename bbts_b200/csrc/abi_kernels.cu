@@ -11,6 +11,7 @@
 
 #include "bbts_b200.h"
 #include "common.h"
+#include "contraction.h"
 #include "gemm_f32.cuh"
 #include "gemm_tc.cuh"
 #include "stream_ops.cuh"
@@ -116,6 +117,7 @@ static int init_tc_attributes() {
   for (auto f : {(const void*)k_stream_bulk<false>, (const void*)k_stream_bulk<true>,
                  (const void*)k_stream_bulk_inline<false>, (const void*)k_stream_bulk_inline<true>})
     rc |= cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kBulkSmemMax) != cudaSuccess;
+  rc |= gather_bulk_init() != BBX_OK;
   return rc ? BBX_ERR_CUDA : BBX_OK;
 }
 
@@ -138,6 +140,15 @@ int device_state(DeviceState** out) {
     d.ready = true;
   }
   *out = &d;
+  return BBX_OK;
+}
+
+int device_status_and_sms(uint32_t** status, int* sms) {
+  DeviceState* d;
+  int rc = device_state(&d);
+  if (rc) return rc;
+  *status = d->status;
+  *sms = d->sms;
   return BBX_OK;
 }
 

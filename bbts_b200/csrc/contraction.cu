@@ -25,6 +25,7 @@
 #include "bbts_b200.h"
 #include "common.h"
 #include "contraction.h"
+#include "ptx.cuh"
 
 namespace bbx {
 
@@ -221,6 +222,158 @@ __global__ void __launch_bounds__(256, 4) k_gather_group(const GatherRec* __rest
     const long long e0 = (c - r.chunk_start) * kGatherChunk;
     const long long e1 = min(e0 + kGatherChunk, r.n);
     for (long long e = e0 + threadIdx.x; e < e1; e += blockDim.x) gather_one(r.src, r.dst, r.dst_bf16, r.a, e);
+  }
+}
+
+// ---- bulk-staged row gather: every record on the row path, its source 16-byte
+// aligned and every destination row 16-byte aligned (the tensor-core staging
+// blocks, whose pitches are padded to 16 bytes). One CTA per SM:
+//  - a producer warp deals items (one row segment of up to kGatherSeg
+//    elements) kGBItems to a stage: lane u finds item u's record and row,
+//    and copies the segment's whole 16-byte blocks into the stage with one
+//    cp.async.bulk, completing on the stage's `full` mbarrier;
+//  - kGBConsumerWarps warps convert each staged segment and store it (8-byte
+//    bf16 / 16-byte f32 stores where the source row is 16-byte aligned, else
+//    element by element); the at most 3 + 3 elements before the first and
+//    after the last whole block are read from global memory directly.
+// The loads leave the consumers' critical path (the row kernel above issues
+// element loads and waits on them).
+constexpr int kGBStages = 3;
+constexpr int kGBItems = 16;
+constexpr int kGBItemBytes = (int)kGatherSeg * 4;
+constexpr int kGBSlot = kGBItems * kGBItemBytes;  // 64 KiB
+constexpr int kGBConsumerWarps = 8;
+constexpr int kGBThreads = 32 * (kGBConsumerWarps + 1);
+constexpr int kGBMaxRecs = 1024;
+struct GBItem {
+  long long so, dso, c0, c1;  // source / destination element of the segment; its whole blocks [c0, c1)
+  int len, rec;               // elements (0: no item), record
+};
+constexpr int kGBSmemBase = kGBStages * kGBSlot + kGBStages * 16 + kGBStages * kGBItems * (int)sizeof(GBItem);
+__host__ __device__ inline int gb_smem_bytes(int count) { return kGBSmemBase + 8 * count; }
+
+__device__ __forceinline__ void gb_locate(const GatherRec& R, long long local, long long& so, long long& dso,
+                                          int& len) {
+  const int outer = R.a.rank_o - 1;
+  const long long row = local / R.segs, start = (local - row * R.segs) * kGatherSeg;
+  long long rem = row, s = start, t = start;
+  for (int d = outer - 1; d >= 0; --d) {
+    const long long idx = rem % R.a.odims[d];
+    rem /= R.a.odims[d];
+    s += idx * R.a.istride[d];
+    t += idx * R.a.ostride[d];
+  }
+  so = s;
+  dso = t;
+  len = (int)min(kGatherSeg, R.row_len - start);
+}
+
+__global__ void __launch_bounds__(kGBThreads, 1) k_gather_bulk(const GatherRec* __restrict__ recs, int count,
+                                                                long long total_items, uint32_t* status) {
+  extern __shared__ __align__(128) uint8_t gb_smem[];
+  uint64_t* full = (uint64_t*)(gb_smem + kGBStages * kGBSlot);
+  uint64_t* empty = full + kGBStages;
+  GBItem* items = (GBItem*)(empty + kGBStages);                     // [kGBStages][kGBItems]
+  long long* starts = (long long*)(items + kGBStages * kGBItems);   // [count]: each record's first item
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < kGBStages; ++q) {
+      mbar_init(&full[q], 1);
+      mbar_init(&empty[q], kGBConsumerWarps);
+    }
+    fence_mbar_init();
+  }
+  for (int i = threadIdx.x; i < count; i += blockDim.x) starts[i] = recs[i].chunk_start;
+  __syncthreads();
+  volatile uint32_t* st = status;
+  const long long step = (long long)gridDim.x * kGBItems;
+  if (warp == kGBConsumerWarps) {
+    // ------------------------------------------------------------ producer
+    int k = 0;
+    for (long long base = (long long)blockIdx.x * kGBItems; base < total_items; base += step, ++k) {
+      const int s = k % kGBStages;
+      const uint32_t ph = (uint32_t)(k / kGBStages) & 1u;
+      bool ok = true;
+      if (lane == 0) ok = mbar_wait(&empty[s], ph ^ 1u, st, DEV_TIMEOUT_EMPTY);
+      if (!__shfl_sync(0xffffffffu, ok, 0)) break;
+      const long long item = base + lane;
+      GBItem it{0, 0, 0, 0, 0, 0};
+      uint32_t bytes = 0;
+      const float* src = nullptr;
+      if (lane < kGBItems && item < total_items) {
+        int lo = 0, hi = count - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (starts[mid] <= item) lo = mid; else hi = mid - 1;
+        }
+        const GatherRec& R = recs[lo];
+        gb_locate(R, item - starts[lo], it.so, it.dso, it.len);
+        it.rec = lo;
+        it.c0 = (it.so + 3) & ~3LL;
+        it.c1 = (it.so + it.len) & ~3LL;
+        if (it.c1 < it.c0) it.c1 = it.c0;
+        bytes = (uint32_t)(it.c1 - it.c0) * 4u;
+        src = R.src;
+      }
+      if (lane < kGBItems) items[s * kGBItems + lane] = it;
+      const uint32_t total = __reduce_add_sync(0xffffffffu, bytes);
+      __syncwarp();  // the item descriptors are written before lane 0's arrive publishes them
+      if (lane == 0) {
+        if (total) mbar_arrive_expect_tx(&full[s], total);
+        else mbar_arrive(&full[s]);
+      }
+      __syncwarp();  // the expected bytes are registered before any copy is issued
+      if (bytes) bulk_load(gb_smem + s * kGBSlot + lane * kGBItemBytes, src + it.c0, bytes, &full[s]);
+    }
+    // copies issued but never consumed (only after an error) land before exit
+    if (lane == 0 && *st != DEV_OK) {
+      const long long t0 = clock64();
+      while (clock64() - t0 < 200000) {}
+    }
+    return;
+  }
+  // -------------------------------------------------------------- consumers
+  int k = 0;
+  for (long long base = (long long)blockIdx.x * kGBItems; base < total_items; base += step, ++k) {
+    const int s = k % kGBStages;
+    const uint32_t ph = (uint32_t)(k / kGBStages) & 1u;
+    if (!__all_sync(0xffffffffu, mbar_wait(&full[s], ph, st, DEV_TIMEOUT_FULL))) break;
+    for (int u = warp; u < kGBItems; u += kGBConsumerWarps) {
+      const GBItem it = items[s * kGBItems + u];
+      if (it.len == 0) continue;
+      const GatherRec& R = recs[it.rec];
+      const float* __restrict__ src = R.src;
+      const bool bf16 = R.dst_bf16 != 0;
+      const float* sp = (const float*)(gb_smem + s * kGBSlot + u * kGBItemBytes);
+      const int nw = (int)(it.c1 - it.c0);  // staged elements
+      if (it.c0 == it.so) {
+        // the row is 16-byte aligned: staged element j is output element j
+        for (int q = lane; q < nw / 4; q += 32) {
+          const float4 v = *(const float4*)(sp + 4 * q);
+          const long long o = it.dso + 4 * q;
+          if (bf16) {
+            const __nv_bfloat162 a = __floats2bfloat162_rn(v.x, v.y), b = __floats2bfloat162_rn(v.z, v.w);
+            *(uint2*)((__nv_bfloat16*)R.dst + o) = make_uint2(*(const uint32_t*)&a, *(const uint32_t*)&b);
+          } else {
+            *(float4*)((float*)R.dst + o) = v;
+          }
+        }
+        for (int y = nw + lane; y < it.len; y += 32) {  // the tail after the last whole block
+          const float v = __ldg(src + it.so + y);
+          if (bf16) ((__nv_bfloat16*)R.dst)[it.dso + y] = __float2bfloat16_rn(v);
+          else ((float*)R.dst)[it.dso + y] = v;
+        }
+      } else {
+        for (int y = lane; y < it.len; y += 32) {
+          const long long x = it.so + y;
+          const float v = (x >= it.c0 && x < it.c1) ? sp[x - it.c0] : __ldg(src + x);
+          if (bf16) ((__nv_bfloat16*)R.dst)[it.dso + y] = __float2bfloat16_rn(v);
+          else ((float*)R.dst)[it.dso + y] = v;
+        }
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
   }
 }
 
@@ -426,22 +579,45 @@ struct GatherPlan {
   GatherRec* d = nullptr;
   int count = 0;
   long long total = 0;
+  bool bulk = false;  // k_gather_bulk: `total` counts row segments, chunk_start each record's first
 };
 
-int gather_plan_create(const GatherRec* recs, int count, GatherPlan** out) {
+// Every record on the row path with a 16-byte aligned source and 16-byte
+// aligned destination rows (base and every row stride).
+static bool bulk_ok(const GatherRec& r) {
+  if (!r.row_mode || (((uintptr_t)r.src) & 15) || (((uintptr_t)r.dst) & 15)) return false;
+  const long long esz = r.dst_bf16 ? 2 : 4;
+  for (int d = 0; d + 1 < r.a.rank_o; ++d)
+    if ((r.a.ostride[d] * esz) & 15) return false;
+  return true;
+}
+
+int gather_bulk_init() {
+  cudaError_t e = cudaFuncSetAttribute(k_gather_bulk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       gb_smem_bytes(kGBMaxRecs));
+  return e == cudaSuccess ? BBX_OK : set_error(BBX_ERR_CUDA, "k_gather_bulk attribute: %s", cudaGetErrorString(e));
+}
+
+int gather_plan_create(const GatherRec* recs, int count, GatherPlan** out, bool allow_bulk) {
   if (!recs || count <= 0 || !out) return set_error(BBX_ERR_INVALID, "bad gather plan");
   std::vector<GatherRec> h(recs, recs + count);
-  long long chunks = 0;
+  bool bulk = allow_bulk && count <= kGBMaxRecs;
   for (auto& r : h) {
     simplify_gather(&r.a);
     set_row_mode(&r);
+    bulk = bulk && bulk_ok(r);
+  }
+  long long chunks = 0;
+  for (auto& r : h) {
     r.chunk_start = chunks;
-    if (r.row_mode) chunks += (row_items(r) + r.items_per_chunk - 1) / r.items_per_chunk;
+    if (bulk) chunks += row_items(r);
+    else if (r.row_mode) chunks += (row_items(r) + r.items_per_chunk - 1) / r.items_per_chunk;
     else chunks += (r.n + kGatherChunk - 1) / kGatherChunk;
   }
   auto* p = new GatherPlan();
   p->count = count;
   p->total = chunks;
+  p->bulk = bulk;
   cudaError_t e = cudaMalloc(&p->d, sizeof(GatherRec) * count);
   if (e == cudaSuccess) e = cudaMemcpy(p->d, h.data(), sizeof(GatherRec) * count, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
@@ -455,6 +631,18 @@ int gather_plan_create(const GatherRec* recs, int count, GatherPlan** out) {
 
 int gather_plan_launch(GatherPlan* p, void* stream) {
   if (!p || p->total == 0) return BBX_OK;
+  if (p->bulk) {
+    uint32_t* status = nullptr;
+    int sms = 148;
+    int rc = device_status_and_sms(&status, &sms);
+    if (rc) return rc;
+    const long long grid = std::min<long long>((p->total + kGBItems - 1) / kGBItems, sms);
+    k_gather_bulk<<<(int)grid, kGBThreads, gb_smem_bytes(p->count), (cudaStream_t)stream>>>(p->d, p->count,
+                                                                                          p->total, status);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_error(BBX_ERR_CUDA, "k_gather_bulk: %s", cudaGetErrorString(e));
+    return BBX_OK;
+  }
   long long grid = std::min<long long>(p->total, 148 * 8);
   k_gather_group<<<(int)grid, 256, 0, (cudaStream_t)stream>>>(p->d, p->count, p->total);
   cudaError_t e = cudaGetLastError();

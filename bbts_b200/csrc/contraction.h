@@ -72,8 +72,15 @@ struct GatherRec {
 void simplify_gather(GatherArgs* a);
 
 struct GatherPlan;
-int gather_plan_create(const GatherRec* recs, int count, GatherPlan** out);
+// allow_bulk: use the bulk-staged kernel when every record qualifies. It holds
+// about 200 KB of shared memory per SM, so it cannot run beside a tensor-core
+// launch; the row kernel, which needs none, can.
+int gather_plan_create(const GatherRec* recs, int count, GatherPlan** out, bool allow_bulk = true);
 int gather_plan_launch(GatherPlan* p, void* stream);
 void gather_plan_destroy(GatherPlan* p);
+// Opts the bulk gather kernel into its shared memory (once per device, outside any capture).
+int gather_bulk_init();
+// The device's status word (bounded waits report into it) and SM count (abi_kernels.cu).
+int device_status_and_sms(uint32_t** status, int* sms);
 
 }  // namespace bbx

@@ -605,8 +605,15 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
   // ---- launch groups per wave
   std::vector<std::vector<int>> by_wave(nw);
   for (int i = 0; i < N; ++i) by_wave[nodes[i].wave].push_back(i);
+  // waves with block matmuls on the tensor stream: a wave's gathers may run
+  // beside its own and the previous wave's matmul launches, which the
+  // bulk-staged gather (its shared memory) would keep off those SMs
+  std::vector<char> wave_mm(nw, 0);
+  for (int i = 0; i < N; ++i)
+    if (nodes[i].kind == NK_TC) wave_mm[nodes[i].wave] = 1;
   for (int w = 0; w < nw; ++w) {
     auto& ids = by_wave[w];
+    const bool bulk_gather = !wave_mm[w] && !(w > 0 && wave_mm[w - 1]);
     if (policy == SCHED_LEARNED)
       std::stable_sort(ids.begin(), ids.end(), [&](int a, int b) { return nodes[a].cost > nodes[b].cost; });
     else
@@ -764,7 +771,7 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
     }
     // group order inside a wave: PRE, STREAM phases, OTHER (memory stream); TC (tensor stream); POST
     if (!pre.empty()) {
-      dag_bbx(bbx::gather_plan_create(pre.data(), (int)pre.size(), &gpre.gather_plan));
+      dag_bbx(bbx::gather_plan_create(pre.data(), (int)pre.size(), &gpre.gather_plan, bulk_gather));
       gpre.bytes = gather_group_bytes(pre);
       d->groups.push_back(std::move(gpre));
       d->stats.stream_launches++;
@@ -825,7 +832,7 @@ dag_t* dag_build(runtime_t* rt, int policy, int tile_n) {
       d->stats.tc_launches++;
     }
     if (!post.empty()) {
-      dag_bbx(bbx::gather_plan_create(post.data(), (int)post.size(), &gpost.gather_plan));
+      dag_bbx(bbx::gather_plan_create(post.data(), (int)post.size(), &gpost.gather_plan, bulk_gather));
       gpost.bytes = gather_group_bytes(post);
       d->groups.push_back(std::move(gpost));
       d->stats.stream_launches++;

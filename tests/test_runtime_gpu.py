@@ -713,6 +713,29 @@ def test_random_bf16_dag_with_contractions_matches_per_op(R, policy):
             assert np.array_equal(a, b), t
 
 
+def test_contraction_only_bf16_dag_matches_per_op(R):
+    """A DAG of contractions only (no block matmul beside them): its operand
+    gathers run on the bulk-staged kernel (row segments copied into shared
+    memory by cp.async.bulk), with sources and rows of every alignment, and the
+    results equal the per-op path (row gather kernel) byte for byte."""
+    runtime, workloads = R
+    mk = lambda rt: workloads.random_dag(rt, n_ops=60, depth=5, seed=33, dtype="bf16", contraction_dims=(13, 90),
+                                         mix=(0.0, 0.0, 0.0, 1.0))
+    rt1 = runtime.Runtime()
+    info = mk(rt1)
+    rt1.run()
+    rt2 = runtime.Runtime()
+    mk(rt2)
+    dag = rt2.build_dag(runtime.HEURISTIC)
+    for rep in range(2):
+        dag.launch()
+        for t in info["finals"]:
+            a = rt1.get_bytes(t)
+            b = dag.read_bytes(t, a.nbytes)
+            assert np.array_equal(a, b), t
+    dag.close()
+
+
 @pytest.mark.parametrize("stream_kernel", [1, 2])
 def test_dag_streaming_kernel_choice_keeps_results(R, stream_kernel):
     """The register streaming kernel (1) and the per-wave choice (2) give the
