@@ -247,7 +247,9 @@ constexpr int kGBThreads = 32 * (kGBConsumerWarps + 1);
 constexpr int kGBMaxRecs = 1024;
 struct GBItem {
   long long so, dso, c0, c1;  // source / destination element of the segment; its whole blocks [c0, c1)
-  int len, rec;               // elements (0: no item), record
+  const float* src;           // the record's source and destination (consumers read no record)
+  void* dst;
+  int len, bf16;              // elements (0: no item); destination bf16
 };
 constexpr int kGBSmemBase = kGBStages * kGBSlot + kGBStages * 16 + kGBStages * kGBItems * (int)sizeof(GBItem);
 __host__ __device__ inline int gb_smem_bytes(int count) { return kGBSmemBase + 8 * count; }
@@ -297,7 +299,7 @@ __global__ void __launch_bounds__(kGBThreads, 1) k_gather_bulk(const GatherRec* 
       if (lane == 0) ok = mbar_wait(&empty[s], ph ^ 1u, st, DEV_TIMEOUT_EMPTY);
       if (!__shfl_sync(0xffffffffu, ok, 0)) break;
       const long long item = base + lane;
-      GBItem it{0, 0, 0, 0, 0, 0};
+      GBItem it{0, 0, 0, 0, nullptr, nullptr, 0, 0};
       uint32_t bytes = 0;
       const float* src = nullptr;
       if (lane < kGBItems && item < total_items) {
@@ -308,7 +310,9 @@ __global__ void __launch_bounds__(kGBThreads, 1) k_gather_bulk(const GatherRec* 
         }
         const GatherRec& R = recs[lo];
         gb_locate(R, item - starts[lo], it.so, it.dso, it.len);
-        it.rec = lo;
+        it.src = R.src;
+        it.dst = R.dst;
+        it.bf16 = R.dst_bf16;
         it.c0 = (it.so + 3) & ~3LL;
         it.c1 = (it.so + it.len) & ~3LL;
         if (it.c1 < it.c0) it.c1 = it.c0;
@@ -341,9 +345,8 @@ __global__ void __launch_bounds__(kGBThreads, 1) k_gather_bulk(const GatherRec* 
     for (int u = warp; u < kGBItems; u += kGBConsumerWarps) {
       const GBItem it = items[s * kGBItems + u];
       if (it.len == 0) continue;
-      const GatherRec& R = recs[it.rec];
-      const float* __restrict__ src = R.src;
-      const bool bf16 = R.dst_bf16 != 0;
+      const float* __restrict__ src = it.src;
+      const bool bf16 = it.bf16 != 0;
       const float* sp = (const float*)(gb_smem + s * kGBSlot + u * kGBItemBytes);
       const int nw = (int)(it.c1 - it.c0);  // staged elements
       if (it.c0 == it.so) {
@@ -353,22 +356,22 @@ __global__ void __launch_bounds__(kGBThreads, 1) k_gather_bulk(const GatherRec* 
           const long long o = it.dso + 4 * q;
           if (bf16) {
             const __nv_bfloat162 a = __floats2bfloat162_rn(v.x, v.y), b = __floats2bfloat162_rn(v.z, v.w);
-            *(uint2*)((__nv_bfloat16*)R.dst + o) = make_uint2(*(const uint32_t*)&a, *(const uint32_t*)&b);
+            *(uint2*)((__nv_bfloat16*)it.dst + o) = make_uint2(*(const uint32_t*)&a, *(const uint32_t*)&b);
           } else {
-            *(float4*)((float*)R.dst + o) = v;
+            *(float4*)((float*)it.dst + o) = v;
           }
         }
         for (int y = nw + lane; y < it.len; y += 32) {  // the tail after the last whole block
           const float v = __ldg(src + it.so + y);
-          if (bf16) ((__nv_bfloat16*)R.dst)[it.dso + y] = __float2bfloat16_rn(v);
-          else ((float*)R.dst)[it.dso + y] = v;
+          if (bf16) ((__nv_bfloat16*)it.dst)[it.dso + y] = __float2bfloat16_rn(v);
+          else ((float*)it.dst)[it.dso + y] = v;
         }
       } else {
         for (int y = lane; y < it.len; y += 32) {
           const long long x = it.so + y;
           const float v = (x >= it.c0 && x < it.c1) ? sp[x - it.c0] : __ldg(src + x);
-          if (bf16) ((__nv_bfloat16*)R.dst)[it.dso + y] = __float2bfloat16_rn(v);
-          else ((float*)R.dst)[it.dso + y] = v;
+          if (bf16) ((__nv_bfloat16*)it.dst)[it.dso + y] = __float2bfloat16_rn(v);
+          else ((float*)it.dst)[it.dso + y] = v;
         }
       }
     }
