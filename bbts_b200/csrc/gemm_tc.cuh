@@ -18,7 +18,7 @@
 //   warp 0      TMA producer (one elected lane) feeding a STAGES-deep smem ring
 //   warp 1      TMEM allocator + MMA issuer (one elected lane)
 //   warps 2..5  epilogue: tcgen05.ld from TMEM -> registers -> global (2..9 with
-//               EP8: two warps per TMEM lane quarter, half the columns each)
+//               EP8: two warps per TMEM lane quarter, alternate 32-column chunks)
 // The accumulator is double buffered in TMEM (2 x BN f32 columns), so the
 // epilogue of tile t overlaps the main loop of tile t+1.
 #pragma once
