@@ -26,6 +26,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
 #include "ptx.cuh"
+#include "tile_order.h"
 
 namespace bbx {
 
@@ -134,7 +135,8 @@ __device__ __forceinline__ void tc_stage_meta(const TcArgs& args, int4* meta) {
 }
 
 // Map a global tile index to (problem, tile_m, tile_n) and the problem's k.
-// Tiles inside a problem are visited in bands of 16 tile-rows so concurrently
+// Tiles inside a problem are visited in bands of kTileBand = 16 tile-rows
+// (band_tile, tile_order.h) so concurrently
 // running CTAs share operand tiles in L2: a 4096^2 block's B panels are then
 // read from DRAM once per problem (with bands of 8, twice; the pair kernel ran
 // 1358 -> 1440 TFLOP/s on the 64 x 4096^3 step, same box and clock).
@@ -158,15 +160,7 @@ __device__ __forceinline__ void tc_locate(const TcArgs& args, const int4* meta, 
   }
   p = lo;
   k = e.w;
-  const int lt = t - e.x;
-  constexpr int G = 16;
-  const int per_group = G * e.z;
-  const int group = lt / per_group;
-  const int first_m = group * G;
-  const int gsize = min(e.y - first_m, G);
-  const int r = lt - group * per_group;
-  tm = first_m + r % gsize;
-  tn = r / gsize;
+  band_tile(t - e.x, e.y, e.z, tm, tn);
 }
 
 // Accumulator drain of one epilogue warp: its 32 rows (row0 .. row0+31, one
@@ -478,15 +472,10 @@ __device__ __forceinline__ void tc_epi_rows_tma(const TcProblem* pr, uint32_t t_
   }
 }
 
-// Tile of CTA blockIdx.x in round `round` (t0 = round * grid + blockIdx.x):
-// snake order, so in odd rounds CTA b takes the round's tile grid - 1 - b and a
-// CTA that drew a costly tile early in the list draws a cheap one next (the
-// plan sorts problems by descending tile cost). A partial last round keeps the
-// plain order. The producer, MMA and epilogue warps all walk this sequence.
+// Tile of CTA blockIdx.x in round `round` (snake order, snake_tile_of in
+// tile_order.h). The producer, MMA and epilogue warps all walk this sequence.
 __device__ __forceinline__ int snake_tile(int t0, int round, int total) {
-  const int base = t0 - (int)blockIdx.x;
-  if ((round & 1) && base + (int)gridDim.x <= total) return base + (int)gridDim.x - 1 - (int)blockIdx.x;
-  return t0;
+  return snake_tile_of(t0, round, total, (int)blockIdx.x, (int)gridDim.x);
 }
 
 template <int BN, bool A_MN, bool B_MN, bool FP8, bool EP8>

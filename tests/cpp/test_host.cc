@@ -13,12 +13,14 @@
 #include <thread>
 #include <sstream>
 #include <tuple>
+#include <vector>
 #include "bbts_b200.h"
 #include "command.h"
 #include "compiler.h"
 #include "contraction.h"
 #include "reservation_station.h"
 #include "tensor.h"
+#include "tile_order.h"
 #include "ud_function.h"
 
 using namespace bbts;
@@ -385,7 +387,50 @@ static void test_contraction_orientation() {
   }
 }
 
+// The grouped tcgen05 launches' tile order (csrc/tile_order.h): the snake
+// rounds of a persistent grid over a group's tile list, and the bands of
+// tile-rows inside a problem, each visit every tile exactly once.
+static void test_tile_order() {
+  unsigned seed = 12345;
+  auto rnd = [&](int lo, int hi) {
+    seed = seed * 1103515245u + 12345u;
+    return lo + (int)((seed >> 8) % (unsigned)(hi - lo + 1));
+  };
+  for (int trial = 0; trial < 300; ++trial) {
+    const int grid = trial < 4 ? (trial == 0 ? 1 : 148) : rnd(1, 160);
+    const int total = trial == 2 ? grid : (trial == 3 ? 3 * grid : rnd(1, 5000));
+    std::vector<int> seen(total, 0);
+    bool in_range = true;
+    for (int b = 0; b < grid; ++b) {
+      int prev = -1;
+      for (int t0 = b, r = 0; t0 < total; t0 += grid, ++r) {
+        const int t = bbx::snake_tile_of(t0, r, total, b, grid);
+        if (t < 0 || t >= total) { in_range = false; continue; }
+        ++seen[t];
+        EXPECT(t / grid == r);  // round r's tiles stay in round r
+        EXPECT(t > prev);
+        prev = t;
+      }
+    }
+    EXPECT(in_range);
+    EXPECT(std::all_of(seen.begin(), seen.end(), [](int c) { return c == 1; }));
+  }
+  for (int tiles_m = 1; tiles_m <= 40; tiles_m += 3)
+    for (int tiles_n = 1; tiles_n <= 9; ++tiles_n) {
+      std::vector<int> seen(tiles_m * tiles_n, 0);
+      for (int lt = 0; lt < tiles_m * tiles_n; ++lt) {
+        int tm = -1, tn = -1;
+        bbx::band_tile(lt, tiles_m, tiles_n, tm, tn);
+        EXPECT(tm >= 0 && tm < tiles_m && tn >= 0 && tn < tiles_n);
+        if (tm >= 0 && tm < tiles_m && tn >= 0 && tn < tiles_n) ++seen[tm * tiles_n + tn];
+        EXPECT(tm / bbx::kTileBand == lt / (bbx::kTileBand * tiles_n));  // bands in order
+      }
+      EXPECT(std::all_of(seen.begin(), seen.end(), [](int c) { return c == 1; }));
+    }
+}
+
 int main() {
+  test_tile_order();
   test_contraction_orientation();
   test_sbbts_compile();
   test_bbts_roundtrip();
