@@ -736,11 +736,13 @@ namespace bbx {
 //    16-byte stores, handing the stage back (`empty` mbarrier) right away.
 // Measured on the FFN and 2000-op DAG levels: 8 consumer warps beat 16, whole
 // input tiles per copy beat 2-8 KiB pieces, and consumer stores beat staging
-// the output tile for a bulk store (kBulkStoreTS, kept as an option). The
+// the output tile for a bulk store (kBulkStoreTS, kept as an option). Fewer,
+// larger stages win: 3 x 72 KiB against 3 x 64 KiB ran the 2000-op DAG's
+// levels of adds at 6.89 against 6.47 TB/s (4 x 48 and 6 x 32 KiB were slower). The
 // last (< 8-element) piece of an op, if any, is read and written with plain
 // accesses.
 constexpr int kBulkStages = 3;
-constexpr int kBulkSlot = 65536;     // bytes per stage: input tiles + output tile
+constexpr int kBulkSlot = 73728;     // bytes per stage: input tiles + output tile
 constexpr int kBulkConsumerWarps = 8;
 constexpr int kBulkConsumers = kBulkConsumerWarps * 32;
 constexpr int kBulkThreads = kBulkConsumers + 32;
@@ -755,8 +757,9 @@ constexpr int kBulkThreads = kBulkConsumers + 32;
 constexpr int kBulkDescBytes = (int)sizeof(StreamOp);
 static_assert(kBulkDescBytes % 16 == 0, "stage descriptors are copied in 16-byte pieces");
 constexpr int kBulkSmem = kBulkStages * kBulkSlot + kBulkStages * 16 + kBulkStages * kBulkDescBytes;
-constexpr int kBulkMaxStagedOps = 4096;
+constexpr int kBulkMaxStagedOps = 1280;
 constexpr int kBulkSmemMax = kBulkSmem + 8 * kBulkMaxStagedOps;
+static_assert(kBulkSmemMax <= 232448, "dynamic shared memory per CTA");
 __host__ __device__ inline int bulk_smem_bytes(int count) {
   return kBulkSmem + (count <= kBulkMaxStagedOps ? 8 * count : 0);
 }
