@@ -752,7 +752,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(EP8 ? 320 : 192, 1)
       uint32_t ph = 0;
       bool ok = true;
       int last_p = -1;
-      for (int t = pair; t < args.total_tiles && ok; t += num_pairs) {
+      for (int t0 = pair, rr = 0; t0 < args.total_tiles && ok; t0 += num_pairs, ++rr) {
+        const int t = snake_tile_of(t0, rr, args.total_tiles, pair, num_pairs);
         int p, tm, tn, kdim;
         tc_locate(args, meta, t, p, tm, tn, kdim);
         const TcProblem* pr = tc_problem(args, p);
@@ -761,10 +762,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(EP8 ? 320 : 192, 1)
           tensormap_acquire(&pr->tmap_b);
           last_p = p;
         }
-        if (args.table && t + num_pairs < args.total_tiles) {
+        if (args.table && t0 + num_pairs < args.total_tiles) {
           // the next tile's tensor maps, if it starts a new problem
           int p2, tm2, tn2, k2;
-          tc_locate(args, meta, t + num_pairs, p2, tm2, tn2, k2);
+          tc_locate(args, meta, snake_tile_of(t0 + num_pairs, rr + 1, args.total_tiles, pair, num_pairs), p2, tm2,
+                    tn2, k2);
           if (p2 != p) {
             prefetch_tensormap(&args.table[p2].tmap_a);
             prefetch_tensormap(&args.table[p2].tmap_b);
@@ -813,7 +815,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(EP8 ? 320 : 192, 1)
       int acc = 0;
       uint32_t acc_ph = 0;
       bool ok = true;
-      for (int t = pair; t < args.total_tiles && ok; t += num_pairs) {
+      for (int t0 = pair, rr = 0; t0 < args.total_tiles && ok; t0 += num_pairs, ++rr) {
+        const int t = snake_tile_of(t0, rr, args.total_tiles, pair, num_pairs);
         int p, tm, tn, kdim;
         tc_locate(args, meta, t, p, tm, tn, kdim);
         const int kb_n = (kdim + C::BK - 1) / C::BK;
@@ -851,7 +854,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(EP8 ? 320 : 192, 1)
     uint32_t acc_ph = 0;
     int last_p = -1;
     int box_sel = 0;
-    for (int t = pair; t < args.total_tiles; t += num_pairs) {
+    for (int t0 = pair, rr = 0; t0 < args.total_tiles; t0 += num_pairs, ++rr) {
+      const int t = snake_tile_of(t0, rr, args.total_tiles, pair, num_pairs);
       int p, tm, tn, kdim;
       tc_locate(args, meta, t, p, tm, tn, kdim);
       const TcProblem* pr = tc_problem(args, p);
