@@ -342,8 +342,8 @@ int learned_tile_n(const runtime_t& rt, int dtype, bool ta, bool tb, const std::
 }
 
 // Bytes per microsecond of the bulk streaming kernel alone on DAG levels
-// (4.7 TB/s measured on the 2000-op DAG's levels).
-constexpr double kBulkStreamBytesPerUs = 4.7e6;
+// (5.0-5.3 TB/s measured on the 2000-op DAG's levels).
+constexpr double kBulkStreamBytesPerUs = 5.2e6;
 
 // Predicted duration (us) of a grouped tensor-core launch with tile `tn`: the
 // tile model's prediction when one is installed, else its FLOPs at 1 PFLOP/s
