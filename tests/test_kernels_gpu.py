@@ -495,10 +495,13 @@ def test_matmul_tc_plan_replay(T):
     plan.close()
 
 
-def test_matmul_fp8_per_block_scale(T):
+@pytest.mark.parametrize("k, tile_n", [(1024, 0), (256, 128), (256, 256)])
+def test_matmul_fp8_per_block_scale(T, k, tile_n):
+    """e4m3 blocks with per-block absmax scales; K = 256 runs the kernel with
+    eight epilogue warps (every K at most 512), K = 1024 the four-warp one."""
     torch, ops = T
-    rng = np.random.default_rng(12)
-    m, n, k = 512, 512, 1024
+    rng = np.random.default_rng(12 + k + tile_n)
+    m, n = 512, 512
     a = rng.uniform(-1, 1, (m, k)).astype(np.float32)
     b = rng.uniform(-1, 1, (k, n)).astype(np.float32)
     qa = torch.empty(m, k, dtype=torch.float8_e4m3fn, device="cuda")
@@ -509,7 +512,7 @@ def test_matmul_fp8_per_block_scale(T):
     ops.quantize_e4m3(dev(torch, b), qb, sb, transpose=True)
     c = torch.empty(m, n, device="cuda")
     scale = float(host(sa)[0] * host(sb)[0])
-    ops.matmul_tc([ops.tc_problem(qa, qb, c, trans_b=True, alpha=scale)], in_dtype=ops.E4M3)
+    ops.matmul_tc([ops.tc_problem(qa, qb, c, trans_b=True, alpha=scale)], in_dtype=ops.E4M3, tile_n=tile_n)
     # e4m3 keeps 3 mantissa bits (relative rounding error up to 2^-4 per input), so
     # the normwise error of a K=1024 dot product sits at a few percent: FP8 is
     # outside the 1e-2 budget, and the error is reported per block instead.
