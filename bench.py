@@ -11,7 +11,9 @@ Reported (one JSON line on rank 0):
   value       TFLOP/s of the graph replay, inputs resident in HBM
   e2e         the same through the public API with pinned HOST blocks:
               bbx_dag_write of the 16 input blocks, bbx_dag_launch,
-              bbx_dag_fetch of the 64 output blocks, every step
+              bbx_dag_fetch of the 64 output blocks, every step; two compiled
+              instances of the command list in turn, so a step's launch
+              overlaps the previous step's fetches
   plain_fp32  the plain FP32 per-op path (bbx_rt_run: one SIMT launch per command)
   roofline    the grouped tcgen05 kernel vs the measured bf16 tensor peak
   cpu_baseline  the CPU restatement of the reference's SGEMM on host cores
@@ -43,7 +45,7 @@ REF_BUDGET_S = 150.0  # the reference arm's whole run (warm-up + timed steps)
 # dram__bytes_read.sum + dram__bytes_write.sum of one launch of a smaller grid,
 # scaled to the full launch by its problem count (traffic grows with the
 # problems: each one reads its own A and B panels). 512 (the 2-SM pair): one
-# launch of the 4x4-block case (16 problems), 2727.9 MB, x4; 256: the 2x2-block
+# launch of the 4x4-block case (16 problems), 2528.8 MB, x4; 256: the 2x2-block
 # case (4 problems), 548 MB, x16.
 TRAFFIC_BYTES_PER_LAUNCH = {512: 10.12e9, 256: 8.77e9}
 TRAFFIC_SOURCE = {512: "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 16-problem launch (--grid 4), x4",
