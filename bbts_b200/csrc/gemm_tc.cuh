@@ -85,7 +85,6 @@ constexpr int kTcMetaBytes = kTcMetaMax * 16;
 // row-major C, or one 32 x 32-element box for column-major C.
 constexpr int kTcEpiPitch = 36;
 constexpr int kTcEpiSlot = 5120;
-constexpr int kTcEpiBytes = 4 * kTcEpiSlot;
 static_assert(32 * kTcEpiPitch * 4 <= kTcEpiSlot && 32 * 128 <= kTcEpiSlot && kTcEpiSlot % 1024 == 0, "epilogue slot");
 
 // EP8: eight epilogue warps (two per TMEM lane quarter, taking alternate
