@@ -73,7 +73,6 @@ constexpr long long kGatherChunk = 4096;
 // short rows and rows as long as a whole tensor both spread over warps. Each
 // warp carries kRowsPerWarp items at once, so every lane keeps that many
 // independent loads in flight.
-constexpr long long kGatherSeg = 1024;
 constexpr int kRowsPerWarp = 4;
 
 static bool row_mode_ok(const GatherArgs& a) {
@@ -254,22 +253,6 @@ struct GBItem {
 constexpr int kGBSmemBase = kGBStages * kGBSlot + kGBStages * 16 + kGBStages * kGBItems * (int)sizeof(GBItem);
 __host__ __device__ inline int gb_smem_bytes(int count) { return kGBSmemBase + 8 * count; }
 
-__device__ __forceinline__ void gb_locate(const GatherRec& R, long long local, long long& so, long long& dso,
-                                          int& len) {
-  const int outer = R.a.rank_o - 1;
-  const long long row = local / R.segs, start = (local - row * R.segs) * kGatherSeg;
-  long long rem = row, s = start, t = start;
-  for (int d = outer - 1; d >= 0; --d) {
-    const long long idx = rem % R.a.odims[d];
-    rem /= R.a.odims[d];
-    s += idx * R.a.istride[d];
-    t += idx * R.a.ostride[d];
-  }
-  so = s;
-  dso = t;
-  len = (int)min(kGatherSeg, R.row_len - start);
-}
-
 __global__ void __launch_bounds__(kGBThreads, 1) k_gather_bulk(const GatherRec* __restrict__ recs, int count,
                                                                 long long total_items, uint32_t* status) {
   extern __shared__ __align__(128) uint8_t gb_smem[];
@@ -309,13 +292,15 @@ __global__ void __launch_bounds__(kGBThreads, 1) k_gather_bulk(const GatherRec* 
           if (starts[mid] <= item) lo = mid; else hi = mid - 1;
         }
         const GatherRec& R = recs[lo];
-        gb_locate(R, item - starts[lo], it.so, it.dso, it.len);
+        const GatherSeg g = gather_segment(R, item - starts[lo]);
+        it.so = g.so;
+        it.dso = g.dso;
+        it.c0 = g.c0;
+        it.c1 = g.c1;
+        it.len = g.len;
         it.src = R.src;
         it.dst = R.dst;
         it.bf16 = R.dst_bf16;
-        it.c0 = (it.so + 3) & ~3LL;
-        it.c1 = (it.so + it.len) & ~3LL;
-        if (it.c1 < it.c0) it.c1 = it.c0;
         bytes = (uint32_t)(it.c1 - it.c0) * 4u;
         src = R.src;
       }

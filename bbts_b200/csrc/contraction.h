@@ -4,6 +4,7 @@
 // and matmuls of a whole wave into single launches).
 #pragma once
 #include <cstdint>
+#include "tile_order.h"  // BBX_HD
 
 namespace bbx {
 
@@ -66,6 +67,37 @@ struct GatherRec {
   long long segs;          // row mode: segments of kGatherSeg elements per row
   long long items_per_chunk;  // row mode: (row, segment) items per chunk
 };
+
+// Elements per work item of the row path: one segment of a row.
+constexpr long long kGatherSeg = 1024;
+
+// Row segment `local` (row-major over the record's rows, then segments) of a
+// row-path record: the source and destination element of its first element,
+// its length, and the whole 16-byte blocks [c0, c1) of its source range, in
+// elements (the source base is 16-byte aligned; c1 == c0 when none fits).
+struct GatherSeg {
+  long long so, dso, c0, c1;
+  int len;
+};
+BBX_HD GatherSeg gather_segment(const GatherRec& R, long long local) {
+  const int outer = R.a.rank_o - 1;
+  const long long row = local / R.segs, start = (local - row * R.segs) * kGatherSeg;
+  long long rem = row, s = start, t = start;
+  for (int d = outer - 1; d >= 0; --d) {
+    const long long idx = rem % R.a.odims[d];
+    rem /= R.a.odims[d];
+    s += idx * R.a.istride[d];
+    t += idx * R.a.ostride[d];
+  }
+  GatherSeg g;
+  g.so = s;
+  g.dso = t;
+  g.len = (int)(R.row_len - start < kGatherSeg ? R.row_len - start : kGatherSeg);
+  g.c0 = (s + 3) & ~3LL;
+  g.c1 = (s + g.len) & ~3LL;
+  if (g.c1 < g.c0) g.c1 = g.c0;
+  return g;
+}
 
 // Merges adjacent output modes that are contiguous in both the source and the
 // destination (a padded or permuted copy then runs as long rows).

@@ -429,8 +429,89 @@ static void test_tile_order() {
     }
 }
 
+// The bulk gather's row segments (gather_segment in csrc/contraction.h): over
+// random row-path records (outer modes in any source order, destination rows
+// padded), the segments write every destination element once and no padding,
+// read the source element the mode strides give, and their whole 16-byte
+// blocks [c0, c1) lie inside the segment with at most 3 elements on each side.
+static void test_gather_segments() {
+  unsigned seed = 777;
+  auto rnd = [&](int lo, int hi) {
+    seed = seed * 1103515245u + 12345u;
+    return lo + (int)((seed >> 8) % (unsigned)(hi - lo + 1));
+  };
+  for (int trial = 0; trial < 200; ++trial) {
+    const int rank = rnd(1, 3);
+    long long dims[3] = {1, 1, 1};
+    for (int d = 0; d < rank; ++d) dims[d] = d == rank - 1 ? rnd(1, 2600) : rnd(1, 7);
+    const long long L = dims[rank - 1];
+    // source: the outer modes in a random order of strides, the row contiguous
+    long long istr[3] = {0, 0, 0};
+    {
+      int order[2] = {0, 1};
+      if (rank == 3 && rnd(0, 1)) std::swap(order[0], order[1]);
+      long long st = L;
+      for (int q = rank - 2; q >= 0; --q) {
+        const int d = rank == 3 ? order[q] : q;
+        istr[d] = st;
+        st *= dims[d];
+      }
+      istr[rank - 1] = 1;
+    }
+    const long long pitch = L + rnd(0, 9);
+    long long ostr[3] = {0, 0, 0};
+    {
+      long long st = pitch;
+      for (int d = rank - 2; d >= 0; --d) {
+        ostr[d] = st;
+        st *= dims[d];
+      }
+      ostr[rank - 1] = 1;
+    }
+    bbx::GatherRec R{};
+    R.a.rank_o = rank;
+    for (int d = 0; d < rank; ++d) {
+      R.a.odims[d] = dims[d];
+      R.a.istride[d] = istr[d];
+      R.a.ostride[d] = ostr[d];
+    }
+    long long rows = 1;
+    for (int d = 0; d + 1 < rank; ++d) rows *= dims[d];
+    R.n = rows * L;
+    R.row_len = L;
+    R.segs = (L + bbx::kGatherSeg - 1) / bbx::kGatherSeg;
+    std::vector<int> hit(rows * pitch, 0);
+    bool ok = true;
+    for (long long local = 0; local < rows * R.segs; ++local) {
+      const bbx::GatherSeg g = bbx::gather_segment(R, local);
+      ok = ok && g.len > 0 && g.len <= bbx::kGatherSeg && g.so >= 0 && g.so + g.len <= R.n;
+      ok = ok && g.c0 % 4 == 0 && g.c1 % 4 == 0 && g.so <= g.c0 && g.c0 <= g.c1 && g.c1 <= g.so + g.len;
+      ok = ok && (g.c1 == g.c0 || (g.c0 - g.so <= 3 && g.so + g.len - g.c1 <= 3));
+      for (int y = 0; y < g.len && ok; ++y) {
+        const long long o = g.dso + y;
+        ok = o >= 0 && o < (long long)hit.size();
+        if (!ok) break;
+        ++hit[o];
+        // destination coordinates of o, and the source element they name
+        long long rem = o / pitch, x = o % pitch, src = x;
+        ok = x < L;
+        for (int d = rank - 2; d >= 0; --d) {
+          src += (rem % dims[d]) * istr[d];
+          rem /= dims[d];
+        }
+        ok = ok && src == g.so + y;
+      }
+    }
+    EXPECT(ok);
+    bool once = true;
+    for (long long o = 0; o < (long long)hit.size(); ++o) once = once && hit[o] == ((o % pitch) < L ? 1 : 0);
+    EXPECT(once);
+  }
+}
+
 int main() {
   test_tile_order();
+  test_gather_segments();
   test_contraction_orientation();
   test_sbbts_compile();
   test_bbts_roundtrip();
