@@ -252,6 +252,8 @@ struct GBItem {
 };
 constexpr int kGBSmemBase = kGBStages * kGBSlot + kGBStages * 16 + kGBStages * kGBItems * (int)sizeof(GBItem);
 __host__ __device__ inline int gb_smem_bytes(int count) { return kGBSmemBase + 8 * count; }
+static_assert(kGBSmemBase + 8 * kGBMaxRecs <= 232448, "dynamic shared memory per CTA");
+static_assert(kGBItems <= 32 && kGBItemBytes >= (int)kGatherSeg * 4, "one segment per producer lane and slot");
 
 __global__ void __launch_bounds__(kGBThreads, 1) k_gather_bulk(const GatherRec* __restrict__ recs, int count,
                                                                 long long total_items, uint32_t* status) {
